@@ -1,0 +1,245 @@
+"""Python host side of the B200 tile-Cholesky library.
+
+A thin ctypes layer over the C ABI in ``include/dplasma_b200.h``
+(``dplasma_b200/libdplasma_b200.so``).  It mirrors the dplasma calls of the
+Cholesky path -- ``dplasma_dpotrf``, ``dplasma_dpotrs``, ``dplasma_dposv``,
+``dplasma_dtrsm``, ``dplasma_dplgsy``, ``dplasma_dplrnt`` -- with the same
+argument meaning, enum values and return codes (INFO > 0 for a non positive
+definite leading minor, negative values for bad arguments), and adds helpers
+to lay numpy arrays out as dplasma tile descriptors.
+
+Every numerical call runs on the GPU through the shared library; when the
+library or a CUDA device is missing the calls raise instead of computing
+anything on the host.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libdplasma_b200.so")
+
+# enum values: src/include/dplasma/constants.h:78-99
+NoTrans, Trans, ConjTrans = 111, 112, 113
+Upper, Lower, UpperLower = 121, 122, 123
+NonUnit, Unit = 131, 132
+Left, Right = 141, 142
+InfNorm = 175
+MATRIX_DOUBLE = 3
+STORAGE_LAPACK, STORAGE_TILE = 0, 1
+HOST, DEVICE = 0, 1
+ERR_NOT_INITIALIZED, ERR_NOT_SUPPORTED, ERR_ILLEGAL_VALUE = -101, -103, -104
+
+
+class Desc(ctypes.Structure):
+    """parsec_tiled_matrix_t as declared in include/dplasma_b200.h."""
+
+    _fields_ = [(n, ctypes.c_int) for n in (
+        "mtype", "storage", "uplo", "mb", "nb", "lm", "ln", "i", "j", "m", "n", "mt", "nt", "lmt", "lnt", "lda",
+        "location")] + [("bsiz", ctypes.c_size_t), ("nb_local_tiles", ctypes.c_size_t), ("mat", ctypes.c_void_p)]
+
+
+_lib = None
+
+EXPORTS = (
+    "dplasma_b200_tile_offset", "dplasma_b200_desc_init", "dplasma_b200_sym_desc_init", "dplasma_b200_init",
+    "dplasma_b200_fini", "dplasma_b200_last_error", "dplasma_dpotrf", "dplasma_dpotrf_New",
+    "dplasma_dpotrf_Destruct", "dplasma_b200_taskpool_run", "dplasma_dpotrf_rec", "dplasma_dpotrf_setrecursive",
+    "dplasma_dpotrs", "dplasma_dposv", "dplasma_dtrsm", "dplasma_dplgsy", "dplasma_dplrnt", "dplasma_dlansy",
+    "dplasma_b200_last_factor_ms", "dplasma_b200_last_solve_ms", "dplasma_b200_last_launches",
+    "dplasma_b200_fp64_peak_tflops",
+)
+
+
+def lib():
+    """Load the shared library (build it first if it is missing)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        from . import build as _build
+        _build.build()
+    L = ctypes.CDLL(LIB_PATH)
+    P, I, D, U64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_ulonglong
+    pd = ctypes.POINTER(Desc)
+    L.dplasma_b200_tile_offset.restype = ctypes.c_int64
+    L.dplasma_b200_tile_offset.argtypes = [pd, I, I]
+    L.dplasma_b200_desc_init.argtypes = [pd, I, I, I, I, I, I, I, I, I, I]
+    L.dplasma_b200_sym_desc_init.argtypes = [pd, I, I, I, I, I, I, I, I, I, I]
+    L.dplasma_b200_init.restype = P
+    L.dplasma_b200_init.argtypes = [I]
+    L.dplasma_b200_fini.argtypes = [ctypes.POINTER(P)]
+    L.dplasma_b200_last_error.restype = ctypes.c_char_p
+    L.dplasma_b200_last_error.argtypes = [P]
+    L.dplasma_dpotrf.argtypes = [P, I, pd]
+    L.dplasma_dpotrf_New.restype = P
+    L.dplasma_dpotrf_New.argtypes = [I, pd, ctypes.POINTER(I)]
+    L.dplasma_dpotrf_Destruct.argtypes = [P]
+    L.dplasma_b200_taskpool_run.argtypes = [P, P]
+    L.dplasma_dpotrf_rec.argtypes = [P, I, pd, I]
+    L.dplasma_dpotrf_setrecursive.argtypes = [P, I]
+    L.dplasma_dpotrs.argtypes = [P, I, pd, pd]
+    L.dplasma_dposv.argtypes = [P, I, pd, pd]
+    L.dplasma_dtrsm.argtypes = [P, I, I, I, I, D, pd, pd]
+    L.dplasma_dplgsy.argtypes = [P, D, I, pd, U64]
+    L.dplasma_dplrnt.argtypes = [P, I, pd, U64]
+    L.dplasma_dlansy.restype = D
+    L.dplasma_dlansy.argtypes = [P, I, I, pd]
+    for f in ("dplasma_b200_last_factor_ms", "dplasma_b200_last_solve_ms"):
+        getattr(L, f).restype = D
+        getattr(L, f).argtypes = [P]
+    L.dplasma_b200_last_launches.argtypes = [P]
+    L.dplasma_b200_fp64_peak_tflops.restype = D
+    L.dplasma_b200_fp64_peak_tflops.argtypes = [P]
+    _lib = L
+    return L
+
+
+# ---------------------------------------------------------------------------
+# descriptors over numpy / device buffers
+# ---------------------------------------------------------------------------
+def desc_general(m: int, n: int, mb: int, nb: int, storage: int = STORAGE_TILE, lda: int | None = None) -> Desc:
+    d = Desc()
+    lib().dplasma_b200_desc_init(ctypes.byref(d), MATRIX_DOUBLE, storage, mb, nb, m, n, 0, 0, m, n)
+    if storage == STORAGE_LAPACK and lda is not None:
+        d.lda = lda
+        d.lm = lda
+    return d
+
+
+def desc_sym(n: int, nb: int, uplo: int) -> Desc:
+    d = Desc()
+    lib().dplasma_b200_sym_desc_init(ctypes.byref(d), MATRIX_DOUBLE, nb, nb, n, n, 0, 0, n, n, uplo)
+    return d
+
+
+def desc_elems(d: Desc) -> int:
+    return d.lda * d.ln if d.storage == STORAGE_LAPACK else d.bsiz * d.nb_local_tiles
+
+
+def tile_offset(d: Desc, m: int, n: int) -> int:
+    return lib().dplasma_b200_tile_offset(ctypes.byref(d), m, n)
+
+
+def _tiles(d: Desc):
+    for n in range(d.nt):
+        for m in range(d.mt):
+            off = tile_offset(d, m, n)
+            if off < 0:
+                continue
+            tm = d.m - m * d.mb if m == d.mt - 1 else d.mb
+            tn = d.n - n * d.nb if n == d.nt - 1 else d.nb
+            yield m, n, off, tm, tn
+
+
+def pack(dense: np.ndarray, d: Desc, buf: np.ndarray | None = None) -> np.ndarray:
+    """Lay a dense (m x n) array out in descriptor d's storage (tiles of the
+    stored triangle only for symmetric storage); returns the flat buffer."""
+    if buf is None:
+        buf = np.zeros(desc_elems(d), dtype=np.float64)
+    if d.storage == STORAGE_LAPACK:
+        v = buf[: d.lda * d.n].reshape(d.n, d.lda).T
+        v[: d.m, : d.n] = dense
+        return buf
+    for m, n, off, tm, tn in _tiles(d):
+        t = buf[off: off + d.bsiz].reshape(d.nb, d.mb).T
+        t[:tm, :tn] = dense[m * d.mb: m * d.mb + tm, n * d.nb: n * d.nb + tn]
+    return buf
+
+
+def unpack(buf: np.ndarray, d: Desc, fill: float = 0.0) -> np.ndarray:
+    """Inverse of pack: dense (m x n) array; entries of unstored tiles = fill."""
+    out = np.full((d.m, d.n), fill, dtype=np.float64, order="F")
+    if d.storage == STORAGE_LAPACK:
+        out[:, :] = buf[: d.lda * d.n].reshape(d.n, d.lda).T[: d.m, : d.n]
+        return out
+    for m, n, off, tm, tn in _tiles(d):
+        t = buf[off: off + d.bsiz].reshape(d.nb, d.mb).T
+        out[m * d.mb: m * d.mb + tm, n * d.nb: n * d.nb + tn] = t[:tm, :tn]
+    return out
+
+
+# ---------------------------------------------------------------------------
+# context and calls
+# ---------------------------------------------------------------------------
+class Context:
+    """One GPU, one stream and its device workspace (the parsec_context_t
+    argument of the dplasma calls)."""
+
+    def __init__(self, device: int = 0):
+        self.h = lib().dplasma_b200_init(device)
+        if not self.h:
+            raise RuntimeError("dplasma_b200_init failed: no usable CUDA device")
+
+    def close(self):
+        if self.h:
+            h = ctypes.c_void_p(self.h)
+            lib().dplasma_b200_fini(ctypes.byref(h))
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- instrumentation
+    def last_error(self) -> str:
+        return lib().dplasma_b200_last_error(self.h).decode()
+
+    def last_factor_ms(self) -> float:
+        return lib().dplasma_b200_last_factor_ms(self.h)
+
+    def last_solve_ms(self) -> float:
+        return lib().dplasma_b200_last_solve_ms(self.h)
+
+    def last_launches(self) -> int:
+        return lib().dplasma_b200_last_launches(self.h)
+
+    def fp64_peak_tflops(self) -> float:
+        return lib().dplasma_b200_fp64_peak_tflops(self.h)
+
+    # -- the dplasma calls (descriptor `mat` must be set by the caller)
+    def dpotrf(self, uplo: int, A: Desc) -> int:
+        return lib().dplasma_dpotrf(self.h, uplo, ctypes.byref(A))
+
+    def dpotrs(self, uplo: int, A: Desc, B: Desc) -> int:
+        return lib().dplasma_dpotrs(self.h, uplo, ctypes.byref(A), ctypes.byref(B))
+
+    def dposv(self, uplo: int, A: Desc, B: Desc) -> int:
+        return lib().dplasma_dposv(self.h, uplo, ctypes.byref(A), ctypes.byref(B))
+
+    def dtrsm(self, side: int, uplo: int, trans: int, diag: int, alpha: float, A: Desc, B: Desc) -> int:
+        return lib().dplasma_dtrsm(self.h, side, uplo, trans, diag, alpha, ctypes.byref(A), ctypes.byref(B))
+
+    def dplgsy(self, bump: float, uplo: int, A: Desc, seed: int) -> int:
+        return lib().dplasma_dplgsy(self.h, bump, uplo, ctypes.byref(A), seed)
+
+    def dplrnt(self, diagdom: int, A: Desc, seed: int) -> int:
+        return lib().dplasma_dplrnt(self.h, diagdom, ctypes.byref(A), seed)
+
+    def dlansy(self, ntype: int, uplo: int, A: Desc) -> float:
+        return lib().dplasma_dlansy(self.h, ntype, uplo, ctypes.byref(A))
+
+
+def attach(d: Desc, buf) -> Desc:
+    """Point descriptor d at `buf`: a numpy array (host) or a torch CUDA tensor
+    (device).  The caller keeps `buf` alive."""
+    if isinstance(buf, np.ndarray):
+        assert buf.dtype == np.float64 and buf.flags.c_contiguous and buf.size >= desc_elems(d)
+        d.mat = buf.ctypes.data
+        d.location = HOST
+    else:  # torch tensor on the GPU
+        assert buf.is_cuda and str(buf.dtype) == "torch.float64" and buf.is_contiguous() and buf.numel() >= desc_elems(d)
+        d.mat = buf.data_ptr()
+        d.location = DEVICE
+    return d

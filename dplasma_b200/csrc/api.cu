@@ -1,0 +1,459 @@
+// api.cu -- the C ABI (include/dplasma_b200.h): dplasma entry points of the
+// Cholesky path mapped onto the device kernels.  Argument checks and return
+// codes follow the reference wrappers cited at each function.
+#include <cuda_runtime.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <new>
+
+#include "internal.h"
+
+using namespace db2;
+
+namespace db2 {
+int potrf_max_blocks_per_sm();
+int sweep_max_blocks_per_sm();
+}
+
+struct parsec_taskpool_s {
+    int kind;                     // 1: dpotrf
+    dplasma_enum_t uplo;
+    parsec_tiled_matrix_t *A;
+    int *info;
+    int hmb;
+};
+
+static void dplasma_error(const char *func, const char *msg) { fprintf(stderr, "[%s] %s\n", func, msg); }
+
+static int getenv_int(const char *name, int dflt)
+{
+    const char *v = getenv(name);
+    return v ? atoi(v) : dflt;
+}
+
+// ---------------------------------------------------------------------------
+// descriptors
+// ---------------------------------------------------------------------------
+extern "C" int64_t dplasma_b200_tile_offset(const parsec_tiled_matrix_t *A, int m, int n)
+{
+    return tile_offset(A, m, n);
+}
+
+extern "C" void dplasma_b200_desc_init(parsec_tiled_matrix_t *A, int mtype, int storage, int mb, int nb, int lm,
+                                       int ln, int i, int j, int m, int n)
+{
+    memset(A, 0, sizeof(*A));
+    A->mtype = mtype;
+    A->storage = storage;
+    A->uplo = dplasmaUpperLower;
+    A->mb = mb;
+    A->nb = nb;
+    A->lm = lm;
+    A->ln = ln;
+    A->i = i;
+    A->j = j;
+    A->m = m;
+    A->n = n;
+    A->mt = (m + mb - 1) / mb;
+    A->nt = (n + nb - 1) / nb;
+    A->lmt = (lm + mb - 1) / mb;
+    A->lnt = (ln + nb - 1) / nb;
+    A->lda = (storage == PARSEC_MATRIX_LAPACK) ? lm : mb;
+    A->location = DPLASMA_B200_HOST;
+    A->bsiz = (size_t)mb * nb;
+    A->nb_local_tiles = (size_t)A->lmt * A->lnt;
+    A->mat = nullptr;
+}
+
+extern "C" void dplasma_b200_sym_desc_init(parsec_tiled_matrix_t *A, int mtype, int mb, int nb, int lm, int ln, int i,
+                                           int j, int m, int n, dplasma_enum_t uplo)
+{
+    dplasma_b200_desc_init(A, mtype, PARSEC_MATRIX_TILE, mb, nb, lm, ln, i, j, m, n);
+    A->uplo = uplo;
+    A->nb_local_tiles = (size_t)A->lmt * (A->lmt + 1) / 2;
+}
+
+static int check_square(const char *func, const parsec_tiled_matrix_t *A)
+{
+    if (!A || A->mtype != PARSEC_MATRIX_DOUBLE || A->m != A->n || A->mb != A->nb || A->mb <= 0 || A->m < 0 ||
+        A->i != 0 || A->j != 0 || (A->m > 0 && !A->mat) ||
+        (A->storage != PARSEC_MATRIX_TILE && A->storage != PARSEC_MATRIX_LAPACK) ||
+        (A->storage == PARSEC_MATRIX_LAPACK && A->lda < A->m)) {
+        dplasma_error(func, "unsupported or malformed descriptor");
+        return DPLASMA_ERR_ILLEGAL_VALUE;
+    }
+    return 0;
+}
+
+static int check_general(const char *func, const parsec_tiled_matrix_t *B)
+{
+    if (!B || B->mtype != PARSEC_MATRIX_DOUBLE || B->mb <= 0 || B->nb <= 0 || B->m < 0 || B->n < 0 || B->i != 0 ||
+        B->j != 0 || ((B->m > 0 && B->n > 0) && !B->mat) ||
+        (B->storage == PARSEC_MATRIX_TILE && B->uplo != dplasmaUpperLower) ||
+        (B->storage != PARSEC_MATRIX_TILE && B->storage != PARSEC_MATRIX_LAPACK) ||
+        (B->storage == PARSEC_MATRIX_LAPACK && B->lda < B->m)) {
+        dplasma_error(func, "unsupported or malformed descriptor");
+        return DPLASMA_ERR_ILLEGAL_VALUE;
+    }
+    return 0;
+}
+
+static bool in_place_ok(const parsec_tiled_matrix_t *A, dplasma_enum_t uplo, const Geom &g)
+{
+    return A->location == DPLASMA_B200_DEVICE && A->storage == PARSEC_MATRIX_TILE && A->uplo == dplasmaLower &&
+           uplo == dplasmaLower && g.nbi == g.nb && (g.n % g.nb) == 0 && A->lmt == g.mt;
+}
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
+extern "C" parsec_context_t *dplasma_b200_init(int device)
+{
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+        cudaGetLastError();
+        dplasma_error("dplasma_b200_init", "no CUDA device available");
+        return nullptr;
+    }
+    if (device < 0 || device >= ndev) {
+        dplasma_error("dplasma_b200_init", "illegal device index");
+        return nullptr;
+    }
+    parsec_context_t *p = new (std::nothrow) parsec_context_t();
+    if (!p) return nullptr;
+    Context *ctx = &p->impl;
+    ctx->device = device;
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess ||
+        cudaEventCreate(&ctx->ev2) != cudaSuccess || cudaEventCreate(&ctx->ev3) != cudaSuccess) {
+        dplasma_error("dplasma_b200_init", cudaGetErrorString(cudaGetLastError()));
+        delete p;
+        return nullptr;
+    }
+    cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, device);
+    int occ = potrf_max_blocks_per_sm();
+    if (occ < 1) {
+        dplasma_error("dplasma_b200_init", "the factorization kernel cannot be resident on this device");
+        delete p;
+        return nullptr;
+    }
+    ctx->potrf_grid = getenv_int("DPLASMA_B200_GRID", ctx->sms * occ);
+    ctx->potrf_delay = getenv_int("DPLASMA_B200_DELAY", 3 * ctx->potrf_grid);
+    int occs = sweep_max_blocks_per_sm();
+    ctx->solve_grid = ctx->sms * (occs < 1 ? 1 : occs);
+    ctx->self_check = getenv_int("DPLASMA_B200_SELFCHECK", 0) != 0;
+    if (const char *tp = getenv("DPLASMA_B200_TRACE")) snprintf(ctx->trace_path, sizeof(ctx->trace_path), "%s", tp);
+    const int lim_ms = getenv_int("DPLASMA_B200_WAIT_LIMIT_MS", 4000);
+    ctx->dep_limit_ns = (uint64_t)lim_ms * 1000000ull;
+    ctx->pipe_limit_ns = (uint64_t)lim_ms * 1000000ull;
+    return p;
+}
+
+extern "C" void dplasma_b200_fini(parsec_context_t **pctx)
+{
+    if (!pctx || !*pctx) return;
+    Context *ctx = &(*pctx)->impl;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    for (int i = 0; i < BUF_COUNT; ++i)
+        if (ctx->bufs[i]) cudaFree(ctx->bufs[i]);
+    cudaEventDestroy(ctx->ev0);
+    cudaEventDestroy(ctx->ev1);
+    cudaEventDestroy(ctx->ev2);
+    cudaEventDestroy(ctx->ev3);
+    cudaStreamDestroy(ctx->stream);
+    delete *pctx;
+    *pctx = nullptr;
+}
+
+extern "C" const char *dplasma_b200_last_error(const parsec_context_t *p) { return p ? p->impl.errmsg : "no context"; }
+extern "C" double dplasma_b200_last_factor_ms(const parsec_context_t *p) { return p ? p->impl.last_factor_ms : 0.0; }
+extern "C" double dplasma_b200_last_solve_ms(const parsec_context_t *p) { return p ? p->impl.last_solve_ms : 0.0; }
+extern "C" int dplasma_b200_last_launches(const parsec_context_t *p) { return p ? p->impl.launches : 0; }
+extern "C" double dplasma_b200_fp64_peak_tflops(parsec_context_t *p)
+{
+    if (!p) return -1.0;
+    cudaSetDevice(p->impl.device);
+    return fp64_peak_tflops(&p->impl);
+}
+
+// ---------------------------------------------------------------------------
+// factorization
+// ---------------------------------------------------------------------------
+static int potrf_impl(Context *ctx, dplasma_enum_t uplo, parsec_tiled_matrix_t *A, double **factor_out, Geom *gout)
+{
+    Geom g = make_geom(A->m, A->mb);
+    if (gout) *gout = g;
+    if (A->m == 0) return 0;
+    if (g.mt > 65535 || g.nbi > 512) {
+        ctx->set_error("unsupported geometry (mt=%d, nb=%d): at most 65535 tile rows and nb <= 512", g.mt, g.nb);
+        return DPLASMA_ERR_INTERNAL_LIMIT;
+    }
+    const bool inplace = in_place_ok(A, uplo, g);
+    double *dA = inplace ? (double *)A->mat : (double *)ctx->buffer(BUF_A, g.elems() * sizeof(double));
+    if (!dA) return DPLASMA_ERR_OUT_OF_RESOURCES;
+    int rc;
+    if (!inplace && (rc = upload_sym(ctx, A, uplo, g, dA))) return rc;
+    int info = 0;
+    if ((rc = potrf_device(ctx, dA, g.mt, g.nbi, g.nb, g.n, &info))) return rc;
+    if (!inplace && (rc = download_sym(ctx, A, uplo, g, dA))) return rc;
+    if (factor_out) *factor_out = dA;
+    return info;
+}
+
+// src/zpotrf_wrapper.c:345-371
+extern "C" int dplasma_dpotrf(parsec_context_t *parsec, dplasma_enum_t uplo, parsec_tiled_matrix_t *A)
+{
+    if (uplo != dplasmaUpper && uplo != dplasmaLower) {
+        dplasma_error("dplasma_dpotrf_New", "illegal value of uplo");
+        return -1;
+    }
+    if (!parsec) return DPLASMA_ERR_NOT_INITIALIZED;
+    int rc = check_square("dplasma_dpotrf", A);
+    if (rc) return rc;
+    Context *ctx = &parsec->impl;
+    cudaSetDevice(ctx->device);
+    ctx->launches = 0;
+    ctx->errmsg[0] = 0;
+    return potrf_impl(ctx, uplo, A, nullptr, nullptr);
+}
+
+// src/zpotrf_wrapper.c:193-258
+extern "C" parsec_taskpool_t *dplasma_dpotrf_New(dplasma_enum_t uplo, parsec_tiled_matrix_t *A, int *info)
+{
+    if (uplo != dplasmaUpper && uplo != dplasmaLower) {
+        dplasma_error("dplasma_dpotrf_New", "illegal value of uplo");
+        return nullptr;
+    }
+    if (!info) return nullptr;
+    *info = 0;
+    parsec_taskpool_t *tp = new (std::nothrow) parsec_taskpool_t();
+    if (!tp) return nullptr;
+    tp->kind = 1;
+    tp->uplo = uplo;
+    tp->A = A;
+    tp->info = info;
+    tp->hmb = 0;
+    return tp;
+}
+
+extern "C" void dplasma_dpotrf_Destruct(parsec_taskpool_t *tp) { delete tp; }
+
+extern "C" void dplasma_dpotrf_setrecursive(parsec_taskpool_t *tp, int hmb)
+{
+    if (tp) tp->hmb = hmb;
+}
+
+extern "C" int dplasma_b200_taskpool_run(parsec_context_t *parsec, parsec_taskpool_t *tp)
+{
+    if (!parsec) return DPLASMA_ERR_NOT_INITIALIZED;
+    if (!tp || tp->kind != 1) return DPLASMA_ERR_ILLEGAL_VALUE;
+    const int r = dplasma_dpotrf(parsec, tp->uplo, tp->A);
+    if (r < 0) return r;
+    *tp->info = r;
+    return 0;
+}
+
+// src/zpotrf_wrapper.c:425-451
+extern "C" int dplasma_dpotrf_rec(parsec_context_t *parsec, dplasma_enum_t uplo, parsec_tiled_matrix_t *A, int hmb)
+{
+    (void)hmb;
+    return dplasma_dpotrf(parsec, uplo, A);
+}
+
+// ---------------------------------------------------------------------------
+// triangular solves
+// ---------------------------------------------------------------------------
+// Solve with the device factor dA (geometry g): forward then backward sweep,
+// or only one of them.  B is the caller's right-hand side descriptor.
+static int solve_impl(Context *ctx, const double *dA, const double *W, const Geom &g, parsec_tiled_matrix_t *B,
+                      int sweeps /* 1 fwd, 2 bwd, 3 both */, double alpha)
+{
+    const int nrhs = B->n;
+    if (nrhs == 0 || g.n == 0) return 0;
+    const int nrhs_pad = ((nrhs + 7) / 8) * 8;
+    const int npad = g.mt * g.nbi;
+    double *dB = (double *)ctx->buffer(BUF_B, (size_t)npad * nrhs_pad * sizeof(double));
+    if (!dB) return DPLASMA_ERR_OUT_OF_RESOURCES;
+    int rc;
+    if ((rc = upload_rhs(ctx, B, g.nb, g.nbi, npad, nrhs_pad, dB))) return rc;
+    CK(cudaEventRecord(ctx->ev2, ctx->stream));
+    if ((sweeps & 1) && (rc = trsm_sweep(ctx, dA, W, g, dB, npad, nrhs_pad, 0, alpha))) return rc;
+    if ((sweeps & 2) && (rc = trsm_sweep(ctx, dA, W, g, dB, npad, nrhs_pad, 1, (sweeps & 1) ? 1.0 : alpha))) return rc;
+    CK(cudaEventRecord(ctx->ev3, ctx->stream));
+    if ((rc = download_rhs(ctx, B, g.nb, g.nbi, npad, nrhs_pad, dB))) return rc;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->ev2, ctx->ev3);
+    ctx->last_solve_ms = ms;
+    return 0;
+}
+
+static int load_factor(Context *ctx, dplasma_enum_t uplo, const parsec_tiled_matrix_t *A, const Geom &g, int unit_diag,
+                       const double **dA_out, double **W_out)
+{
+    const bool inplace = in_place_ok(A, uplo, g);
+    double *dA = inplace ? (double *)A->mat : (double *)ctx->buffer(BUF_A, g.elems() * sizeof(double));
+    double *W = (double *)ctx->buffer(BUF_W2, (size_t)g.mt * (g.nbi / 128) * 128 * 128 * sizeof(double));
+    if (!dA || !W) return DPLASMA_ERR_OUT_OF_RESOURCES;
+    int rc;
+    if (!inplace && (rc = upload_sym(ctx, A, uplo, g, dA))) return rc;
+    if ((rc = trtri_diag(ctx, dA, g, W, unit_diag))) return rc;
+    *dA_out = dA;
+    *W_out = W;
+    return 0;
+}
+
+// src/zpotrs_wrapper.c:56-97
+extern "C" int dplasma_dpotrs(parsec_context_t *parsec, dplasma_enum_t uplo, const parsec_tiled_matrix_t *A,
+                              parsec_tiled_matrix_t *B)
+{
+    if (uplo != dplasmaUpper && uplo != dplasmaLower) {
+        dplasma_error("dplasma_dpotrs", "illegal value of uplo");
+        return -1;
+    }
+    if (!parsec) return DPLASMA_ERR_NOT_INITIALIZED;
+    int rc;
+    if ((rc = check_square("dplasma_dpotrs", A)) || (rc = check_general("dplasma_dpotrs", B))) return rc;
+    if (B->m != A->n) {
+        dplasma_error("dplasma_dpotrs", "illegal matrix B");
+        return -6;
+    }
+    Context *ctx = &parsec->impl;
+    cudaSetDevice(ctx->device);
+    ctx->launches = 0;
+    ctx->errmsg[0] = 0;
+    if (A->m == 0) return 0;
+    Geom g = make_geom(A->m, A->mb);
+    const double *dA;
+    double *W;
+    if ((rc = load_factor(ctx, uplo, A, g, 0, &dA, &W))) return rc;
+    return solve_impl(ctx, dA, W, g, B, 3, 1.0);
+}
+
+// src/zposv_wrapper.c:63-113
+extern "C" int dplasma_dposv(parsec_context_t *parsec, dplasma_enum_t uplo, parsec_tiled_matrix_t *A,
+                             parsec_tiled_matrix_t *B)
+{
+    if (uplo != dplasmaUpper && uplo != dplasmaLower) {
+        dplasma_error("dplasma_dposv", "illegal value of uplo");
+        return -1;
+    }
+    if (!parsec) return DPLASMA_ERR_NOT_INITIALIZED;
+    int rc;
+    if ((rc = check_square("dplasma_dposv", A)) || (rc = check_general("dplasma_dposv", B))) return rc;
+    if (B->m != A->n) {
+        dplasma_error("dplasma_dposv", "illegal matrix B");
+        return -6;
+    }
+    Context *ctx = &parsec->impl;
+    cudaSetDevice(ctx->device);
+    ctx->launches = 0;
+    ctx->errmsg[0] = 0;
+    double *dA = nullptr;
+    Geom g;
+    const int info = potrf_impl(ctx, uplo, A, &dA, &g);
+    if (info != 0 || A->m == 0) return info;
+    // the factorization left the inverses of the diagonal blocks in BUF_W
+    return (rc = solve_impl(ctx, dA, (double *)ctx->buffer(BUF_W, 0), g, B, 3, 1.0)) ? rc : 0;
+}
+
+// src/ztrsm_wrapper.c:263-309 (left side: src/ztrsm_L{LN,LT,UN,UT}.jdf)
+extern "C" int dplasma_dtrsm(parsec_context_t *parsec, dplasma_enum_t side, dplasma_enum_t uplo,
+                             dplasma_enum_t trans, dplasma_enum_t diag, double alpha,
+                             const parsec_tiled_matrix_t *A, parsec_tiled_matrix_t *B)
+{
+    if (side != dplasmaLeft && side != dplasmaRight) {
+        dplasma_error("dplasma_dtrsm", "illegal value of side");
+        return -1;
+    }
+    if (uplo != dplasmaUpper && uplo != dplasmaLower) {
+        dplasma_error("dplasma_dtrsm", "illegal value of uplo");
+        return -2;
+    }
+    if (trans != dplasmaConjTrans && trans != dplasmaNoTrans && trans != dplasmaTrans) {
+        dplasma_error("dplasma_dtrsm", "illegal value of trans");
+        return -3;
+    }
+    if (diag != dplasmaUnit && diag != dplasmaNonUnit) {
+        dplasma_error("dplasma_dtrsm", "illegal value of diag");
+        return -4;
+    }
+    if (!A || !B || (A->m != A->n) || ((side == dplasmaLeft) && (A->n != B->m)) ||
+        ((side == dplasmaRight) && (A->n != B->n))) {
+        dplasma_error("dplasma_dtrsm", "illegal matrix A");
+        return -6;
+    }
+    if (side == dplasmaRight) {
+        dplasma_error("dplasma_dtrsm", "side == dplasmaRight is not provided by this library");
+        return DPLASMA_ERR_NOT_SUPPORTED;
+    }
+    if (!parsec) return DPLASMA_ERR_NOT_INITIALIZED;
+    int rc;
+    if ((rc = check_square("dplasma_dtrsm", A)) || (rc = check_general("dplasma_dtrsm", B))) return rc;
+    Context *ctx = &parsec->impl;
+    cudaSetDevice(ctx->device);
+    ctx->launches = 0;
+    ctx->errmsg[0] = 0;
+    if (A->m == 0) return 0;
+    Geom g = make_geom(A->m, A->mb);
+    const double *dA;
+    double *W;
+    if ((rc = load_factor(ctx, uplo, A, g, diag == dplasmaUnit, &dA, &W))) return rc;
+    // device tiles hold L (lower) or U^T (upper)
+    const bool notrans = (trans == dplasmaNoTrans);
+    const bool backward = (uplo == dplasmaLower) ? !notrans : notrans;
+    return solve_impl(ctx, dA, W, g, B, backward ? 2 : 1, alpha);
+}
+
+// ---------------------------------------------------------------------------
+// generators and norms
+// ---------------------------------------------------------------------------
+// src/zplgsy_wrapper.c:185-215
+extern "C" int dplasma_dplgsy(parsec_context_t *parsec, double bump, dplasma_enum_t uplo, parsec_tiled_matrix_t *A,
+                              unsigned long long int seed)
+{
+    if ((uplo != dplasmaLower) && (uplo != dplasmaUpper) && (uplo != dplasmaUpperLower)) {
+        dplasma_error("dplasma_dplgsy", "illegal value of type");
+        return -3;
+    }
+    if (!parsec) return DPLASMA_ERR_NOT_INITIALIZED;
+    if (!A || A->mtype != PARSEC_MATRIX_DOUBLE || (A->m > 0 && A->n > 0 && !A->mat)) return -4;
+    Context *ctx = &parsec->impl;
+    cudaSetDevice(ctx->device);
+    ctx->launches = 0;
+    if (A->m == 0 || A->n == 0) return 0;
+    return generate_plgsy(ctx, bump, uplo, A, seed);
+}
+
+// src/zplrnt_wrapper.c (dplasma_zplrnt)
+extern "C" int dplasma_dplrnt(parsec_context_t *parsec, int diagdom, parsec_tiled_matrix_t *A,
+                              unsigned long long int seed)
+{
+    if (!parsec) return DPLASMA_ERR_NOT_INITIALIZED;
+    if (!A || A->mtype != PARSEC_MATRIX_DOUBLE || (A->m > 0 && A->n > 0 && !A->mat)) return -3;
+    Context *ctx = &parsec->impl;
+    cudaSetDevice(ctx->device);
+    ctx->launches = 0;
+    if (A->m == 0 || A->n == 0) return 0;
+    return generate_plrnt(ctx, diagdom, A, seed);
+}
+
+extern "C" double dplasma_dlansy(parsec_context_t *parsec, dplasma_enum_t ntype, dplasma_enum_t uplo,
+                                 const parsec_tiled_matrix_t *A)
+{
+    if (!parsec || ntype != dplasmaInfNorm || (uplo != dplasmaLower && uplo != dplasmaUpper)) return -1.0;
+    if (check_square("dplasma_dlansy", A)) return -1.0;
+    Context *ctx = &parsec->impl;
+    cudaSetDevice(ctx->device);
+    if (A->m == 0) return 0.0;
+    Geom g = make_geom(A->m, A->mb);
+    const bool inplace = in_place_ok(A, uplo, g);
+    double *dA = inplace ? (double *)A->mat : (double *)ctx->buffer(BUF_A, g.elems() * sizeof(double));
+    if (!dA) return -1.0;
+    if (!inplace && upload_sym(ctx, A, uplo, g, dA)) return -1.0;
+    double out = -1.0;
+    if (lansy_inf_device(ctx, dA, g, &out)) return -1.0;
+    return out;
+}
+

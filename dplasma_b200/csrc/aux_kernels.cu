@@ -1,0 +1,126 @@
+// aux_kernels.cu -- norms on the device tiles and the FP64 tensor-core peak
+// probe used as the roofline denominator.
+#include <cuda_runtime.h>
+
+#include "dev_common.cuh"
+#include "internal.h"
+
+namespace db2 {
+
+// ---------------------------------------------------------------------------
+// infinity norm of the symmetric matrix held by the device tiles (lower):
+// row sums of |A| with each strictly-lower entry counted for its row and its
+// column, restricted to the n valid rows; dplasma_dlansy(InfNorm).
+// ---------------------------------------------------------------------------
+__global__ void rowsum_sym_kernel(const double *A, int mt, int nb, int nbi, int n, double *rows)
+{
+    // block per tile, linear tile index
+    const int64_t idx = blockIdx.x;
+    int lo = 0, hi = mt - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) / 2;
+        int64_t start = (int64_t)mid * mt - ((int64_t)mid * (mid - 1)) / 2;
+        if (start <= idx) lo = mid; else hi = mid - 1;
+    }
+    const int tn = lo;
+    const int tm = tn + (int)(idx - ((int64_t)tn * mt - ((int64_t)tn * (tn - 1)) / 2));
+    const double *T = A + idx * (int64_t)nbi * nbi;
+    const int rows_m = (tm == mt - 1) ? n - tm * nb : nb;
+    const int rows_n = (tn == mt - 1) ? n - tn * nb : nb;
+    // column sums (contributions of the mirrored upper part to rows of tile n)
+    for (int c = threadIdx.x; c < rows_n; c += blockDim.x) {
+        double cs = 0.0;
+        for (int r = 0; r < rows_m; ++r) {
+            if (tm == tn && r <= c) continue;
+            cs += fabs(T[(int64_t)c * nbi + r]);
+        }
+        atomicAdd(rows + (int64_t)tn * nb + c, cs);
+    }
+    for (int r = threadIdx.x; r < rows_m; r += blockDim.x) {
+        double rs = 0.0;
+        const int cmax = (tm == tn) ? r : rows_n - 1;
+        for (int c = 0; c <= cmax; ++c) rs += fabs(T[(int64_t)c * nbi + r]);
+        atomicAdd(rows + (int64_t)tm * nb + r, rs);
+    }
+}
+
+__global__ void max_kernel(const double *v, int n, double *out)
+{
+    __shared__ double sm[256];
+    double m = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double x = v[i];
+        if (x != x) m = x; else if (!(m != m) && x > m) m = x;
+    }
+    sm[threadIdx.x] = m;
+    __syncthreads();
+    for (int s = 128; s > 0; s >>= 1) {
+        if (threadIdx.x < s) {
+            const double a = sm[threadIdx.x], b = sm[threadIdx.x + s];
+            sm[threadIdx.x] = (a != a) ? a : ((b != b) ? b : (a > b ? a : b));
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = sm[0];
+}
+
+int lansy_inf_device(Context *ctx, const double *dA, const Geom &g, double *out)
+{
+    double *rows = (double *)ctx->buffer(BUF_NORM, ((size_t)g.n + 1) * sizeof(double));
+    if (!rows) return DPLASMA_ERR_OUT_OF_RESOURCES;
+    CK(cudaMemsetAsync(rows, 0, ((size_t)g.n + 1) * sizeof(double), ctx->stream));
+    rowsum_sym_kernel<<<(unsigned)g.ntiles(), 256, 0, ctx->stream>>>(dA, g.mt, g.nb, g.nbi, g.n, rows);
+    CK(cudaGetLastError());
+    max_kernel<<<1, 256, 0, ctx->stream>>>(rows, g.n, rows + g.n);
+    CK(cudaGetLastError());
+    ctx->launches += 2;
+    CK(cudaMemcpyAsync(out, rows + g.n, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// FP64 tensor-core peak: register-only DMMA chains on every SM.
+// ---------------------------------------------------------------------------
+constexpr int PEAK_ITERS = 4096;
+__global__ void __launch_bounds__(256) dmma_peak_kernel(double *out, double seed)
+{
+    double a0 = seed + threadIdx.x * 1e-3, a1 = a0 + 1.0, b0 = seed - threadIdx.x * 1e-3;
+    double c[8][4];
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) c[j][q] = 0.0;
+    for (int it = 0; it < PEAK_ITERS; ++it) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) dmma_16x8x4(c[j], a0, a1, b0);
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) s += c[j][q];
+    if (s == 1234.5678) out[0] = s;   // keeps the chains live
+}
+
+double fp64_peak_tflops(Context *ctx)
+{
+    double *out = (double *)ctx->buffer(BUF_NORM, 64);
+    if (!out) return -1.0;
+    const int blocks = ctx->sms * 2;
+    float best = 1e30f;
+    for (int rep = 0; rep < 4; ++rep) {
+        cudaEventRecord(ctx->ev2, ctx->stream);
+        dmma_peak_kernel<<<blocks, 256, 0, ctx->stream>>>(out, 1.0);
+        cudaEventRecord(ctx->ev3, ctx->stream);
+        cudaEventSynchronize(ctx->ev3);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ctx->ev2, ctx->ev3);
+        if (rep > 0 && ms < best) best = ms;
+    }
+    if (cudaGetLastError() != cudaSuccess) return -1.0;
+    const double flops = 2.0 * 16 * 8 * 4 * 8.0 * PEAK_ITERS * (double)blocks * 8 /* warps */;
+    return flops / (best * 1e-3) / 1e12;
+}
+
+}  // namespace db2

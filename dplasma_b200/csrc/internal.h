@@ -1,0 +1,120 @@
+// internal.h -- host-side internals of the library: the context object (one
+// GPU, one stream, grow-only device buffers, cached task lists) and the
+// functions the C ABI layer calls.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdarg.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include "../../include/dplasma_b200.h"
+
+namespace db2 {
+
+enum BufferId : int {
+    BUF_A = 0,        // device tiles of the factored matrix (lower, packed, padded)
+    BUF_STAGE,        // copy of the caller's matrix in its own layout
+    BUF_W,            // inverses of 128x128 diagonal blocks (factorization)
+    BUF_W2,           // inverses of 128x128 diagonal blocks (triangular solves)
+    BUF_COUNTERS,     // scheduler counters
+    BUF_TASKS,        // scheduler ticket order
+    BUF_B,            // right-hand sides, padded column-major
+    BUF_BSTAGE,       // copy of the caller's right-hand sides in its own layout
+    BUF_SOLVE_CTR,    // triangular-solve flags
+    BUF_NORM,         // reductions
+    BUF_TRACE,        // scheduler trace (opt-in)
+    BUF_COUNT
+};
+
+struct Context {
+    int device = 0;
+    int sms = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr, ev3 = nullptr;
+    int potrf_grid = 0;
+    int potrf_delay = 0;
+    int solve_grid = 0;
+    uint64_t dep_limit_ns = 4000000000ull;   // 4 s
+    uint64_t pipe_limit_ns = 4000000000ull;  // 4 s
+    bool self_check = false;
+    void *bufs[BUF_COUNT] = {};
+    size_t bufsz[BUF_COUNT] = {};
+    int task_mt = -1, task_nbs = -1, task_delay = -1, ntasks = 0;
+    double last_factor_ms = 0.0, last_solve_ms = 0.0;
+    int launches = 0;
+    long long last_tasks_executed = 0;
+    char errmsg[512] = {0};
+    char trace_path[512] = {0};   // DPLASMA_B200_TRACE: per-task timestamps of the scheduler
+
+    // grow-only device buffer; bytes == 0 returns the current one
+    void *buffer(int id, size_t bytes)
+    {
+        if (bytes == 0 || bytes <= bufsz[id]) return bufs[id];
+        if (bufs[id]) cudaFree(bufs[id]);
+        bufs[id] = nullptr;
+        bufsz[id] = 0;
+        if (cudaMalloc(&bufs[id], bytes) != cudaSuccess) {
+            cudaGetLastError();
+            set_error("cudaMalloc of %zu bytes failed (buffer %d)", bytes, id);
+            return nullptr;
+        }
+        bufsz[id] = bytes;
+        return bufs[id];
+    }
+    void set_error(const char *fmt, ...)
+    {
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(errmsg, sizeof(errmsg), fmt, ap);
+        va_end(ap);
+        fprintf(stderr, "dplasma_b200: %s\n", errmsg);
+    }
+};
+
+#define CK(call)                                                                                        \
+    do {                                                                                                \
+        cudaError_t e_ = (call);                                                                        \
+        if (e_ != cudaSuccess) {                                                                        \
+            ctx->set_error("%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+            return DPLASMA_ERR_UNEXPECTED;                                                              \
+        }                                                                                               \
+    } while (0)
+
+// Geometry of the device copy of an N x N symmetric matrix with caller tile nb.
+struct Geom {
+    int n, nb, nbi, mt;
+    size_t ntiles() const { return (size_t)mt * (mt + 1) / 2; }
+    size_t tile_elems() const { return (size_t)nbi * nbi; }
+    size_t elems() const { return ntiles() * tile_elems(); }
+};
+Geom make_geom(int n, int nb);
+
+// potrf_kernel.cu
+int potrf_device(Context *ctx, double *dA, int mt, int nbi, int nb_user, int n_user, int *info);
+
+// layout.cu : caller layout <-> device tiles
+int upload_sym(Context *ctx, const parsec_tiled_matrix_t *A, dplasma_enum_t uplo, const Geom &g, double *dA);
+int download_sym(Context *ctx, parsec_tiled_matrix_t *A, dplasma_enum_t uplo, const Geom &g, const double *dA);
+int upload_rhs(Context *ctx, const parsec_tiled_matrix_t *B, int nb, int nbi, int npad, int nrhs, double *dB);
+int download_rhs(Context *ctx, parsec_tiled_matrix_t *B, int nb, int nbi, int npad, int nrhs, const double *dB);
+int generate_plgsy(Context *ctx, double bump, dplasma_enum_t uplo, parsec_tiled_matrix_t *A, unsigned long long seed);
+int generate_plrnt(Context *ctx, int diagdom, parsec_tiled_matrix_t *A, unsigned long long seed);
+int64_t tile_offset(const parsec_tiled_matrix_t *A, int m, int n);
+size_t desc_elems(const parsec_tiled_matrix_t *A);
+
+// potrs_kernel.cu : triangular solves with the device tiles
+int trtri_diag(Context *ctx, const double *dA, const Geom &g, double *W, int unit_diag);
+int trsm_sweep(Context *ctx, const double *dA, const double *W, const Geom &g, double *dB, int ldb, int nrhs,
+               int transposed, double alpha);
+
+// norms.cu
+int lansy_inf_device(Context *ctx, const double *dA, const Geom &g, double *out);
+
+// peak.cu
+double fp64_peak_tflops(Context *ctx);
+
+}  // namespace db2
+
+struct parsec_context_s {
+    db2::Context impl;
+};

@@ -1,0 +1,633 @@
+// potrf_kernel.cu -- the persistent tile-Cholesky kernel (see potrf_kernel.cuh)
+// and its host-side launcher.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <algorithm>
+#include <vector>
+
+#include "internal.h"
+#include "potrf_kernel.cuh"
+#include "dev_trtri.cuh"
+
+namespace db2 {
+
+// First failure wins: record the status and where it happened.
+__device__ __forceinline__ void report(const PotrfArgs &a, int code, int site, int v0, int v1)
+{
+    if (atomicCAS(a.status, ST_OK, code) == ST_OK) {
+        a.diag[0] = site;
+        a.diag[1] = blockIdx.x;
+        a.diag[2] = v0;
+        a.diag[3] = v1;
+    }
+    atomicExch(a.abort_flag, 1);
+}
+
+// ---------------------------------------------------------------------------
+// dependencies of a task (dataflow of src/zpotrf_L.jdf:107-112, 229-237,
+// 364-368, 486-491, expressed as per-tile completion counts)
+// ---------------------------------------------------------------------------
+__device__ bool wait_deps(const PotrfArgs &a, uint64_t t)
+{
+    const int k = task_k(t), m = task_m(t), n = task_n(t);
+    const int nbs = a.nbs, nbd = nbs * (nbs + 1) / 2;
+    switch (task_type(t)) {
+    case T_POTRF:
+        return wait_geq(a.upd_done + (int64_t)k * a.mt + k, k * nbd, a.abort_flag, a.status, a.dep_limit_ns);
+    case T_TRSM:
+        return wait_geq(a.potrf_done + k, 1, a.abort_flag, a.status, a.dep_limit_ns) &&
+               wait_geq(a.upd_done + (int64_t)m * a.mt + k, k * nbs * nbs, a.abort_flag, a.status, a.dep_limit_ns);
+    case T_GEMM: {
+        const int nblk = (m == n) ? nbd : nbs * nbs;
+        return wait_geq(a.trsm_done + (int64_t)m * a.mt + k, nbs, a.abort_flag, a.status, a.dep_limit_ns) &&
+               wait_geq(a.trsm_done + (int64_t)n * a.mt + k, nbs, a.abort_flag, a.status, a.dep_limit_ns) &&
+               wait_geq(a.upd_done + (int64_t)m * a.mt + n, k * nblk, a.abort_flag, a.status, a.dep_limit_ns);
+    }
+    default:
+        atomicCAS(a.status, ST_OK, ST_BAD_TASK);
+        return false;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// producer warp
+// ---------------------------------------------------------------------------
+__device__ void producer_warp(const PotrfArgs &a, SmemCtl *ctl, double *ring)
+{
+    const int lane = threadIdx.x & 31;
+    uint32_t stage_it = 0, task_it = 0, epi_it = 0;
+    bool pipe_ok = true;
+    while (true) {
+        int tk = -1;
+        if (lane == 0) tk = ld_volatile(a.abort_flag) ? -1 : atomicAdd(a.ticket, 1);
+        tk = __shfl_sync(0xffffffffu, tk, 0);
+        bool end = (tk < 0 || tk >= a.ntasks);
+        uint64_t t = end ? 0 : a.tasks[tk];
+        int ok = 1;
+        if (!end && lane == 0) {
+            if (a.trace) a.trace[4 * (int64_t)tk + 0] = globaltimer_ns();
+            ok = wait_deps(a, t) ? 1 : 0;
+            if (a.trace) a.trace[4 * (int64_t)tk + 1] = globaltimer_ns();
+            if (!ok && ld_volatile(a.status) == ST_DEP_TIMEOUT && a.diag[0] == 0) {
+                a.diag[0] = 7;
+                a.diag[1] = blockIdx.x;
+                a.diag[2] = tk;
+                a.diag[3] = (int)(t & 0xFFFFFFFF);
+            }
+        }
+        ok = __shfl_sync(0xffffffffu, ok, 0);
+        if (!ok) end = true;
+
+        const uint32_t slot = task_it % TASKQ, round = task_it / TASKQ;
+        if (round > 0 && !warp_mbar_wait(&ctl->tempty[slot], (round - 1) & 1, a.pipe_limit_ns)) {
+            if (lane == 0) report(a, ST_MBAR_TIMEOUT, 1, task_it, tk);
+            pipe_ok = false;
+            break;
+        }
+        if (lane == 0) {
+            ctl->task[slot] = end ? (uint64_t)T_END : t;
+            ctl->tick[slot] = tk;
+            if (a.trace && end) a.trace_exit[6 * blockIdx.x + 3] = globaltimer_ns();
+            mbar_arrive(&ctl->tfull[slot]);
+        }
+        task_it++;
+        if (end) break;
+        if (task_type(t) == T_POTRF) {
+            // the consumers use the ring as scratch: wait until they are done
+            if (!warp_mbar_wait(&ctl->tempty[slot], round & 1, a.pipe_limit_ns)) {
+                if (lane == 0) report(a, ST_MBAR_TIMEOUT, 2, task_it, tk);
+                pipe_ok = false;
+                break;
+            }
+            if (a.trace && lane == 0) a.trace_exit[6 * blockIdx.x + 2] = globaltimer_ns();
+            continue;
+        }
+        fence_proxy_async();
+        const int nj = task_njobs(a, t);
+        bool prev_signal = false;
+        for (int j = 0; j < nj && pipe_ok; ++j) {
+            const Job jb = task_job(a, t, j);
+            if (prev_signal) {
+                if (!warp_mbar_wait(&ctl->epi, epi_it & 1, a.pipe_limit_ns)) {
+                    if (lane == 0) report(a, ST_MBAR_TIMEOUT, 3, epi_it, tk);
+                    pipe_ok = false;
+                    break;
+                }
+                epi_it++;
+                fence_proxy_async();
+            }
+            for (int k0 = 0; k0 < jb.K; k0 += BK) {
+                const uint32_t s = stage_it % NSTAGE, r = stage_it / NSTAGE;
+                if (r > 0 && !warp_mbar_wait(&ctl->empty[s], (r - 1) & 1, a.pipe_limit_ns)) {
+                    if (lane == 0) report(a, ST_MBAR_TIMEOUT, 4, stage_it, tk);
+                    pipe_ok = false;
+                    break;
+                }
+                double *As = ring + s * STAGE_DOUBLES;
+                double *Bs = As + BK * SP;
+                if (lane == 0) mbar_arrive_expect_tx(&ctl->full[s], 2 * BK * BLK * (uint32_t)sizeof(double));
+                __syncwarp();
+                if (lane < BK)
+                    bulk_g2s(As + lane * SP, jb.A + (int64_t)(k0 + lane) * jb.lda, BLK * sizeof(double),
+                             &ctl->full[s]);
+                else
+                    bulk_g2s(Bs + (lane - BK) * SP, jb.B + (int64_t)(k0 + lane - BK) * jb.ldb,
+                             BLK * sizeof(double), &ctl->full[s]);
+                stage_it++;
+            }
+            prev_signal = jb.signal;
+        }
+        if (!pipe_ok) break;
+    }
+    if (!pipe_ok) {
+        // Error path: tell the consumers to stop, then let the copies already
+        // issued land before the CTA can exit.
+        if (lane == 0) {
+            atomicExch(a.abort_flag, 1);
+        }
+        const uint32_t first = stage_it > NSTAGE ? stage_it - NSTAGE : 0;
+        for (uint32_t it = first; it < stage_it; ++it)
+            warp_mbar_wait(&ctl->full[it % NSTAGE], (it / NSTAGE) & 1, a.pipe_limit_ns);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// consumers: one 128x128 GEMM job
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool consume_job(const PotrfArgs &a, SmemCtl *ctl, const double *ring, const Job &jb,
+                                            uint32_t &stage_it)
+{
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int g = lane >> 2, t = lane & 3;
+    const int wm = warp & 1, wn = warp >> 1;
+    double acc[4][4][4];
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[mi][ni][q] = 0.0;
+
+    for (int k0 = 0; k0 < jb.K; k0 += BK) {
+        const uint32_t s = stage_it % NSTAGE, r = stage_it / NSTAGE;
+        if (!warp_mbar_wait(&ctl->full[s], r & 1, a.pipe_limit_ns)) {
+            if (threadIdx.x == 0) report(a, ST_MBAR_TIMEOUT, 6, stage_it, task_type(0));
+            return false;
+        }
+        const double *As = ring + s * STAGE_DOUBLES + wm * 64 + g;
+        const double *Bs = ring + s * STAGE_DOUBLES + BK * SP + wn * 32 + g;
+#pragma unroll
+        for (int kk = 0; kk < BK; kk += 4) {
+            double af[4][2], bf[4];
+            const int row = (kk + t) * SP;
+#pragma unroll
+            for (int mi = 0; mi < 4; ++mi) {
+                af[mi][0] = As[row + mi * 16];
+                af[mi][1] = As[row + mi * 16 + 8];
+            }
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni) bf[ni] = Bs[row + ni * 8];
+#pragma unroll
+            for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni) dmma_16x8x4(acc[mi][ni], af[mi][0], af[mi][1], bf[ni]);
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&ctl->empty[s]);
+        stage_it++;
+    }
+
+    // epilogue: straight to global (each warp writes 64x32; 64-byte runs)
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int r = wm * 64 + mi * 16 + g + ((q & 2) ? 8 : 0);
+                const int c = wn * 32 + ni * 8 + 2 * t + (q & 1);
+                double *p = jb.C + (int64_t)c * jb.ldc + r;
+                if (jb.mode == J_STORE) {
+                    *p = acc[mi][ni][q];
+                } else if (jb.mode == J_SUB || r >= c) {
+                    *p = __ldcg(p) - acc[mi][ni][q];
+                }
+            }
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// consumers: POTRF(k) of one diagonal tile + inverses of its 128x128 diagonal
+// blocks (src/zpotrf_L.jdf:194-206 computes the factor with
+// LAPACKE_dpotrf_work; the inverses feed the TRSM jobs).
+// Blocked right-looking with 32-column panels: one warp factors the 32x32
+// diagonal block with shuffles, all warps form the panel, the trailing
+// update runs on the FP64 tensor cores.
+// ---------------------------------------------------------------------------
+__device__ void potrf_task(const PotrfArgs &a, SmemCtl *ctl, double *ring, int k)
+{
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int g = lane >> 2, t = lane & 3;
+    const int nbi = a.nbi;
+    double *T = tile_ptr(a, k, k);
+    double *Wk = wblk_ptr(a, k, 0);
+    double *Ls = ring;               // 32 x 33, row-major
+    double *Dv = Ls + 32 * 33;       // 32 x 33, row-major: inverse of the 32x32 diagonal block
+    double *colb = Dv + 32 * 33;     // 32 (+pad)
+    double *Xs = colb + 64;          // panel X, [c][r] with pitch XP
+    double *Sw = colb + 64;          // W assembly staging (aliases Xs, used afterwards)
+    const int XP = nbi + 4;
+
+    for (int e = tid; e < a.nbs * BLK * BLK; e += NCONS) Wk[e] = 0.0;
+    if (tid == 0) ctl->fail = 0;
+    named_bar_sync(1, NCONS);
+
+    for (int p0 = 0; p0 < nbi; p0 += 32) {
+        // (a) 32x32 diagonal block: unblocked Cholesky, lane i owns row i
+        if (warp == 0) {
+            double d[32];
+#pragma unroll
+            for (int c = 0; c < 32; ++c) d[c] = (c <= lane) ? __ldcg(T + (int64_t)(p0 + c) * nbi + p0 + lane) : 0.0;
+            int failcol = -1;
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+                const double piv = __shfl_sync(0xffffffffu, d[j], j);
+                if (!(piv > 0.0)) {   // LAPACK dpotf2: ajj <= 0 or NaN stops the factorization
+                    failcol = j;
+                    break;
+                }
+                const double s = sqrt(piv);
+                const double rs = 1.0 / s;
+                const double lij = (lane == j) ? s : d[j] * rs;
+                if (lane >= j) d[j] = lij;
+                colb[lane] = lij;
+                __syncwarp();
+#pragma unroll
+                for (int c = j + 1; c < 32; ++c)
+                    if (lane >= c) d[c] -= lij * colb[c];
+                __syncwarp();
+            }
+            if (failcol >= 0) {
+                if (lane == 0) {
+                    ctl->fail = 1;
+                    const int col = p0 + failcol;   // tile-local column; padding follows the valid part
+                    if (col < a.nb_user && k * a.nb_user + col < a.n_user) atomicCAS(a.info, 0, k * a.nb_user + col + 1);
+                    atomicExch(a.abort_flag, 1);
+                }
+            } else {
+#pragma unroll
+                for (int c = 0; c < 32; ++c) {
+                    if (c <= lane) T[(int64_t)(p0 + c) * nbi + p0 + lane] = d[c];
+                    Ls[lane * 33 + c] = (c <= lane) ? d[c] : 0.0;
+                }
+                __syncwarp();
+                // inverse of the 32x32 lower block: lane c forms column c
+                const int b = p0 / BLK, q0 = p0 % BLK;
+                double *Wb = Wk + (int64_t)b * BLK * BLK;
+                invert32_lower(Ls, lane, 0, [&](int i, int c, double v) {
+                    Dv[i * 33 + c] = v;
+                    Wb[(int64_t)(q0 + c) * BLK + q0 + i] = v;
+                });
+            }
+        }
+        named_bar_sync(1, NCONS);
+        if (ctl->fail) return;
+
+        // (b) panel below the block: X = P * Dinv^T  (P = T[p0+32:, p0:p0+32])
+        const int R = nbi - p0 - 32;
+        for (int rr = tid; rr < R; rr += NCONS) {
+            const int r = p0 + 32 + rr;
+            double av[32];
+#pragma unroll
+            for (int l = 0; l < 32; ++l) av[l] = __ldcg(T + (int64_t)(p0 + l) * nbi + r);
+#pragma unroll
+            for (int c = 0; c < 32; ++c) {
+                double x = 0.0;
+#pragma unroll
+                for (int l = 0; l <= c; ++l) x += av[l] * Dv[c * 33 + l];
+                T[(int64_t)(p0 + c) * nbi + r] = x;
+                Xs[c * XP + rr] = x;
+            }
+        }
+        named_bar_sync(1, NCONS);
+
+        // (c) trailing update of the lower part: T22 -= X X^T (DMMA, 32x32 blocks)
+        const int nb32 = R / 32;
+        const int nitems = nb32 * (nb32 + 1) / 2;
+        for (int it = warp; it < nitems; it += NCONS / 32) {
+            int bi = (int)((sqrtf(8.0f * it + 1.0f) - 1.0f) * 0.5f);
+            while ((bi + 1) * (bi + 2) / 2 <= it) ++bi;
+            while (bi * (bi + 1) / 2 > it) --bi;
+            const int bj = it - bi * (bi + 1) / 2;
+            double acc[2][4][4];
+#pragma unroll
+            for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) acc[mi][ni][q] = 0.0;
+#pragma unroll
+            for (int kk = 0; kk < 32; kk += 4) {
+                const double *xr = Xs + (kk + t) * XP;
+                double af[2][2], bf[4];
+#pragma unroll
+                for (int mi = 0; mi < 2; ++mi) {
+                    af[mi][0] = xr[bi * 32 + mi * 16 + g];
+                    af[mi][1] = xr[bi * 32 + mi * 16 + g + 8];
+                }
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni) bf[ni] = xr[bj * 32 + ni * 8 + g];
+#pragma unroll
+                for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                    for (int ni = 0; ni < 4; ++ni) dmma_16x8x4(acc[mi][ni], af[mi][0], af[mi][1], bf[ni]);
+            }
+#pragma unroll
+            for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int r = p0 + 32 + bi * 32 + mi * 16 + g + ((q & 2) ? 8 : 0);
+                        const int c = p0 + 32 + bj * 32 + ni * 8 + 2 * t + (q & 1);
+                        if (r >= c) {
+                            double *p = T + (int64_t)c * nbi + r;
+                            *p = __ldcg(p) - acc[mi][ni][q];
+                        }
+                    }
+        }
+        named_bar_sync(1, NCONS);
+    }
+
+    // Inverses of the 128x128 diagonal blocks from the 32x32 ones.
+    assemble_w128(T, nbi, Wk, a.nbs, Sw, warp, lane, NCONS / 32, 1, NCONS);
+}
+
+// ---------------------------------------------------------------------------
+// consumers: task loop
+// ---------------------------------------------------------------------------
+__device__ void consumer_warps(const PotrfArgs &a, SmemCtl *ctl, double *ring)
+{
+    const int tid = threadIdx.x;
+    uint32_t stage_it = 0, task_it = 0;
+    int executed = 0;
+    while (true) {
+        const uint32_t slot = task_it % TASKQ, round = task_it / TASKQ;
+        if (!warp_mbar_wait(&ctl->tfull[slot], round & 1, a.pipe_limit_ns)) {
+            if (tid == 0) report(a, ST_MBAR_TIMEOUT, 5, task_it, stage_it);
+            break;
+        }
+        const uint64_t t = ctl->task[slot];
+        const int tk = ctl->tick[slot];
+        task_it++;
+        const int ty = task_type(t);
+        if (ty == T_END) {
+            if (a.trace && tid == 0) a.trace_exit[6 * blockIdx.x + 4] = globaltimer_ns();
+            break;
+        }
+        if (a.trace && tid == 0) a.trace[4 * (int64_t)tk + 2] = globaltimer_ns();
+        const int k = task_k(t), m = task_m(t), n = task_n(t);
+        int *release = nullptr;
+        bool ok = true;
+        if (ty == T_POTRF) {
+            potrf_task(a, ctl, ring, k);
+            if (!ctl->fail) release = a.potrf_done + k;
+        } else {
+            const int nj = task_njobs(a, t);
+            for (int j = 0; j < nj && ok; ++j) {
+                const Job jb = task_job(a, t, j);
+                ok = consume_job(a, ctl, ring, jb, stage_it);
+                if (ok && jb.signal) {
+                    fence_proxy_async();
+                    named_bar_sync(1, NCONS);
+                    if (tid == 0) mbar_arrive(&ctl->epi);
+                }
+            }
+            release = (ty == T_TRSM) ? a.trsm_done + (int64_t)m * a.mt + k : a.upd_done + (int64_t)m * a.mt + n;
+        }
+        if (!ok) {
+            atomicExch(a.abort_flag, 1);
+            break;
+        }
+        fence_proxy_async();
+        named_bar_sync(1, NCONS);
+        if (tid == 0) {
+            if (release) {
+                __threadfence();
+                red_release_add(release, 1);
+            }
+            if (a.trace) {
+                a.trace[4 * (int64_t)tk + 3] = globaltimer_ns();
+                a.trace_cta[tk] = blockIdx.x;
+            }
+            mbar_arrive(&ctl->tempty[slot]);
+        }
+        executed++;
+    }
+    if (tid == 0 && a.task_count) a.task_count[blockIdx.x] = executed;
+    if (tid == 0 && a.trace) a.trace_exit[6 * blockIdx.x + 1] = globaltimer_ns();
+}
+
+__global__ void __launch_bounds__(NTHREADS, 1) potrf_persistent_kernel(PotrfArgs a)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    SmemCtl *ctl = reinterpret_cast<SmemCtl *>(smem_raw);
+    double *ring = reinterpret_cast<double *>(smem_raw + ((sizeof(SmemCtl) + 127) / 128) * 128);
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < NSTAGE; ++s) {
+            mbar_init(&ctl->full[s], 1);
+            mbar_init(&ctl->empty[s], NCONS / 32);
+        }
+        for (int s = 0; s < TASKQ; ++s) {
+            mbar_init(&ctl->tfull[s], 1);
+            mbar_init(&ctl->tempty[s], 1);
+        }
+        mbar_init(&ctl->epi, 1);
+        ctl->fail = 0;
+    }
+    __syncthreads();
+    if (threadIdx.x >= NCONS) {
+        producer_warp(a, ctl, ring);
+        if (a.trace && threadIdx.x == NCONS) a.trace_exit[6 * blockIdx.x] = globaltimer_ns();
+    } else {
+        consumer_warps(a, ctl, ring);
+    }
+}
+
+size_t potrf_smem_bytes()
+{
+    return ((sizeof(SmemCtl) + 127) / 128) * 128 + (size_t)NSTAGE * STAGE_DOUBLES * sizeof(double);
+}
+
+// ---------------------------------------------------------------------------
+// host: ticket order
+// ---------------------------------------------------------------------------
+// POTRF(0), TRSM(*,0); then for each step k: the update of column k+1
+// (critical path), POTRF(k+1), `delay` tasks of the remaining step-k update,
+// TRSM(*,k+1), the rest of the step-k update by increasing column.  Every
+// task's dependencies precede it, so CTAs that take tickets in order always
+// make progress (no co-residency assumption).
+std::vector<uint64_t> build_potrf_tasks(int mt, int nbs, int delay)
+{
+    std::vector<uint64_t> v;
+    auto push_update_tile = [&](int m, int n, int k) {
+        for (int bi = 0; bi < nbs; ++bi)
+            for (int bj = 0; bj < nbs; ++bj) {
+                if (m == n && bj > bi) continue;
+                v.push_back(make_task(T_GEMM, k, m, n, bi, bj));
+            }
+    };
+    auto push_trsm = [&](int k) {
+        for (int m = k + 1; m < mt; ++m)
+            for (int bi = 0; bi < nbs; ++bi) v.push_back(make_task(T_TRSM, k, m, k, bi, 0));
+    };
+    v.push_back(make_task(T_POTRF, 0, 0, 0, 0, 0));
+    push_trsm(0);
+    std::vector<uint64_t> rest;
+    for (int k = 0; k + 1 < mt; ++k) {
+        for (int m = k + 1; m < mt; ++m) push_update_tile(m, k + 1, k);
+        v.push_back(make_task(T_POTRF, k + 1, k + 1, k + 1, 0, 0));
+        rest.clear();
+        for (int n = k + 2; n < mt; ++n)
+            for (int m = n; m < mt; ++m)
+                for (int bi = 0; bi < nbs; ++bi)
+                    for (int bj = 0; bj < nbs; ++bj) {
+                        if (m == n && bj > bi) continue;
+                        rest.push_back(make_task(T_GEMM, k, m, n, bi, bj));
+                    }
+        const size_t d = std::min<size_t>(rest.size(), (size_t)std::max(delay, 0));
+        v.insert(v.end(), rest.begin(), rest.begin() + d);
+        push_trsm(k + 1);
+        v.insert(v.end(), rest.begin() + d, rest.end());
+    }
+    return v;
+}
+
+// ---------------------------------------------------------------------------
+// host: run one factorization of the device tiles
+// ---------------------------------------------------------------------------
+int potrf_device(Context *ctx, double *dA, int mt, int nbi, int nb_user, int n_user, int *info)
+{
+    const int nbs = nbi / BLK;
+    cudaStream_t st = ctx->stream;
+    const int grid = ctx->potrf_grid;
+    // task list (cached per shape)
+    if (ctx->task_mt != mt || ctx->task_nbs != nbs || ctx->task_delay != ctx->potrf_delay) {
+        std::vector<uint64_t> tasks = build_potrf_tasks(mt, nbs, ctx->potrf_delay);
+        uint64_t *dt = (uint64_t *)ctx->buffer(BUF_TASKS, tasks.size() * sizeof(uint64_t));
+        if (!dt) return DPLASMA_ERR_OUT_OF_RESOURCES;
+        CK(cudaMemcpyAsync(dt, tasks.data(), tasks.size() * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+        ctx->task_mt = mt;
+        ctx->task_nbs = nbs;
+        ctx->task_delay = ctx->potrf_delay;
+        ctx->ntasks = (int)tasks.size();
+    }
+    double *W = (double *)ctx->buffer(BUF_W, (size_t)mt * nbs * BLK * BLK * sizeof(double));
+    const size_t nctr = 8 + (size_t)mt + 2 * (size_t)mt * mt + grid;
+    int *ctr = (int *)ctx->buffer(BUF_COUNTERS, nctr * sizeof(int));
+    if (!W || !ctr) return DPLASMA_ERR_OUT_OF_RESOURCES;
+    CK(cudaMemsetAsync(ctr, 0, nctr * sizeof(int), st));
+
+    PotrfArgs a;
+    a.A = dA;
+    a.W = W;
+    a.tasks = (const uint64_t *)ctx->buffer(BUF_TASKS, 0);
+    a.ntasks = ctx->ntasks;
+    a.mt = mt;
+    a.nbi = nbi;
+    a.nbs = nbs;
+    a.nb_user = nb_user;
+    a.n_user = n_user;
+    a.ticket = ctr + 0;
+    a.info = ctr + 1;
+    a.abort_flag = ctr + 2;
+    a.status = ctr + 3;
+    a.potrf_done = ctr + 8;
+    a.trsm_done = a.potrf_done + mt;
+    a.upd_done = a.trsm_done + (size_t)mt * mt;
+    a.task_count = a.upd_done + (size_t)mt * mt;
+    a.diag = ctr + 4;
+    a.trace = nullptr;
+    if (ctx->trace_path[0]) {
+        const size_t tbytes = ((size_t)a.ntasks * 4 + 6 * (size_t)grid) * sizeof(unsigned long long) + (size_t)a.ntasks * sizeof(int);
+        a.trace = (unsigned long long *)ctx->buffer(BUF_TRACE, tbytes);
+        if (!a.trace) return DPLASMA_ERR_OUT_OF_RESOURCES;
+        a.trace_exit = a.trace + (size_t)a.ntasks * 4;
+        a.trace_cta = (int *)(a.trace_exit + 6 * (size_t)grid);
+        CK(cudaMemsetAsync(a.trace, 0, tbytes, st));
+    }
+    a.dep_limit_ns = ctx->dep_limit_ns;
+    a.pipe_limit_ns = ctx->pipe_limit_ns;
+
+    const size_t smem = potrf_smem_bytes();
+    CK(cudaFuncSetAttribute(potrf_persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CK(cudaEventRecord(ctx->ev0, st));
+    potrf_persistent_kernel<<<grid, NTHREADS, smem, st>>>(a);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(ctx->ev1, st));
+    ctx->launches += 1;
+    int hs[8];
+    CK(cudaMemcpyAsync(hs, ctr, 8 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    ctx->last_factor_ms = ms;
+    if (hs[3] != ST_OK) {
+        ctx->set_error("potrf scheduler status %d (1: dependency wait timed out, 2: pipeline wait timed out); "
+                       "site %d cta %d values %d %d; tickets taken %d of %d",
+                       hs[3], hs[4], hs[5], hs[6], hs[7], hs[0], ctx->ntasks);
+        return DPLASMA_ERR_UNEXPECTED;
+    }
+    if (ctx->self_check) {
+        std::vector<int> cnt(grid);
+        CK(cudaMemcpy(cnt.data(), a.task_count, grid * sizeof(int), cudaMemcpyDeviceToHost));
+        long long tot = 0;
+        for (int c : cnt) tot += c;
+        ctx->last_tasks_executed = tot;
+    }
+    if (a.trace) {
+        // one line per ticket: type k m n bi bj fetched deps_met started finished cta (ns, relative)
+        std::vector<unsigned long long> tr((size_t)a.ntasks * 4), tx(6 * (size_t)grid);
+        std::vector<int> tc(a.ntasks);
+        std::vector<uint64_t> tl(a.ntasks);
+        CK(cudaMemcpy(tr.data(), a.trace, tr.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(tx.data(), a.trace_exit, tx.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(tc.data(), a.trace_cta, tc.size() * sizeof(int), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(tl.data(), a.tasks, tl.size() * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+        unsigned long long t0 = ~0ull;
+        for (int i = 0; i < a.ntasks; ++i)
+            if (tr[4 * i] && tr[4 * i] < t0) t0 = tr[4 * i];
+        FILE *f = fopen(ctx->trace_path, "w");
+        if (f) {
+            fprintf(f, "ticket type k m n bi bj fetched deps_met started finished cta\n");
+            auto rel = [&](unsigned long long v) { return v ? (long long)(v - t0) : -1ll; };
+            for (int i = 0; i < a.ntasks; ++i) {
+                const uint64_t t = tl[i];
+                fprintf(f, "%d %d %d %d %d %d %d %lld %lld %lld %lld %d\n", i, task_type(t), task_k(t), task_m(t),
+                        task_n(t), task_bi(t), task_bj(t), rel(tr[4 * i]), rel(tr[4 * i + 1]), rel(tr[4 * i + 2]),
+                        rel(tr[4 * i + 3]), tc[i]);
+            }
+            for (int c = 0; c < grid; ++c)
+                fprintf(f, "# cta %d producer_exit %lld consumer_exit %lld potrf_wait_done %lld end_pushed %lld end_seen %lld\n", c,
+                        rel(tx[6 * c]), rel(tx[6 * c + 1]), rel(tx[6 * c + 2]), rel(tx[6 * c + 3]), rel(tx[6 * c + 4]));
+            fclose(f);
+        }
+    }
+    *info = hs[1];
+    return 0;
+}
+
+}  // namespace db2
+
+namespace db2 {
+int potrf_max_blocks_per_sm()
+{
+    const size_t smem = potrf_smem_bytes();
+    if (cudaFuncSetAttribute(potrf_persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+        return 0;
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, potrf_persistent_kernel, NTHREADS, smem) != cudaSuccess) return 0;
+    return n;
+}
+}  // namespace db2

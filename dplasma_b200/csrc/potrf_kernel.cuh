@@ -1,0 +1,161 @@
+// potrf_kernel.cuh -- persistent, dependency-counted tile Cholesky (lower) on
+// sm_100a with FP64 tensor cores.
+//
+// The tile DAG of dplasma's src/zpotrf_L.jdf (POTRF(k) -> TRSM(m,k) ->
+// SYRK(k,m) / GEMM(m,n,k)) is executed by one resident CTA per SM.  Each CTA
+// pulls task tickets from a global counter in a precomputed topological order
+// (critical path first, one step of look-ahead), waits on per-tile completion
+// counters (bounded waits), and runs the task:
+//
+//   warp 8  (producer): fetches tickets, waits for the task's dependencies,
+//            streams operand columns into a shared-memory ring with bulk
+//            copies (cp.async.bulk, the TMA engine) completing on mbarriers;
+//   warps 0-7 (consumers): FP64 DMMA (mma.sync m16n8k4 .f64) on 128x128
+//            output blocks, epilogue straight to global memory, then release
+//            the completion counter.
+//
+// Device layout: lower triangle of nbi x nbi tiles, packed by columns
+// (db2::lower_tile_index), nbi a multiple of 128.  A ragged last tile is
+// padded with the identity, which leaves the factor of the valid part
+// unchanged.
+//
+// TRSM(m,k) uses the inverses of the 128x128 diagonal blocks of L(k,k),
+// computed by POTRF(k) into the workspace W: the strip X = A(m,k) L(k,k)^{-T}
+// is solved block-left-looking as GEMM jobs (X_p = (A_p - sum_q X_q L_pq^T)
+// W_pp^T), so all FP64 flops of the path run on the tensor cores except the
+// 32x32 diagonal factorizations.
+#pragma once
+#include "dev_common.cuh"
+
+namespace db2 {
+
+constexpr int BLK = 128;         // output block edge handled by one CTA job
+constexpr int BK = 16;           // K depth of one pipeline stage
+constexpr int SP = BLK + 4;      // shared pitch (doubles) of an operand row, = 4 mod 16
+constexpr int NSTAGE = 5;        // pipeline stages
+constexpr int NCONS = 256;       // consumer threads (8 warps)
+constexpr int NTHREADS = NCONS + 32;
+constexpr int TASKQ = 4;         // task ring depth
+constexpr int STAGE_DOUBLES = 2 * BK * SP;
+
+// Task encoding (64 bits): type[0:4) k[4:20) m[20:36) n[36:52) bi[52:56) bj[56:60)
+enum : int { T_END = 0, T_POTRF = 1, T_TRSM = 2, T_GEMM = 3 };
+__host__ __device__ __forceinline__ uint64_t make_task(int type, int k, int m, int n, int bi, int bj)
+{
+    return (uint64_t)type | ((uint64_t)k << 4) | ((uint64_t)m << 20) | ((uint64_t)n << 36) |
+           ((uint64_t)bi << 52) | ((uint64_t)bj << 56);
+}
+__host__ __device__ __forceinline__ int task_type(uint64_t t) { return (int)(t & 0xF); }
+__host__ __device__ __forceinline__ int task_k(uint64_t t) { return (int)((t >> 4) & 0xFFFF); }
+__host__ __device__ __forceinline__ int task_m(uint64_t t) { return (int)((t >> 20) & 0xFFFF); }
+__host__ __device__ __forceinline__ int task_n(uint64_t t) { return (int)((t >> 36) & 0xFFFF); }
+__host__ __device__ __forceinline__ int task_bi(uint64_t t) { return (int)((t >> 52) & 0xF); }
+__host__ __device__ __forceinline__ int task_bj(uint64_t t) { return (int)((t >> 56) & 0xF); }
+
+struct PotrfArgs {
+    double *A;             // device tiles (lower, packed)
+    double *W;             // mt * nbs blocks of 128x128: inverses of diagonal blocks
+    const uint64_t *tasks; // ticket order
+    int ntasks;
+    int mt, nbi, nbs;      // tiles per side, tile edge, 128-blocks per tile edge
+    int nb_user;           // caller's tile size (INFO numbering)
+    int n_user;            // caller's matrix order
+    int *ticket;           // next ticket
+    int *potrf_done;       // [mt]
+    int *trsm_done;        // [mt*mt]: strips done for tile (m,k)
+    int *upd_done;         // [mt*mt]: update blocks done on tile (m,n)
+    int *info;             // first failing minor (1-based), 0 if none
+    int *abort_flag;       // set on failure: stop fetching tasks
+    int *status;           // ST_* error word
+    int *task_count;       // per-CTA executed-task counters (self check), may be null
+    int *diag;             // [4]: where the first failed wait gave up (site, CTA, two values)
+    unsigned long long *trace; // opt-in, 4 per ticket: fetched, dependencies met, started, finished (ns); may be null
+    unsigned long long *trace_exit; // 2 per CTA: producer and consumer exit times
+    int *trace_cta;        // CTA that ran each ticket
+    uint64_t dep_limit_ns; // bounded dependency waits
+    uint64_t pipe_limit_ns;// bounded pipeline waits
+};
+
+__device__ __forceinline__ double *tile_ptr(const PotrfArgs &a, int m, int n)
+{
+    return a.A + lower_tile_index(m, n, a.mt) * (int64_t)a.nbi * a.nbi;
+}
+__device__ __forceinline__ double *wblk_ptr(const PotrfArgs &a, int k, int b)
+{
+    return a.W + ((int64_t)k * a.nbs + b) * (BLK * BLK);
+}
+
+// One GEMM job: C(128x128) {-=, =} A(128 x K) * B(128 x K)^T.  A and B are
+// given by their first element and column stride; every column segment of
+// 128 doubles is contiguous (1 KB), which is what the bulk copies move.
+enum : int { J_SUB = 0, J_SUB_LOWER = 1, J_STORE = 2 };
+struct Job {
+    const double *A;
+    const double *B;
+    double *C;
+    int lda, ldb, ldc;
+    int K;
+    int mode;
+    bool signal;   // the next job of the same task reads this job's output
+};
+
+// The job sequence of a task (identical on producer and consumer sides).
+__device__ __forceinline__ int task_njobs(const PotrfArgs &a, uint64_t t)
+{
+    int ty = task_type(t);
+    if (ty == T_GEMM) return 1;
+    if (ty == T_TRSM) return 2 * a.nbs - 1;
+    return 0;
+}
+__device__ __forceinline__ Job task_job(const PotrfArgs &a, uint64_t t, int j)
+{
+    Job jb;
+    const int nbi = a.nbi;
+    const int k = task_k(t), m = task_m(t), n = task_n(t), bi = task_bi(t), bj = task_bj(t);
+    if (task_type(t) == T_GEMM) {
+        // C(m,n)[bi,bj] -= A(m,k)[bi,:] * A(n,k)[bj,:]^T     (src/zpotrf_L.jdf:619-623, :453-456)
+        jb.A = tile_ptr(a, m, k) + bi * BLK;
+        jb.B = tile_ptr(a, n, k) + bj * BLK;
+        jb.C = tile_ptr(a, m, n) + (int64_t)bj * BLK * nbi + bi * BLK;
+        jb.lda = nbi; jb.ldb = nbi; jb.ldc = nbi;
+        jb.K = nbi;
+        jb.mode = (m == n && bi == bj) ? J_SUB_LOWER : J_SUB;
+        jb.signal = false;
+    } else {
+        // TRSM strip bi of tile (m,k): X = A L^{-T} (src/zpotrf_L.jdf:330-333),
+        // block-left-looking: jobs  [STORE p=0] [SUB p=1] [STORE p=1] ...
+        const int p = (j + 1) / 2;
+        const bool store = (j % 2) == 0;
+        double *Amk = tile_ptr(a, m, k);
+        double *Cp = Amk + (int64_t)p * BLK * nbi + bi * BLK;
+        if (store) {
+            jb.A = Cp; jb.lda = nbi;
+            jb.B = wblk_ptr(a, k, p); jb.ldb = BLK;
+            jb.K = BLK;
+            jb.mode = J_STORE;
+            jb.signal = (p < a.nbs - 1);
+        } else {
+            jb.A = Amk + bi * BLK; jb.lda = nbi;                    // X_0..X_{p-1}
+            jb.B = tile_ptr(a, k, k) + p * BLK; jb.ldb = nbi;        // L(k,k)[p, 0:p]
+            jb.K = p * BLK;
+            jb.mode = J_SUB;
+            jb.signal = true;
+        }
+        jb.C = Cp; jb.ldc = nbi;
+    }
+    return jb;
+}
+
+struct __align__(16) SmemCtl {
+    uint64_t full[NSTAGE];
+    uint64_t empty[NSTAGE];
+    uint64_t tfull[TASKQ];
+    uint64_t tempty[TASKQ];
+    uint64_t epi;
+    uint64_t task[TASKQ];
+    int tick[TASKQ];
+    int fail;
+    int pad[3];
+};
+
+}  // namespace db2

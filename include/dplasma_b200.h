@@ -1,0 +1,208 @@
+/*
+ * dplasma_b200.h -- C ABI of the B200-native tile Cholesky library.
+ *
+ * A drop-in for DPLASMA's Cholesky factor-and-solve path on a 1x1 process
+ * grid: the entry points below keep the names, argument meaning, enum values
+ * and return conventions of the dplasma C API they replace (each is cited
+ * with the reference file:line it mirrors; paths are relative to the dplasma
+ * source tree).  Signatures use only plain C types and pointers.
+ *
+ * Matrices are described by a parsec_tiled_matrix_t-shaped descriptor (the
+ * reference type lives in PaRSEC; its field names and the meaning of each are
+ * kept, the struct layout is this library's own).  `mat` points either to
+ * host memory (the default, as in the reference, where the caller allocates
+ * and owns it) or, when `location == DPLASMA_B200_DEVICE`, to device memory
+ * on the context's GPU.  Calls are blocking and in place: results are in
+ * `mat` when they return.
+ */
+#ifndef DPLASMA_B200_H
+#define DPLASMA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- constants: src/include/dplasma/constants.h:32-42, 47, 78-99 -------- */
+#define DPLASMA_SUCCESS                 0
+#define DPLASMA_ERR_NOT_INITIALIZED  -101
+#define DPLASMA_ERR_REINITIALIZED    -102
+#define DPLASMA_ERR_NOT_SUPPORTED    -103
+#define DPLASMA_ERR_ILLEGAL_VALUE    -104
+#define DPLASMA_ERR_NOT_FOUND        -105
+#define DPLASMA_ERR_OUT_OF_RESOURCES -106
+#define DPLASMA_ERR_INTERNAL_LIMIT   -107
+#define DPLASMA_ERR_UNALLOCATED      -108
+#define DPLASMA_ERR_FILESYSTEM       -109
+#define DPLASMA_ERR_UNEXPECTED       -110
+#define DPLASMA_ERR_SEQUENCE_FLUSHED -111
+
+typedef int dplasma_enum_t;
+
+#define dplasmaNoTrans       111
+#define dplasmaTrans         112
+#define dplasmaConjTrans     113
+#define dplasmaUpper         121
+#define dplasmaLower         122
+#define dplasmaUpperLower    123
+#define dplasmaNonUnit       131
+#define dplasmaUnit          132
+#define dplasmaLeft          141
+#define dplasmaRight         142
+#define dplasmaOneNorm       171
+#define dplasmaFrobeniusNorm 174
+#define dplasmaInfNorm       175
+#define dplasmaMaxNorm       177
+
+/* ---- matrix descriptor -------------------------------------------------- */
+/* Element types (the PaRSEC matrix-type enumeration: byte, int, float,
+ * double, complex float, complex double).  Only DOUBLE is on this path. */
+#define PARSEC_MATRIX_BYTE           0
+#define PARSEC_MATRIX_INTEGER        1
+#define PARSEC_MATRIX_FLOAT          2
+#define PARSEC_MATRIX_DOUBLE         3
+#define PARSEC_MATRIX_COMPLEX_FLOAT  4
+#define PARSEC_MATRIX_COMPLEX_DOUBLE 5
+
+/* Storage kinds (src/utils/dplasma_lapack_adtt.h:29-31 names them TILED and
+ * LAPACK).  TILE: every tile is a contiguous mb*nb column-major block with
+ * leading dimension mb, the last tile row/column padded to full size.
+ * LAPACK: one column-major array with leading dimension `lda`. */
+#define PARSEC_MATRIX_LAPACK 0
+#define PARSEC_MATRIX_TILE   1
+
+/* Where `mat` lives. */
+#define DPLASMA_B200_HOST   0
+#define DPLASMA_B200_DEVICE 1
+
+typedef struct parsec_tiled_matrix_s {
+    int mtype;            /* PARSEC_MATRIX_DOUBLE                                    */
+    int storage;          /* PARSEC_MATRIX_TILE or PARSEC_MATRIX_LAPACK              */
+    int uplo;             /* tiles held in TILE storage: dplasmaUpperLower (whole
+                             grid), dplasmaLower / dplasmaUpper (symmetric storage,
+                             only that triangle of tiles)                            */
+    int mb, nb;           /* tile size                                               */
+    int lm, ln;           /* size of the allocated matrix                            */
+    int i, j;             /* first row/column of this (sub)matrix: 0 only            */
+    int m, n;             /* size of the matrix                                      */
+    int mt, nt;           /* tile rows / columns of the matrix                       */
+    int lmt, lnt;         /* tile rows / columns of the allocation                   */
+    int lda;              /* leading dimension (LAPACK storage)                      */
+    int location;         /* DPLASMA_B200_HOST or DPLASMA_B200_DEVICE                */
+    size_t bsiz;          /* elements per tile (mb*nb)                               */
+    size_t nb_local_tiles;/* tiles in the allocation                                 */
+    void *mat;            /* caller-owned data                                       */
+} parsec_tiled_matrix_t;
+
+/* Tile (m,n) of a TILE-storage descriptor starts at element
+ * dplasma_b200_tile_offset(A, m, n) of `mat`:
+ *   uplo == dplasmaUpperLower: tiles column-major over the lmt x lnt grid,
+ *                              offset = (m + n*lmt) * bsiz;
+ *   uplo == dplasmaLower:      only m >= n tiles, packed column by column,
+ *                              offset = (n*lmt - n*(n-1)/2 + (m-n)) * bsiz;
+ *   uplo == dplasmaUpper:      only m <= n tiles, packed column by column,
+ *                              offset = (n*(n+1)/2 + m) * bsiz.
+ * For LAPACK storage it is m*mb + n*nb*lda.  Returns -1 for a tile outside
+ * the stored triangle. */
+int64_t dplasma_b200_tile_offset(const parsec_tiled_matrix_t *A, int m, int n);
+
+/* Fill a descriptor for a general (two-dimensional block-cyclic, 1x1 grid)
+ * matrix; mirrors parsec_matrix_block_cyclic_init's size arguments
+ * (as called in tests/testing_zposv.c:40-51).  `mat` is left NULL; the
+ * number of elements to allocate is bsiz * nb_local_tiles (TILE) or
+ * lda * n (LAPACK). */
+void dplasma_b200_desc_init(parsec_tiled_matrix_t *A, int mtype, int storage,
+                            int mb, int nb, int lm, int ln, int i, int j, int m, int n);
+/* Same for symmetric TILE storage of one triangle of tiles; mirrors
+ * parsec_matrix_sym_block_cyclic_init (tests/testing_zpotrf.c:42-45). */
+void dplasma_b200_sym_desc_init(parsec_tiled_matrix_t *A, int mtype, int mb, int nb,
+                                int lm, int ln, int i, int j, int m, int n, dplasma_enum_t uplo);
+
+/* ---- context ------------------------------------------------------------ */
+/* Replaces the parsec_context_t the dplasma calls take (created by
+ * parsec_init, tests/common.c:684).  One context owns one GPU, a CUDA stream
+ * and the device workspace; it is used from one host thread at a time. */
+typedef struct parsec_context_s parsec_context_t;
+typedef struct parsec_taskpool_s parsec_taskpool_t;
+
+parsec_context_t *dplasma_b200_init(int device);
+void dplasma_b200_fini(parsec_context_t **ctx);
+/* Last error message of this context (empty when none). */
+const char *dplasma_b200_last_error(const parsec_context_t *ctx);
+
+/* ---- the Cholesky path -------------------------------------------------- */
+/* dplasma_dpotrf: src/zpotrf_wrapper.c:345-371 (declared at
+ * src/include/dplasma/dplasma_z.h:82).  Returns 0, -1 for a bad uplo, or
+ * i > 0 when the leading minor of order i is not positive definite
+ * (k*NB + iinfo, src/zpotrf_L.jdf:200-202). */
+int dplasma_dpotrf(parsec_context_t *parsec, dplasma_enum_t uplo, parsec_tiled_matrix_t *A);
+
+/* dplasma_dpotrf_New / _Destruct: src/zpotrf_wrapper.c:193-258, 280-297
+ * (dplasma_z.h:172, 239).  New returns NULL on a bad uplo; the factorization
+ * runs when the taskpool is executed by dplasma_b200_taskpool_run (the
+ * analogue of parsec_context_add_taskpool + dplasma_wait_until_completion),
+ * and *info receives the INFO value. */
+parsec_taskpool_t *dplasma_dpotrf_New(dplasma_enum_t uplo, parsec_tiled_matrix_t *A, int *info);
+void dplasma_dpotrf_Destruct(parsec_taskpool_t *tp);
+int dplasma_b200_taskpool_run(parsec_context_t *parsec, parsec_taskpool_t *tp);
+
+/* dplasma_dpotrf_rec / _setrecursive: src/zpotrf_wrapper.c:425-451
+ * (dplasma_z.h:83, 273).  The hierarchical split of the reference is subsumed
+ * by the device scheduler; hmb is validated and otherwise ignored. */
+int dplasma_dpotrf_rec(parsec_context_t *parsec, dplasma_enum_t uplo, parsec_tiled_matrix_t *A, int hmb);
+void dplasma_dpotrf_setrecursive(parsec_taskpool_t *tp, int hmb);
+
+/* dplasma_dpotrs: src/zpotrs_wrapper.c:56-97 (dplasma_z.h:84).  A holds the
+ * factor from dplasma_dpotrf, B (N x NRHS) is overwritten by the solution.
+ * Returns 0 or -1 for a bad uplo. */
+int dplasma_dpotrs(parsec_context_t *parsec, dplasma_enum_t uplo, const parsec_tiled_matrix_t *A,
+                   parsec_tiled_matrix_t *B);
+
+/* dplasma_dposv: src/zposv_wrapper.c:63-113 (dplasma_z.h:81).  Factor, then
+ * solve when INFO == 0; returns INFO. */
+int dplasma_dposv(parsec_context_t *parsec, dplasma_enum_t uplo, parsec_tiled_matrix_t *A,
+                  parsec_tiled_matrix_t *B);
+
+/* dplasma_dtrsm: src/ztrsm_wrapper.c:263-309 (dplasma_z.h:51).  Left side
+ * only (the four sweeps src/ztrsm_L{LN,LT,UN,UT}.jdf); side == dplasmaRight
+ * returns DPLASMA_ERR_NOT_SUPPORTED.  -1..-4 bad enums, -6 bad shapes. */
+int dplasma_dtrsm(parsec_context_t *parsec, dplasma_enum_t side, dplasma_enum_t uplo,
+                  dplasma_enum_t trans, dplasma_enum_t diag, double alpha,
+                  const parsec_tiled_matrix_t *A, parsec_tiled_matrix_t *B);
+
+/* Generators.  dplasma_dplgsy: src/zplgsy_wrapper.c:185-215 with
+ * CORE_dplgsy (src/cores/core_zplgsy.c:72-150); dplasma_dplrnt:
+ * src/zplrnt_wrapper.c (CORE_dplrnt, src/cores/core_zplrnt.c:68-91)
+ * (dplasma_z.h:108-109).  Bit-identical values.  Return 0 or -i for a bad
+ * argument i. */
+int dplasma_dplgsy(parsec_context_t *parsec, double bump, dplasma_enum_t uplo,
+                   parsec_tiled_matrix_t *A, unsigned long long int seed);
+int dplasma_dplrnt(parsec_context_t *parsec, int diagdom, parsec_tiled_matrix_t *A,
+                   unsigned long long int seed);
+
+/* Infinity norm of a symmetric matrix stored by its `uplo` triangle
+ * (dplasma_dlansy with dplasmaInfNorm, dplasma_z.h:101), computed on the GPU;
+ * returns a negative value for an unsupported norm or descriptor. */
+double dplasma_dlansy(parsec_context_t *parsec, dplasma_enum_t ntype, dplasma_enum_t uplo,
+                      const parsec_tiled_matrix_t *A);
+
+/* ---- instrumentation ---------------------------------------------------- */
+/* Device time in milliseconds of the last factorization (CUDA events around
+ * the scheduler launch only) and of the last triangular-solve pair. */
+double dplasma_b200_last_factor_ms(const parsec_context_t *ctx);
+double dplasma_b200_last_solve_ms(const parsec_context_t *ctx);
+/* Number of kernel launches issued by the last public call. */
+int dplasma_b200_last_launches(const parsec_context_t *ctx);
+
+/* Measured FP64 tensor-core (DMMA) throughput of this GPU in TFLOP/s: a
+ * register-only mma.sync.m16n8k4.f64 loop on every SM, timed with CUDA
+ * events.  The roofline denominator for the FP64 kernels. */
+double dplasma_b200_fp64_peak_tflops(parsec_context_t *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DPLASMA_B200_H */
