@@ -197,7 +197,11 @@ __device__ __forceinline__ bool consume_job(const PotrfArgs &a, SmemCtl *ctl, co
         stage_it++;
     }
 
-    // epilogue: straight to global (each warp writes 64x32; 64-byte runs)
+    // Epilogue straight from registers.  C -= acc is issued as fire-and-forget
+    // FP64 reductions performed in L2 (red.global.add.f64 of -acc): the same
+    // rounding as a load-subtract-store (c + (-a) == c - a), without the
+    // round trip that would idle the tensor pipe; updates of one tile are
+    // serialized by the scheduler, so the result is deterministic.
 #pragma unroll
     for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
@@ -210,9 +214,10 @@ __device__ __forceinline__ bool consume_job(const PotrfArgs &a, SmemCtl *ctl, co
                 if (jb.mode == J_STORE) {
                     *p = acc[mi][ni][q];
                 } else if (jb.mode == J_SUB || r >= c) {
-                    *p = __ldcg(p) - acc[mi][ni][q];
+                    atomicAdd(p, -acc[mi][ni][q]);
                 }
             }
+    __threadfence();   // this thread's reductions are performed before any later release
     return true;
 }
 
@@ -428,6 +433,11 @@ __device__ void consumer_warps(const PotrfArgs &a, SmemCtl *ctl, double *ring)
     if (tid == 0 && a.trace) a.trace_exit[6 * blockIdx.x + 1] = globaltimer_ns();
 }
 
+// Registers are allocated per SM sub-partition, so a CTA of 12 warps launches
+// with at most 168 per thread.  The producer warpgroup gives registers back
+// (setmaxnreg.dec to PRODUCER_REGS) and the two consumer warpgroups take them
+// (setmaxnreg.inc to CONSUMER_REGS): 4*32*48 + 8*32*224 = 63488 <= 384*168, and
+// per sub-partition 1*32*48 + 2*32*224 = 15872 <= 16384.
 __global__ void __launch_bounds__(NTHREADS, 1) potrf_persistent_kernel(PotrfArgs a)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -447,9 +457,13 @@ __global__ void __launch_bounds__(NTHREADS, 1) potrf_persistent_kernel(PotrfArgs
     }
     __syncthreads();
     if (threadIdx.x >= NCONS) {
-        producer_warp(a, ctl, ring);
-        if (a.trace && threadIdx.x == NCONS) a.trace_exit[6 * blockIdx.x] = globaltimer_ns();
+        asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;\n" ::"n"(PRODUCER_REGS));
+        if (threadIdx.x < NCONS + 32) {
+            producer_warp(a, ctl, ring);
+            if (a.trace && threadIdx.x == NCONS) a.trace_exit[6 * blockIdx.x] = globaltimer_ns();
+        }
     } else {
+        asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;\n" ::"n"(CONSUMER_REGS));
         consumer_warps(a, ctl, ring);
     }
 }

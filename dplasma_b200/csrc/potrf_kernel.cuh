@@ -7,7 +7,7 @@
 // (critical path first, one step of look-ahead), waits on per-tile completion
 // counters (bounded waits), and runs the task:
 //
-//   warp 8  (producer): fetches tickets, waits for the task's dependencies,
+//   warp 8  (producer; warps 9-11 only lend their registers): fetches tickets, waits for the task's dependencies,
 //            streams operand columns into a shared-memory ring with bulk
 //            copies (cp.async.bulk, the TMA engine) completing on mbarriers;
 //   warps 0-7 (consumers): FP64 DMMA (mma.sync m16n8k4 .f64) on 128x128
@@ -33,8 +33,10 @@ constexpr int BLK = 128;         // output block edge handled by one CTA job
 constexpr int BK = 16;           // K depth of one pipeline stage
 constexpr int SP = BLK + 4;      // shared pitch (doubles) of an operand row, = 4 mod 16
 constexpr int NSTAGE = 5;        // pipeline stages
-constexpr int NCONS = 256;       // consumer threads (8 warps)
-constexpr int NTHREADS = NCONS + 32;
+constexpr int NCONS = 256;       // consumer threads (2 warpgroups)
+constexpr int NTHREADS = NCONS + 128;   // + producer warpgroup (one active warp)
+constexpr int PRODUCER_REGS = 48;
+constexpr int CONSUMER_REGS = 224;
 constexpr int TASKQ = 4;         // task ring depth
 constexpr int STAGE_DOUBLES = 2 * BK * SP;
 
