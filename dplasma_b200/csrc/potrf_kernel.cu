@@ -645,3 +645,100 @@ int potrf_max_blocks_per_sm()
     return n;
 }
 }  // namespace db2
+
+// ---------------------------------------------------------------------------
+// Launch on caller-provided scratch (no allocation, no context): used by the
+// allocation-free entry point in noalloc.cu.
+// ---------------------------------------------------------------------------
+namespace db2 {
+
+// Same ticket order as build_potrf_tasks, written into a caller buffer
+// without heap use; returns the count, or 0 if it does not fit in `cap`.
+size_t build_potrf_tasks_into(uint64_t *out, size_t cap, int mt, int nbs, int delay)
+{
+    size_t n = 0;
+    bool fits = true;
+    auto put = [&](uint64_t t) {
+        if (n < cap) out[n] = t; else fits = false;
+        ++n;
+    };
+    auto put_trsm = [&](int k) {
+        for (int m = k + 1; m < mt; ++m)
+            for (int bi = 0; bi < nbs; ++bi) put(make_task(T_TRSM, k, m, k, bi, 0));
+    };
+    // the rest of step k, i-th task (columns n >= k+2 by increasing n, then m, bi, bj)
+    auto put_rest_range = [&](int k, size_t from, size_t to) {
+        size_t i = 0;
+        for (int n2 = k + 2; n2 < mt; ++n2)
+            for (int m = n2; m < mt; ++m)
+                for (int bi = 0; bi < nbs; ++bi)
+                    for (int bj = 0; bj < nbs; ++bj) {
+                        if (m == n2 && bj > bi) continue;
+                        if (i >= from && i < to) put(make_task(T_GEMM, k, m, n2, bi, bj));
+                        ++i;
+                    }
+        return i;
+    };
+    put(make_task(T_POTRF, 0, 0, 0, 0, 0));
+    put_trsm(0);
+    for (int k = 0; k + 1 < mt; ++k) {
+        for (int m = k + 1; m < mt; ++m)
+            for (int bi = 0; bi < nbs; ++bi)
+                for (int bj = 0; bj < nbs; ++bj) {
+                    if (m == k + 1 && bj > bi) continue;
+                    put(make_task(T_GEMM, k, m, k + 1, bi, bj));
+                }
+        put(make_task(T_POTRF, k + 1, k + 1, k + 1, 0, 0));
+        const size_t total = put_rest_range(k, 0, 0);
+        const size_t d = (size_t)std::max(delay, 0) < total ? (size_t)std::max(delay, 0) : total;
+        put_rest_range(k, 0, d);
+        put_trsm(k + 1);
+        put_rest_range(k, d, total);
+    }
+    return fits ? n : 0;
+}
+
+int potrf_launch_prealloc(cudaStream_t st, double *dA, int mt, int nbi, int nb_user, int n_user, double *W,
+                          const uint64_t *tasks, int ntasks, int *ctr, int grid, uint64_t limit_ns, int *info,
+                          int *status, int diag[4])
+{
+    PotrfArgs a;
+    a.A = dA;
+    a.W = W;
+    a.tasks = tasks;
+    a.ntasks = ntasks;
+    a.mt = mt;
+    a.nbi = nbi;
+    a.nbs = nbi / BLK;
+    a.nb_user = nb_user;
+    a.n_user = n_user;
+    a.ticket = ctr + 0;
+    a.info = ctr + 1;
+    a.abort_flag = ctr + 2;
+    a.status = ctr + 3;
+    a.diag = ctr + 4;
+    a.potrf_done = ctr + 8;
+    a.trsm_done = a.potrf_done + mt;
+    a.upd_done = a.trsm_done + (size_t)mt * mt;
+    a.task_count = nullptr;
+    a.trace = nullptr;
+    a.trace_exit = nullptr;
+    a.trace_cta = nullptr;
+    a.dep_limit_ns = limit_ns;
+    a.pipe_limit_ns = limit_ns;
+    const size_t smem = potrf_smem_bytes();
+    if (cudaFuncSetAttribute(potrf_persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+        return DPLASMA_ERR_UNEXPECTED;
+    potrf_persistent_kernel<<<grid, NTHREADS, smem, st>>>(a);
+    if (cudaGetLastError() != cudaSuccess) return DPLASMA_ERR_UNEXPECTED;
+    int hs[8];
+    if (cudaMemcpyAsync(hs, ctr, sizeof(hs), cudaMemcpyDeviceToHost, st) != cudaSuccess) return DPLASMA_ERR_UNEXPECTED;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return DPLASMA_ERR_UNEXPECTED;
+    *info = hs[1];
+    *status = hs[3];
+    for (int i = 0; i < 4; ++i) diag[i] = hs[4 + i];
+    return 0;
+}
+
+}  // namespace db2

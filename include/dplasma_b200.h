@@ -188,6 +188,20 @@ int dplasma_dplrnt(parsec_context_t *parsec, int diagdom, parsec_tiled_matrix_t 
 double dplasma_dlansy(parsec_context_t *parsec, dplasma_enum_t ntype, dplasma_enum_t uplo,
                       const parsec_tiled_matrix_t *A);
 
+/* dplasma_b200_dpotrf_noalloc: no counterpart in the reference.  The lower
+ * tile Cholesky of a device-resident matrix (TILE storage of the lower
+ * triangle of tiles, nb a multiple of 128 and at most 512, n a multiple of nb,
+ * n <= 8192) for callers that cannot allocate device memory, e.g. code that
+ * hands the library memory from its own pool and may not let the device heap
+ * grow.  It allocates nothing: its scratch is one fixed array of about
+ * 8.4 MiB in the library's device image, held on every GPU that loads the
+ * library until exit; larger n is rejected with DPLASMA_ERR_INTERNAL_LIMIT.
+ * Runs on `stream` (a cudaStream_t, or NULL for the default stream) of the
+ * current device and returns INFO as dplasma_dpotrf does.  All calls share
+ * the scratch, so calls that overlap on the GPU race; the first call on a
+ * device looks the scratch up and should come before any stream capture. */
+int dplasma_b200_dpotrf_noalloc(void *stream, dplasma_enum_t uplo, parsec_tiled_matrix_t *A);
+
 /* ---- instrumentation ---------------------------------------------------- */
 /* Device time in milliseconds of the last factorization (CUDA events around
  * the scheduler launch only) and of the last triangular-solve pair. */
