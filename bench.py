@@ -268,15 +268,15 @@ def run_gpu(args):
                "sample": f"dpotrf N={args.cpu_n} NB=256 lower, one run of {t:.2f} s: the reference's CORE_d* kernels "
                          "(compiled from its sources) as the tile DAG, OpenMP tasks over OpenBLAS on all host cores"}
 
+    # DRAM bytes of one factorization launch: an ncu capture at a smaller N
+    # (profiles/potrf_traffic_N16384.txt), scaled by (N/n)^3 at the same NB.
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", "potrf_traffic.json")
-    if os.path.exists(tpath):
-        try:
-            tj = json.load(open(tpath))
-            # bytes per launch measured on a smaller capture, scaled by units (N^3)
-            traffic = tj["dram_bytes_per_launch"] * (N / tj["n"]) ** 3
-        except Exception:
-            traffic = None
+    tpath = os.path.join(ROOT, "profiles", "potrf_traffic_N16384.txt")
+    if os.path.exists(tpath) and NB == 256:
+        for line in open(tpath):
+            if line.startswith("dram_bytes_per_launch"):
+                _, b, _, n0 = line.split()
+                traffic = float(b) * (N / float(n0)) ** 3
 
     clocks = clk.summary()
     line = {
