@@ -34,6 +34,7 @@ struct Context {
     int potrf_grid = 0;
     int potrf_delay = 0;
     int solve_grid = 0;
+    int wave_occ = 0;                        // CTAs per SM of the wavefront solve (0: not usable)
     uint64_t dep_limit_ns = 4000000000ull;   // 4 s
     uint64_t pipe_limit_ns = 4000000000ull;  // 4 s
     bool self_check = false;
@@ -106,6 +107,11 @@ size_t desc_elems(const parsec_tiled_matrix_t *A);
 int trtri_diag(Context *ctx, const double *dA, const Geom &g, double *W, int unit_diag);
 int trsm_sweep(Context *ctx, const double *dA, const double *W, const Geom &g, double *dB, int ldb, int nrhs,
                int transposed, double alpha);
+// wave_kernel.cu: cooperative wavefront form of the same sweep; returns 1 when
+// the shape needs more than its per-CTA block budget (caller falls back).
+int trsm_wave(Context *ctx, const double *dA, const double *W, const Geom &g, double *dB, int ldb, int nrhs,
+              int transposed, double alpha);
+int wave_max_blocks_per_sm();
 
 // norms.cu
 int lansy_inf_device(Context *ctx, const double *dA, const Geom &g, double *out);

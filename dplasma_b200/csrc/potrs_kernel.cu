@@ -321,6 +321,8 @@ static int launch_sweep(Context *ctx, SweepArgs &a)
 int trsm_sweep(Context *ctx, const double *dA, const double *W, const Geom &g, double *dB, int ldb, int nrhs,
                int transposed, double alpha)
 {
+    const int wrc = trsm_wave(ctx, dA, W, g, dB, ldb, nrhs, transposed, alpha);
+    if (wrc <= 0) return wrc;
     const int nblk = g.mt * (g.nbi / 128);
     // flags + ticket + status + abort per 32-column chunk
     const int nchunks = (nrhs + 31) / 32;

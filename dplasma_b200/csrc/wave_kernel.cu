@@ -1,0 +1,366 @@
+// wave_kernel.cu -- triangular solve sweep as a cooperative wavefront.
+//
+//   forward   L   Y = alpha B   (q ascending)
+//   backward  L^T Y = alpha B   (q descending)
+// over 128-row blocks.  CTA c owns the blocks p = c, c+G, c+2G, ... (at most
+// WV_RMAX of them) and keeps their partial sums in registers.  For every
+// block q in solve order it
+//   * if it owns q: forms Y_q = W_qq^{op} acc_q (W_qq the inverse of the
+//     diagonal block), stores it and raises q's flag;
+//   * otherwise: waits for q's flag and stages Y_q in shared memory;
+//   * applies acc_p -= op(L)_pq Y_q to each owned block p still to solve.
+// Each owned accumulator is updated in increasing q by one CTA, so the result
+// is deterministic.  A producer warp streams the L blocks into a ring of
+// bulk copies ahead of the flags (they do not depend on Y), so the critical
+// path per block is one flag, one 128x128 update and the diagonal multiply,
+// while the bulk of L streams from HBM on all SMs at once.  CTAs wait on one
+// another, hence the cooperative launch.
+#include <cuda_runtime.h>
+
+#include "dev_common.cuh"
+#include "internal.h"
+
+namespace db2 {
+
+constexpr int WV_RMAX = 4;
+constexpr int WV_KS = 32;
+constexpr int WV_NST = 3;
+constexpr int WV_APF = 132;            // forward stage: As[kk][r]
+constexpr int WV_APB = 36;             // backward stage: As[r][kk]
+constexpr int WV_A_DOUBLES = 128 * 36; // >= 32 * 132
+constexpr int WV_YP = 132;             // Y stage [n][k], k < 128 (two of them)
+constexpr int WV_THREADS = 384;
+
+struct WaveArgs {
+    const double *A;
+    const double *W;
+    double *Y;
+    int ldy;
+    int mt, nbi, nbs, nblk;
+    int c0;
+    double alpha;
+    int *flags;
+    int *status;
+    uint64_t limit_ns;
+};
+
+struct __align__(16) WaveCtl {
+    uint64_t full[WV_NST];
+    uint64_t empty[WV_NST];
+};
+
+__device__ __forceinline__ const double *wv_lblock(const WaveArgs &a, int p, int q)
+{
+    const int tp = p / a.nbs, tq = q / a.nbs;
+    return a.A + lower_tile_index(tp, tq, a.mt) * (int64_t)a.nbi * a.nbi + (int64_t)(q % a.nbs) * 128 * a.nbi +
+           (p % a.nbs) * 128;
+}
+
+// Solve order position qi -> block q, and its successor.
+template <bool TRANS>
+__device__ __forceinline__ int wv_block(int qi, int P) { return TRANS ? P - 1 - qi : qi; }
+
+template <int NC, bool TRANS>
+__global__ void __launch_bounds__(WV_THREADS, 1) trsm_wave_kernel(WaveArgs a)
+{
+    extern __shared__ __align__(128) unsigned char smraw[];
+    WaveCtl *ctl = reinterpret_cast<WaveCtl *>(smraw);
+    double *ring = reinterpret_cast<double *>(smraw + 128);
+    double *Ybuf = ring + WV_NST * WV_A_DOUBLES;   // two Y stages of 32 x WV_YP
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int c = blockIdx.x, G = gridDim.x, P = a.nblk;
+    if (tid == 0) {
+        for (int s = 0; s < WV_NST; ++s) {
+            mbar_init(&ctl->full[s], 1);
+            mbar_init(&ctl->empty[s], 8);
+        }
+    }
+    __syncthreads();
+
+    // Work of position qi for this CTA, in order:
+    //   [critical] if it owns the next block nq: L(nq, q) then W(nq)   (8 stages)
+    //   [rest]     L(p, q) for its other blocks p still to solve        (4 stages each)
+    // plus, before position 0, W(first block) if it owns it.
+    if (warp >= 8) {
+        asm volatile("setmaxnreg.dec.sync.aligned.u32 48;\n");
+        if (warp != 8) return;
+        uint32_t it = 0;
+        bool ok = true;
+        auto issue = [&](const double *src, int ld) {
+            for (int s0 = 0; s0 < 128 && ok; s0 += WV_KS) {
+                const uint32_t s = it % WV_NST, r = it / WV_NST;
+                if (r > 0 && !warp_mbar_wait(&ctl->empty[s], (r - 1) & 1, a.limit_ns)) {
+                    if (lane == 0) atomicCAS(a.status, ST_OK, ST_MBAR_TIMEOUT);
+                    ok = false;
+                    break;
+                }
+                double *As = ring + s * WV_A_DOUBLES;
+                if (lane == 0) mbar_arrive_expect_tx(&ctl->full[s], 128 * WV_KS * (uint32_t)sizeof(double));
+                __syncwarp();
+                if (!TRANS) {
+                    bulk_g2s(As + lane * WV_APF, src + (int64_t)(s0 + lane) * ld, 128 * sizeof(double), &ctl->full[s]);
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const int r2 = lane + 32 * j;
+                        bulk_g2s(As + r2 * WV_APB, src + (int64_t)r2 * ld + s0, WV_KS * sizeof(double), &ctl->full[s]);
+                    }
+                }
+                ++it;
+            }
+        };
+        const int first = wv_block<TRANS>(0, P);
+        if (first % G == c) issue(a.W + (int64_t)first * 128 * 128, 128);
+        for (int qi = 0; qi < P && ok; ++qi) {
+            const int q = wv_block<TRANS>(qi, P);
+            const int nq = (qi + 1 < P) ? wv_block<TRANS>(qi + 1, P) : -1;
+            if (nq >= 0 && nq % G == c) {
+                issue(TRANS ? wv_lblock(a, q, nq) : wv_lblock(a, nq, q), a.nbi);
+                issue(a.W + (int64_t)nq * 128 * 128, 128);
+            }
+            for (int i = 0; i < WV_RMAX && ok; ++i) {
+                const int p = c + i * G;
+                if (p >= P || p == nq || !(TRANS ? p < q : p > q)) continue;
+                issue(TRANS ? wv_lblock(a, q, p) : wv_lblock(a, p, q), a.nbi);
+            }
+        }
+        const uint32_t fst = it > WV_NST ? it - WV_NST : 0;
+        for (uint32_t k = fst; k < it; ++k) warp_mbar_wait(&ctl->full[k % WV_NST], (k / WV_NST) & 1, a.limit_ns);
+        return;
+    }
+
+    asm volatile("setmaxnreg.inc.sync.aligned.u32 224;\n");
+    constexpr int NT = NC / 8;
+    const int g = lane >> 2, t = lane & 3;
+    double acc[WV_RMAX][NT][4];
+#pragma unroll
+    for (int i = 0; i < WV_RMAX; ++i) {
+        const int p = c + i * G;
+#pragma unroll
+        for (int ni = 0; ni < NT; ++ni)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int r = warp * 16 + g + ((e & 2) ? 8 : 0);
+                const int col = ni * 8 + 2 * t + (e & 1);
+                acc[i][ni][e] = (p < P) ? a.alpha * __ldcg(a.Y + (int64_t)(a.c0 + col) * a.ldy + (int64_t)p * 128 + r)
+                                        : 0.0;
+            }
+    }
+    uint32_t it = 0;
+    bool ok = true;
+
+    // acc_i -= op(L) * Ystage, four stages from the ring
+    auto update = [&](double (&ac)[NT][4], const double *Yst) {
+        for (int s0 = 0; s0 < 128 && ok; s0 += WV_KS) {
+            const uint32_t s = it % WV_NST, r = it / WV_NST;
+            if (!warp_mbar_wait(&ctl->full[s], r & 1, a.limit_ns)) {
+                if (lane == 0) atomicCAS(a.status, ST_OK, ST_MBAR_TIMEOUT);
+                ok = false;
+                break;
+            }
+            const double *As = ring + s * WV_A_DOUBLES;
+#pragma unroll
+            for (int kk = 0; kk < WV_KS; kk += 4) {
+                double a0, a1;
+                if (!TRANS) {
+                    a0 = As[(kk + t) * WV_APF + warp * 16 + g];
+                    a1 = As[(kk + t) * WV_APF + warp * 16 + g + 8];
+                } else {
+                    a0 = As[(warp * 16 + g) * WV_APB + kk + t];
+                    a1 = As[(warp * 16 + g + 8) * WV_APB + kk + t];
+                }
+#pragma unroll
+                for (int ni = 0; ni < NT; ++ni) dmma_16x8x4(ac[ni], -a0, -a1, Yst[(ni * 8 + g) * WV_YP + s0 + kk + t]);
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&ctl->empty[s]);
+            ++it;
+        }
+    };
+    // Y_q = op(W_qq) * acc (W streamed through the ring); result to Yst and global
+    auto diag = [&](double (&ac)[NT][4], double *Yst, int q) {
+#pragma unroll
+        for (int ni = 0; ni < NT; ++ni)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int r = warp * 16 + g + ((e & 2) ? 8 : 0);
+                const int col = ni * 8 + 2 * t + (e & 1);
+                Yst[col * WV_YP + r] = ac[ni][e];
+                ac[ni][e] = 0.0;
+            }
+        named_bar_sync(1, 256);
+        double res[NT][4];
+#pragma unroll
+        for (int ni = 0; ni < NT; ++ni)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) res[ni][e] = 0.0;
+        for (int s0 = 0; s0 < 128 && ok; s0 += WV_KS) {
+            const uint32_t s = it % WV_NST, r = it / WV_NST;
+            if (!warp_mbar_wait(&ctl->full[s], r & 1, a.limit_ns)) {
+                if (lane == 0) atomicCAS(a.status, ST_OK, ST_MBAR_TIMEOUT);
+                ok = false;
+                break;
+            }
+            const double *As = ring + s * WV_A_DOUBLES;
+#pragma unroll
+            for (int kk = 0; kk < WV_KS; kk += 4) {
+                double a0, a1;
+                if (!TRANS) {   // A = W: rows of W are the ring's columns
+                    a0 = As[(kk + t) * WV_APF + warp * 16 + g];
+                    a1 = As[(kk + t) * WV_APF + warp * 16 + g + 8];
+                } else {        // A = W^T
+                    a0 = As[(warp * 16 + g) * WV_APB + kk + t];
+                    a1 = As[(warp * 16 + g + 8) * WV_APB + kk + t];
+                }
+#pragma unroll
+                for (int ni = 0; ni < NT; ++ni) dmma_16x8x4(res[ni], a0, a1, Yst[(ni * 8 + g) * WV_YP + s0 + kk + t]);
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&ctl->empty[s]);
+            ++it;
+        }
+        named_bar_sync(1, 256);
+        double *Yq = a.Y + (int64_t)a.c0 * a.ldy + (int64_t)q * 128;
+#pragma unroll
+        for (int ni = 0; ni < NT; ++ni)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int r = warp * 16 + g + ((e & 2) ? 8 : 0);
+                const int col = ni * 8 + 2 * t + (e & 1);
+                Yst[col * WV_YP + r] = res[ni][e];
+                Yq[(int64_t)col * a.ldy + r] = res[ni][e];
+            }
+        __threadfence();
+        named_bar_sync(1, 256);
+        if (tid == 0) red_release_add(a.flags + q, 1);
+    };
+
+    // first block: its owner solves it right away
+    const int first = wv_block<TRANS>(0, P);
+    if (first % G == c) {
+#pragma unroll
+        for (int i = 0; i < WV_RMAX; ++i)
+            if (c + i * G == first) diag(acc[i], Ybuf, first);
+    }
+    for (int qi = 0; qi < P && ok; ++qi) {
+        const int q = wv_block<TRANS>(qi, P);
+        const int nq = (qi + 1 < P) ? wv_block<TRANS>(qi + 1, P) : -1;
+        double *Yq = Ybuf + (qi & 1) * (32 * WV_YP);          // holds Y_q
+        double *Ynext = Ybuf + ((qi + 1) & 1) * (32 * WV_YP); // receives Y_nq if owned
+        bool any = false;
+#pragma unroll
+        for (int i = 0; i < WV_RMAX; ++i) {
+            const int p = c + i * G;
+            any |= (p < P) && (TRANS ? p < q : p > q);
+        }
+        if (!any) continue;
+        if (q % G != c) {
+            // Y_q from its owner
+            int good = 1;
+            if (tid == 0) good = wait_geq(a.flags + q, 1, a.status, a.status, a.limit_ns) ? 1 : 0;
+            named_bar_sync(1, 256);
+            if (ld_volatile(a.status) != ST_OK || !good) break;
+            const double *Yg = a.Y + (int64_t)a.c0 * a.ldy + (int64_t)q * 128;
+            for (int e = tid; e < NC * 128; e += 256) {
+                const int col = e / 128, r = e % 128;
+                Yq[col * WV_YP + r] = __ldcg(Yg + (int64_t)col * a.ldy + r);
+            }
+            named_bar_sync(1, 256);
+        }
+        // critical path first: the next block, if owned
+        if (nq >= 0 && nq % G == c) {
+#pragma unroll
+            for (int i = 0; i < WV_RMAX; ++i) {
+                if (c + i * G != nq) continue;
+                update(acc[i], Yq);
+                if (ok) diag(acc[i], Ynext, nq);
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < WV_RMAX; ++i) {
+            const int p = c + i * G;
+            if (p >= P || p == nq || !(TRANS ? p < q : p > q)) continue;
+            update(acc[i], Yq);
+        }
+        named_bar_sync(1, 256);   // Yq is overwritten two positions later
+    }
+}
+
+template <int NC, bool TRANS>
+static int launch_wave(Context *ctx, WaveArgs &a, int grid)
+{
+    const size_t smem = 128 + (size_t)(WV_NST * WV_A_DOUBLES + 2 * 32 * WV_YP) * sizeof(double);
+    CK(cudaFuncSetAttribute(trsm_wave_kernel<NC, TRANS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    void *args[] = {&a};
+    CK(cudaLaunchCooperativeKernel((const void *)trsm_wave_kernel<NC, TRANS>, dim3(grid), dim3(WV_THREADS), args, smem,
+                                   ctx->stream));
+    ctx->launches++;
+    return 0;
+}
+
+int wave_max_blocks_per_sm()
+{
+    const size_t smem = 128 + (size_t)(WV_NST * WV_A_DOUBLES + 2 * 32 * WV_YP) * sizeof(double);
+    int best = 1 << 30;
+    const void *fns[] = {(const void *)trsm_wave_kernel<32, false>, (const void *)trsm_wave_kernel<32, true>};
+    for (const void *fn : fns) {
+        int n = 0;
+        if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, WV_THREADS, smem) != cudaSuccess)
+            n = 0;
+        if (n < best) best = n;
+    }
+    return best;
+}
+
+// Returns 1 when the shape does not fit the wavefront kernel (more than
+// WV_RMAX blocks per CTA), 0 on success, a negative dplasma error otherwise.
+int trsm_wave(Context *ctx, const double *dA, const double *W, const Geom &g, double *dB, int ldb, int nrhs,
+              int transposed, double alpha)
+{
+    const int nblk = g.mt * (g.nbi / 128);
+    const int grid = ctx->sms * (ctx->wave_occ > 0 ? 1 : 0);
+    if (grid < 1 || nblk > WV_RMAX * grid) return 1;
+    const int nchunks = (nrhs + 31) / 32;
+    const size_t per = (size_t)nblk + 4;
+    int *ctr = (int *)ctx->buffer(BUF_SOLVE_CTR, per * nchunks * sizeof(int));
+    if (!ctr) return DPLASMA_ERR_OUT_OF_RESOURCES;
+    CK(cudaMemsetAsync(ctr, 0, per * nchunks * sizeof(int), ctx->stream));
+    for (int ch = 0; ch < nchunks; ++ch) {
+        WaveArgs a;
+        a.A = dA;
+        a.W = W;
+        a.Y = dB;
+        a.ldy = ldb;
+        a.mt = g.mt;
+        a.nbi = g.nbi;
+        a.nbs = g.nbi / 128;
+        a.nblk = nblk;
+        a.c0 = ch * 32;
+        a.alpha = alpha;
+        a.status = ctr + per * ch;
+        a.flags = ctr + per * ch + 4;
+        a.limit_ns = ctx->dep_limit_ns;
+        const int nc = (nrhs - a.c0) < 32 ? (nrhs - a.c0) : 32;   // nrhs is a multiple of 8
+        int rc;
+        if (transposed)
+            rc = nc <= 8 ? launch_wave<8, true>(ctx, a, grid) : nc <= 16 ? launch_wave<16, true>(ctx, a, grid)
+                 : nc <= 24 ? launch_wave<24, true>(ctx, a, grid) : launch_wave<32, true>(ctx, a, grid);
+        else
+            rc = nc <= 8 ? launch_wave<8, false>(ctx, a, grid) : nc <= 16 ? launch_wave<16, false>(ctx, a, grid)
+                 : nc <= 24 ? launch_wave<24, false>(ctx, a, grid) : launch_wave<32, false>(ctx, a, grid);
+        if (rc) return rc;
+    }
+    int st = 0;
+    for (int ch = 0; ch < nchunks; ++ch) {
+        CK(cudaMemcpyAsync(&st, ctr + per * ch, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        if (st != ST_OK) {
+            ctx->set_error("triangular wavefront status %d", st);
+            return DPLASMA_ERR_UNEXPECTED;
+        }
+    }
+    return 0;
+}
+
+}  // namespace db2
