@@ -42,6 +42,24 @@ class Desc(ctypes.Structure):
         "location")] + [("bsiz", ctypes.c_size_t), ("nb_local_tiles", ctypes.c_size_t), ("mat", ctypes.c_void_p)]
 
 
+class RefineOpts(ctypes.Structure):
+    """dplasma_b200_refine_opts_t."""
+
+    _fields_ = [("fmt", ctypes.c_int), ("solver", ctypes.c_int), ("itermax", ctypes.c_int), ("gmres_m", ctypes.c_int),
+                ("gmres_tol", ctypes.c_double), ("bwdmax", ctypes.c_double)]
+
+
+class RefineStats(ctypes.Structure):
+    """dplasma_b200_refine_stats_t."""
+
+    _fields_ = [("iter", ctypes.c_int), ("inner_iters", ctypes.c_int), ("fallback", ctypes.c_int),
+                ("solver_used", ctypes.c_int), ("backward_error", ctypes.c_double), ("factor_ms", ctypes.c_double),
+                ("refine_ms", ctypes.c_double)]
+
+
+FP16, BF16 = 0, 1
+IR_AUTO, IR_PLAIN, IR_GMRES = 0, 1, 2
+
 _lib = None
 
 EXPORTS = (
@@ -50,7 +68,8 @@ EXPORTS = (
     "dplasma_dpotrf_Destruct", "dplasma_b200_taskpool_run", "dplasma_dpotrf_rec", "dplasma_dpotrf_setrecursive",
     "dplasma_dpotrs", "dplasma_dposv", "dplasma_dtrsm", "dplasma_dplgsy", "dplasma_dplrnt", "dplasma_dlansy",
     "dplasma_b200_last_factor_ms", "dplasma_b200_last_solve_ms", "dplasma_b200_last_launches",
-    "dplasma_b200_fp64_peak_tflops",
+    "dplasma_b200_fp64_peak_tflops", "dplasma_b200_refine_opts_default", "dplasma_dsposv",
+    "dplasma_b200_dsposv_ex",
 )
 
 
@@ -94,6 +113,9 @@ def lib():
     L.dplasma_b200_last_launches.argtypes = [P]
     L.dplasma_b200_fp64_peak_tflops.restype = D
     L.dplasma_b200_fp64_peak_tflops.argtypes = [P]
+    L.dplasma_b200_refine_opts_default.argtypes = [ctypes.POINTER(RefineOpts)]
+    L.dplasma_dsposv.argtypes = [P, I, pd, pd, pd, ctypes.POINTER(I)]
+    L.dplasma_b200_dsposv_ex.argtypes = [P, I, pd, pd, pd, ctypes.POINTER(RefineOpts), ctypes.POINTER(RefineStats)]
     _lib = L
     return L
 
@@ -229,6 +251,17 @@ class Context:
 
     def dlansy(self, ntype: int, uplo: int, A: Desc) -> float:
         return lib().dplasma_dlansy(self.h, ntype, uplo, ctypes.byref(A))
+
+    def dsposv(self, uplo: int, A: Desc, B: Desc, X: Desc, fmt: int = FP16, solver: int = IR_AUTO,
+               itermax: int = 30, gmres_m: int = 30, gmres_tol: float = 1e-4, bwdmax: float = 1.0):
+        """Mixed-precision solve (dplasma_b200_dsposv_ex): returns (rc, stats dict)."""
+        o = RefineOpts()
+        lib().dplasma_b200_refine_opts_default(ctypes.byref(o))
+        o.fmt, o.solver, o.itermax, o.gmres_m, o.gmres_tol, o.bwdmax = fmt, solver, itermax, gmres_m, gmres_tol, bwdmax
+        st = RefineStats()
+        rc = lib().dplasma_b200_dsposv_ex(self.h, uplo, ctypes.byref(A), ctypes.byref(B), ctypes.byref(X),
+                                          ctypes.byref(o), ctypes.byref(st))
+        return rc, {f: getattr(st, f) for f, _ in RefineStats._fields_}
 
 
 def attach(d: Desc, buf) -> Desc:

@@ -139,6 +139,7 @@ extern "C" parsec_context_t *dplasma_b200_init(int device)
         return nullptr;
     }
     ctx->potrf_grid = getenv_int("DPLASMA_B200_GRID", ctx->sms * occ);
+    ctx->potrf_grid_mixed = ctx->sms * potrf_max_blocks_per_sm(true);
     ctx->potrf_delay = getenv_int("DPLASMA_B200_DELAY", 3 * ctx->potrf_grid);
     ctx->wave_occ = getenv_int("DPLASMA_B200_NO_WAVE", 0) ? 0 : wave_max_blocks_per_sm();
     int occs = sweep_max_blocks_per_sm();
@@ -458,3 +459,107 @@ extern "C" double dplasma_dlansy(parsec_context_t *parsec, dplasma_enum_t ntype,
     return out;
 }
 
+
+// ---------------------------------------------------------------------------
+// mixed precision (no dplasma counterpart; LAPACK dsposv argument meaning)
+// ---------------------------------------------------------------------------
+extern "C" void dplasma_b200_refine_opts_default(dplasma_b200_refine_opts_t *o)
+{
+    if (!o) return;
+    o->fmt = DPLASMA_B200_FP16;
+    o->solver = DPLASMA_B200_IR_AUTO;
+    o->itermax = 30;
+    o->gmres_m = 30;
+    o->gmres_tol = 1e-4;
+    o->bwdmax = 1.0;
+}
+
+extern "C" int dplasma_b200_dsposv_ex(parsec_context_t *parsec, dplasma_enum_t uplo, parsec_tiled_matrix_t *A,
+                                      const parsec_tiled_matrix_t *B, parsec_tiled_matrix_t *X,
+                                      const dplasma_b200_refine_opts_t *opts, dplasma_b200_refine_stats_t *stats)
+{
+    if (stats) memset(stats, 0, sizeof(*stats));
+    if (uplo != dplasmaUpper && uplo != dplasmaLower) {
+        dplasma_error("dplasma_dsposv", "illegal value of uplo");
+        return -1;
+    }
+    dplasma_b200_refine_opts_t o;
+    dplasma_b200_refine_opts_default(&o);
+    if (opts) o = *opts;
+    if ((o.fmt != DPLASMA_B200_FP16 && o.fmt != DPLASMA_B200_BF16) || o.solver < 0 || o.solver > 2 ||
+        o.itermax < 0 || o.gmres_m < 1 || o.gmres_m > 200 || !(o.gmres_tol > 0.0) || !(o.bwdmax > 0.0)) {
+        dplasma_error("dplasma_dsposv", "illegal options");
+        return DPLASMA_ERR_ILLEGAL_VALUE;
+    }
+    if (!parsec) return DPLASMA_ERR_NOT_INITIALIZED;
+    int rc;
+    if ((rc = check_square("dplasma_dsposv", A)) || (rc = check_general("dplasma_dsposv", B)) ||
+        (rc = check_general("dplasma_dsposv", X)))
+        return rc;
+    if (B->m != A->n || X->m != B->m || X->n != B->n || X->mb != B->mb) {
+        dplasma_error("dplasma_dsposv", "illegal matrix B or X");
+        return -6;
+    }
+    Context *ctx = &parsec->impl;
+    cudaSetDevice(ctx->device);
+    ctx->launches = 0;
+    ctx->errmsg[0] = 0;
+    if (A->m == 0 || B->n == 0) return 0;
+    Geom g = make_geom(A->m, A->mb);
+    if (g.nbi != 256 || g.mt > 65535) {
+        ctx->set_error("mixed-precision solve needs a tile size nb with 128 < nb <= 256 (got %d)", g.nb);
+        return DPLASMA_ERR_NOT_SUPPORTED;
+    }
+    const bool inplace = in_place_ok(A, uplo, g);
+    double *A0 = inplace ? (double *)A->mat : (double *)ctx->buffer(BUF_A0, g.elems() * sizeof(double));
+    double *L = (double *)ctx->buffer(BUF_A, g.elems() * sizeof(double));
+    if (!A0 || !L) return DPLASMA_ERR_OUT_OF_RESOURCES;
+    if (!inplace && (rc = upload_sym(ctx, A, uplo, g, A0))) return rc;
+    const int nrhs_pad = ((B->n + 7) / 8) * 8;
+    const int npad = g.mt * g.nbi;
+    double *b = (double *)ctx->buffer(BUF_B0, (size_t)npad * nrhs_pad * sizeof(double));
+    double *x = (double *)ctx->buffer(BUF_X, (size_t)npad * nrhs_pad * sizeof(double));
+    if (!b || !x) return DPLASMA_ERR_OUT_OF_RESOURCES;
+    if ((rc = upload_rhs(ctx, B, g.nb, g.nbi, npad, nrhs_pad, b))) return rc;
+    RefineOpts ro;
+    ro.fmt = o.fmt;
+    ro.solver = o.solver;
+    ro.itermax = o.itermax;
+    ro.gmres_m = o.gmres_m;
+    ro.gmres_tol = o.gmres_tol;
+    ro.bwd_factor = o.bwdmax;
+    RefineStats st;
+    rc = refine_solve(ctx, A0, L, g, b, x, npad, nrhs_pad, ro, st);
+    if (stats) {
+        stats->iter = st.iter;
+        stats->inner_iters = st.inner_iters;
+        stats->fallback = st.fallback;
+        stats->solver_used = st.solver_used;
+        stats->backward_error = st.backward_error;
+        stats->factor_ms = st.factor_ms;
+        stats->refine_ms = st.refine_ms;
+    }
+    if (rc) return rc;   // error, or INFO > 0 of the FP64 fallback
+    ctx->last_factor_ms = st.factor_ms;
+    ctx->last_solve_ms = st.refine_ms;
+    if ((rc = download_rhs(ctx, X, g.nb, g.nbi, npad, nrhs_pad, x))) return rc;
+    // dsposv: A holds the FP64 factor when the fallback produced the solution
+    if (st.fallback) {
+        if (!inplace) {
+            if ((rc = download_sym(ctx, A, uplo, g, L))) return rc;
+        } else {
+            CK(cudaMemcpyAsync(A->mat, L, g.elems() * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+        }
+    }
+    return 0;
+}
+
+extern "C" int dplasma_dsposv(parsec_context_t *parsec, dplasma_enum_t uplo, parsec_tiled_matrix_t *A,
+                              const parsec_tiled_matrix_t *B, parsec_tiled_matrix_t *X, int *iter)
+{
+    dplasma_b200_refine_stats_t st;
+    const int rc = dplasma_b200_dsposv_ex(parsec, uplo, A, B, X, nullptr, &st);
+    if (iter) *iter = st.iter;
+    return rc;
+}

@@ -160,6 +160,19 @@ __device__ __forceinline__ void named_bar_sync(int id, int nthreads)
     asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
 }
 
+// Named barrier that also ORs a predicate over the participating threads:
+// every thread gets the same answer, so all of them take the same branch.
+__device__ __forceinline__ bool named_bar_or(int id, int nthreads, bool pred)
+{
+    uint32_t r;
+    asm volatile(
+        "{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.or.pred q, %2, %3, p;\n selp.u32 %0, 1, 0, q;\n}\n"
+        : "=r"(r)
+        : "r"((uint32_t)pred), "r"(id), "r"(nthreads)
+        : "memory");
+    return r != 0;
+}
+
 // ---------------------------------------------------------------------------
 // Device matrix layout: lower triangle of tiles, packed column by column,
 // each tile nbi x nbi column-major (leading dimension nbi).

@@ -23,6 +23,13 @@ enum BufferId : int {
     BUF_SOLVE_CTR,    // triangular-solve flags
     BUF_NORM,         // reductions
     BUF_TRACE,        // scheduler trace (opt-in)
+    BUF_P16,          // mixed precision: 16-bit panel copies and their scales
+    BUF_A0,           // mixed precision: FP64 copy of A for the residuals
+    BUF_B0,           // mixed precision: right-hand sides, padded
+    BUF_X,            // mixed precision: solution, padded
+    BUF_R,            // residual / correction
+    BUF_SMALL,        // per-column reductions
+    BUF_KRYLOV,       // GMRES basis
     BUF_COUNT
 };
 
@@ -32,6 +39,7 @@ struct Context {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr, ev3 = nullptr;
     int potrf_grid = 0;
+    int potrf_grid_mixed = 0;
     int potrf_delay = 0;
     int solve_grid = 0;
     int wave_occ = 0;                        // CTAs per SM of the wavefront solve (0: not usable)
@@ -41,6 +49,7 @@ struct Context {
     void *bufs[BUF_COUNT] = {};
     size_t bufsz[BUF_COUNT] = {};
     int task_mt = -1, task_nbs = -1, task_delay = -1, ntasks = 0;
+    bool task_mixed = false;
     double last_factor_ms = 0.0, last_solve_ms = 0.0;
     int launches = 0;
     long long last_tasks_executed = 0;
@@ -92,6 +101,9 @@ Geom make_geom(int n, int nb);
 
 // potrf_kernel.cu
 int potrf_device(Context *ctx, double *dA, int mt, int nbi, int nb_user, int n_user, int *info);
+// p16_fmt < 0: FP64 updates; 0/1: FP16/BF16 tensor-core updates (nbi == 256)
+int potrf_run(Context *ctx, double *dA, int mt, int nbi, int nb_user, int n_user, int *info, int p16_fmt);
+int potrf_max_blocks_per_sm(bool mixed);
 
 // layout.cu : caller layout <-> device tiles
 int upload_sym(Context *ctx, const parsec_tiled_matrix_t *A, dplasma_enum_t uplo, const Geom &g, double *dA);
@@ -112,6 +124,20 @@ int trsm_sweep(Context *ctx, const double *dA, const double *W, const Geom &g, d
 int trsm_wave(Context *ctx, const double *dA, const double *W, const Geom &g, double *dB, int ldb, int nrhs,
               int transposed, double alpha);
 int wave_max_blocks_per_sm();
+
+// refine.cu: mixed-precision factorization + FP64 refinement
+struct RefineOpts {
+    int fmt = 0, solver = 0, itermax = 30, gmres_m = 30;
+    double gmres_tol = 1e-4, bwd_factor = 1.0;
+};
+struct RefineStats {
+    int iter = 0, inner_iters = 0, fallback = 0, solver_used = 0;
+    double backward_error = 0.0, factor_ms = 0.0, refine_ms = 0.0;
+};
+int refine_solve(Context *ctx, const double *A0, double *L, const Geom &g, double *b, double *x, int npad, int nc,
+                 const RefineOpts &o, RefineStats &st);
+int symm_tiles(Context *ctx, const double *dA, const Geom &g, const double *in, int ldin, double *out, int ldout,
+               int ncols, double alpha, int *status);
 
 // norms.cu
 int lansy_inf_device(Context *ctx, const double *dA, const Geom &g, double *out);

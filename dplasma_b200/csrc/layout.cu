@@ -236,7 +236,9 @@ int upload_rhs(Context *ctx, const parsec_tiled_matrix_t *B, int nb, int nbi, in
 int download_rhs(Context *ctx, parsec_tiled_matrix_t *B, int nb, int nbi, int npad, int nrhs, const double *dB)
 {
     cudaStream_t st = ctx->stream;
-    double *dst = (B->location != DPLASMA_B200_DEVICE) ? (double *)ctx->buffer(BUF_BSTAGE, 0) : (double *)B->mat;
+    double *dst = (B->location != DPLASMA_B200_DEVICE) ? (double *)ctx->buffer(BUF_BSTAGE, desc_elems(B) * sizeof(double))
+                                                       : (double *)B->mat;
+    if (!dst) return DPLASMA_ERR_OUT_OF_RESOURCES;
     DescView v = view_of(B, dst);
     rhs_out_kernel<<<ctx->sms * 4, 256, 0, st>>>(v, nb, nbi, npad, nrhs, dB);
     CK(cudaGetLastError());

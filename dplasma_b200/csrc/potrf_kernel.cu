@@ -2,12 +2,16 @@
 // and its host-side launcher.
 #include <cuda_runtime.h>
 #include <math.h>
+#include <string.h>
 #include <algorithm>
 #include <vector>
 
 #include "internal.h"
 #include "potrf_kernel.cuh"
 #include "dev_trtri.cuh"
+#include "dev_tcgen05.cuh"
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 namespace db2 {
 
@@ -25,37 +29,61 @@ __device__ __forceinline__ void report(const PotrfArgs &a, int code, int site, i
 
 // ---------------------------------------------------------------------------
 // dependencies of a task (dataflow of src/zpotrf_L.jdf:107-112, 229-237,
-// 364-368, 486-491, expressed as per-tile completion counts)
+// 364-368, 486-491, expressed as per-tile completion counts).  A tile update
+// of one step is nbs*nbs FP64 blocks (nbs*(nbs+1)/2 on a diagonal tile), or
+// nbs 16-bit block rows in the mixed-precision variant.
 // ---------------------------------------------------------------------------
+template <bool MIXED>
+__device__ __forceinline__ int step_blocks(const PotrfArgs &a, int m, int n)
+{
+    if (MIXED) return a.nbs;
+    return (m == n) ? a.nbs * (a.nbs + 1) / 2 : a.nbs * a.nbs;
+}
+
+template <bool MIXED>
 __device__ bool wait_deps(const PotrfArgs &a, uint64_t t)
 {
     const int k = task_k(t), m = task_m(t), n = task_n(t);
-    const int nbs = a.nbs, nbd = nbs * (nbs + 1) / 2;
+    const int nbs = a.nbs;
     switch (task_type(t)) {
     case T_POTRF:
-        return wait_geq(a.upd_done + (int64_t)k * a.mt + k, k * nbd, a.abort_flag, a.status, a.dep_limit_ns);
+        return wait_geq(a.upd_done + (int64_t)k * a.mt + k, k * step_blocks<MIXED>(a, k, k), a.abort_flag, a.status,
+                        a.dep_limit_ns);
     case T_TRSM:
         return wait_geq(a.potrf_done + k, 1, a.abort_flag, a.status, a.dep_limit_ns) &&
-               wait_geq(a.upd_done + (int64_t)m * a.mt + k, k * nbs * nbs, a.abort_flag, a.status, a.dep_limit_ns);
-    case T_GEMM: {
-        const int nblk = (m == n) ? nbd : nbs * nbs;
+               wait_geq(a.upd_done + (int64_t)m * a.mt + k, k * step_blocks<MIXED>(a, m, k), a.abort_flag, a.status,
+                        a.dep_limit_ns);
+    case T_GEMM:
         return wait_geq(a.trsm_done + (int64_t)m * a.mt + k, nbs, a.abort_flag, a.status, a.dep_limit_ns) &&
                wait_geq(a.trsm_done + (int64_t)n * a.mt + k, nbs, a.abort_flag, a.status, a.dep_limit_ns) &&
-               wait_geq(a.upd_done + (int64_t)m * a.mt + n, k * nblk, a.abort_flag, a.status, a.dep_limit_ns);
-    }
+               wait_geq(a.upd_done + (int64_t)m * a.mt + n, k * step_blocks<MIXED>(a, m, n), a.abort_flag, a.status,
+                        a.dep_limit_ns);
     default:
         atomicCAS(a.status, ST_OK, ST_BAD_TASK);
         return false;
     }
 }
 
+// 16-bit stages follow the FP64 stages, 1024-byte aligned in the shared
+// window (128-byte swizzle atoms of 8 rows).
+__device__ __forceinline__ unsigned char *ring16_of(double *ring)
+{
+    unsigned char *p = reinterpret_cast<unsigned char *>(ring + NSTAGE_MIXED * STAGE_DOUBLES);
+    const uint32_t s = smem_u32(p);
+    return p + (((s + 1023u) & ~1023u) - s);
+}
+
 // ---------------------------------------------------------------------------
 // producer warp
 // ---------------------------------------------------------------------------
-__device__ void producer_warp(const PotrfArgs &a, SmemCtl *ctl, double *ring)
+template <bool MIXED>
+__device__ void producer_warp(const PotrfArgs &a, SmemCtl *ctl, double *ring, const CUtensorMap *tmap)
 {
+    constexpr uint32_t NST = MIXED ? NSTAGE_MIXED : NSTAGE;
     const int lane = threadIdx.x & 31;
-    uint32_t stage_it = 0, task_it = 0, epi_it = 0;
+    uint32_t stage_it = 0, task_it = 0, epi_it = 0, st16 = 0;
+    unsigned char *ring16 = MIXED ? ring16_of(ring) : nullptr;
+    if (MIXED && lane == 0) tma_prefetch_desc(tmap);
     bool pipe_ok = true;
     while (true) {
         int tk = -1;
@@ -66,7 +94,7 @@ __device__ void producer_warp(const PotrfArgs &a, SmemCtl *ctl, double *ring)
         int ok = 1;
         if (!end && lane == 0) {
             if (a.trace) a.trace[4 * (int64_t)tk + 0] = globaltimer_ns();
-            ok = wait_deps(a, t) ? 1 : 0;
+            ok = wait_deps<MIXED>(a, t) ? 1 : 0;
             if (a.trace) a.trace[4 * (int64_t)tk + 1] = globaltimer_ns();
             if (!ok && ld_volatile(a.status) == ST_DEP_TIMEOUT && a.diag[0] == 0) {
                 a.diag[0] = 7;
@@ -92,8 +120,9 @@ __device__ void producer_warp(const PotrfArgs &a, SmemCtl *ctl, double *ring)
         }
         task_it++;
         if (end) break;
-        if (task_type(t) == T_POTRF) {
-            // the consumers use the ring as scratch: wait until they are done
+        const int ty = task_type(t);
+        if (ty == T_POTRF) {
+            // POTRF uses the ring as scratch: wait until the consumers are done
             if (!warp_mbar_wait(&ctl->tempty[slot], round & 1, a.pipe_limit_ns)) {
                 if (lane == 0) report(a, ST_MBAR_TIMEOUT, 2, task_it, tk);
                 pipe_ok = false;
@@ -103,6 +132,32 @@ __device__ void producer_warp(const PotrfArgs &a, SmemCtl *ctl, double *ring)
             continue;
         }
         fence_proxy_async();
+        if (MIXED && ty == T_GEMM) {
+            // 16-bit operands by TMA tensor loads (128B swizzle, canonical
+            // K-major UMMA layout): A = block row bi of P16(m,k), B = P16(n,k)
+            const int k = task_k(t), m = task_m(t), n = task_n(t), bi = task_bi(t);
+            const int rowA = (int)(lower_tile_index(m, k, a.mt) * a.nbi) + bi * BLK;
+            const int rowB = (int)(lower_tile_index(n, k, a.mt) * a.nbi);
+            for (int kc = 0; kc < a.nbi; kc += MX_KC) {
+                const uint32_t s = st16 % MX_NST, r = st16 / MX_NST;
+                if (r > 0 && !warp_mbar_wait(&ctl->empty16[s], (r - 1) & 1, a.pipe_limit_ns)) {
+                    if (lane == 0) report(a, ST_MBAR_TIMEOUT, 8, st16, tk);
+                    pipe_ok = false;
+                    break;
+                }
+                unsigned char *st = ring16 + s * MX_STAGE_BYTES;
+                if (lane == 0) {
+                    mbar_arrive_expect_tx(&ctl->full16[s], MX_STAGE_BYTES);
+                    tma_load_2d(st, tmap, kc, rowA, &ctl->full16[s]);
+                    tma_load_2d(st + MX_A_BYTES, tmap, kc, rowB, &ctl->full16[s]);
+                    tma_load_2d(st + MX_A_BYTES + BLK * 128, tmap, kc, rowB + BLK, &ctl->full16[s]);
+                }
+                __syncwarp();
+                st16++;
+            }
+            if (!pipe_ok) break;
+            continue;
+        }
         const int nj = task_njobs(a, t);
         bool prev_signal = false;
         for (int j = 0; j < nj && pipe_ok; ++j) {
@@ -117,7 +172,7 @@ __device__ void producer_warp(const PotrfArgs &a, SmemCtl *ctl, double *ring)
                 fence_proxy_async();
             }
             for (int k0 = 0; k0 < jb.K; k0 += BK) {
-                const uint32_t s = stage_it % NSTAGE, r = stage_it / NSTAGE;
+                const uint32_t s = stage_it % NST, r = stage_it / NST;
                 if (r > 0 && !warp_mbar_wait(&ctl->empty[s], (r - 1) & 1, a.pipe_limit_ns)) {
                     if (lane == 0) report(a, ST_MBAR_TIMEOUT, 4, stage_it, tk);
                     pipe_ok = false;
@@ -138,25 +193,38 @@ __device__ void producer_warp(const PotrfArgs &a, SmemCtl *ctl, double *ring)
             prev_signal = jb.signal;
         }
         if (!pipe_ok) break;
+        if (MIXED && ty == T_TRSM) {
+            // the consumers re-lay the strip out through the ring after its
+            // jobs: no new FP64 stage may land before they are done
+            if (!warp_mbar_wait(&ctl->tempty[slot], round & 1, a.pipe_limit_ns)) {
+                if (lane == 0) report(a, ST_MBAR_TIMEOUT, 2, task_it, tk);
+                pipe_ok = false;
+                break;
+            }
+        }
     }
     if (!pipe_ok) {
         // Error path: tell the consumers to stop, then let the copies already
         // issued land before the CTA can exit.
-        if (lane == 0) {
-            atomicExch(a.abort_flag, 1);
+        if (lane == 0) atomicExch(a.abort_flag, 1);
+        const uint32_t first = stage_it > NST ? stage_it - NST : 0;
+        for (uint32_t it = first; it < stage_it; ++it) warp_mbar_wait(&ctl->full[it % NST], (it / NST) & 1, a.pipe_limit_ns);
+        if (MIXED) {
+            const uint32_t f16 = st16 > MX_NST ? st16 - MX_NST : 0;
+            for (uint32_t it = f16; it < st16; ++it)
+                warp_mbar_wait(&ctl->full16[it % MX_NST], (it / MX_NST) & 1, a.pipe_limit_ns);
         }
-        const uint32_t first = stage_it > NSTAGE ? stage_it - NSTAGE : 0;
-        for (uint32_t it = first; it < stage_it; ++it)
-            warp_mbar_wait(&ctl->full[it % NSTAGE], (it / NSTAGE) & 1, a.pipe_limit_ns);
     }
 }
 
 // ---------------------------------------------------------------------------
-// consumers: one 128x128 GEMM job
+// consumers: one 128x128 FP64 GEMM job.  Returns false if a wait gave up.
 // ---------------------------------------------------------------------------
+template <bool MIXED>
 __device__ __forceinline__ bool consume_job(const PotrfArgs &a, SmemCtl *ctl, const double *ring, const Job &jb,
                                             uint32_t &stage_it)
 {
+    constexpr uint32_t NST = MIXED ? NSTAGE_MIXED : NSTAGE;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int g = lane >> 2, t = lane & 3;
     const int wm = warp & 1, wn = warp >> 1;
@@ -169,9 +237,10 @@ __device__ __forceinline__ bool consume_job(const PotrfArgs &a, SmemCtl *ctl, co
             for (int q = 0; q < 4; ++q) acc[mi][ni][q] = 0.0;
 
     for (int k0 = 0; k0 < jb.K; k0 += BK) {
-        const uint32_t s = stage_it % NSTAGE, r = stage_it / NSTAGE;
+        const uint32_t s = stage_it % NST, r = stage_it / NST;
         if (!warp_mbar_wait(&ctl->full[s], r & 1, a.pipe_limit_ns)) {
-            if (threadIdx.x == 0) report(a, ST_MBAR_TIMEOUT, 6, stage_it, task_type(0));
+            if (lane == 0) report(a, ST_MBAR_TIMEOUT, 6, stage_it, warp);
+            stage_it += (jb.K - k0) / BK;
             return false;
         }
         const double *As = ring + s * STAGE_DOUBLES + wm * 64 + g;
@@ -369,16 +438,151 @@ __device__ void potrf_task(const PotrfArgs &a, SmemCtl *ctl, double *ring, int k
 }
 
 // ---------------------------------------------------------------------------
-// consumers: task loop
+// mixed precision: 16-bit copy of a finished TRSM strip.  The strip (128 rows
+// of tile (m,k), FP64, column-major) is scaled by a power of two so that its
+// largest magnitude is at most p16_target, rounded to bf16/fp16 and stored
+// K-major (row r holds the nbi values of row r), the operand layout of the
+// tcgen05 update.  All 256 consumer threads; the FP64 ring is scratch.
 // ---------------------------------------------------------------------------
+__device__ void emit_p16_strip(const PotrfArgs &a, double *ring, int m, int k, int bi)
+{
+    const int tid = threadIdx.x;
+    const int nbi = a.nbi;
+    const double *X = tile_ptr(a, m, k) + bi * BLK;     // column stride nbi
+    double *red = ring;                                  // 8 partial maxima
+    float amax = 0.f;
+    for (int e = tid; e < BLK * nbi; e += NCONS) {
+        const int r = e % BLK, c = e / BLK;
+        amax = fmaxf(amax, (float)fabs(__ldcg(X + (int64_t)c * nbi + r)));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, o));
+    if ((tid & 31) == 0) red[tid >> 5] = amax;
+    named_bar_sync(1, NCONS);
+    amax = 0.f;
+#pragma unroll
+    for (int w = 0; w < NCONS / 32; ++w) amax = fmaxf(amax, (float)red[w]);
+    // power-of-two scale with amax * scale <= target
+    int e2 = 0;
+    if (amax > 0.f && isfinite(amax)) {
+        const float q = a.p16_target / amax;
+        if (isfinite(q)) {
+            frexpf(q, &e2);
+            e2 = max(-120, min(120, e2 - 1));
+        } else {
+            e2 = 120;
+        }
+    }
+    const float scale = ldexpf(1.f, e2);
+    const int64_t tile = lower_tile_index(m, k, a.mt);
+    if (tid == 0) a.scl[tile * a.nbs + bi] = scale;
+    // transpose through shared memory, 32 columns at a time
+    double *buf = ring + 64;                               // 128 x 33
+    unsigned short *P = reinterpret_cast<unsigned short *>(a.P16) + (tile * nbi + bi * BLK) * (int64_t)nbi;
+    for (int c0 = 0; c0 < nbi; c0 += 32) {
+        named_bar_sync(1, NCONS);
+        for (int e = tid; e < BLK * 32; e += NCONS) {
+            const int r = e % BLK, c = e / BLK;
+            buf[r * 33 + c] = __ldcg(X + (int64_t)(c0 + c) * nbi + r);
+        }
+        named_bar_sync(1, NCONS);
+        for (int e = tid; e < BLK * 32; e += NCONS) {
+            const int c = e % 32, r = e / 32;
+            const float v = (float)buf[r * 33 + c] * scale;
+            unsigned short h;
+            if (a.p16_fmt) h = __bfloat16_as_ushort(__float2bfloat16_rn(v));
+            else h = __half_as_ushort(__float2half_rn(v));
+            P[(int64_t)r * nbi + c0 + c] = h;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// mixed precision: one update task, C(m,n)[bi, :] -= P16(m,k)[bi] P16(n,k)^T
+// scaled back.  Warp 4 lane 0 issues tcgen05.mma (M=128, N=256, K=16) per
+// 16-bit stage and commits each stage to its empty barrier; warps 0-3 read
+// the 128x256 FP32 accumulator from TMEM (each its 32 lanes) and reduce it
+// into the FP64 tile in L2.  Returns false if a wait gave up.
+// ---------------------------------------------------------------------------
+__device__ bool mixed_update(const PotrfArgs &a, SmemCtl *ctl, unsigned char *ring16, uint64_t t, uint32_t &st16,
+                             uint32_t &mx_it)
+{
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int k = task_k(t), m = task_m(t), n = task_n(t), bi = task_bi(t);
+    const uint32_t tmem = ctl->tmem_base;
+    const int nchunks = a.nbi / MX_KC;
+    bool ok = true;
+    if (warp == 4) {
+        if (lane == 0) {
+            const uint32_t idesc = umma_idesc_f16(a.p16_fmt, BLK, 256);
+            tc_fence_after();
+            uint32_t s16 = st16;
+            for (int kc = 0; kc < nchunks; ++kc, ++s16) {
+                const uint32_t s = s16 % MX_NST, r = s16 / MX_NST;
+                if (!mbar_wait(&ctl->full16[s], r & 1, a.pipe_limit_ns)) {
+                    report(a, ST_MBAR_TIMEOUT, 9, s16, tid);
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t sa = smem_u32(ring16 + s * MX_STAGE_BYTES), sb = sa + MX_A_BYTES;
+#pragma unroll
+                for (int k16 = 0; k16 < MX_KC / 16; ++k16)
+                    umma_f16(tmem, umma_desc_k_sw128(sa + k16 * 32), umma_desc_k_sw128(sb + k16 * 32), idesc,
+                             (kc | k16) != 0);
+                umma_commit(&ctl->empty16[s]);
+            }
+            // also on failure: the barrier then fires once the MMAs already
+            // issued are complete, so nothing is in flight at exit
+            umma_commit(&ctl->tmem_full);
+        }
+        ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+    }
+    st16 += nchunks;
+    if (warp < 4) {
+        if (!warp_mbar_wait(&ctl->tmem_full, mx_it & 1, a.pipe_limit_ns)) {
+            if (lane == 0) report(a, ST_MBAR_TIMEOUT, 10, mx_it, warp);
+            ok = false;
+        } else if (!__shfl_sync(0xffffffffu, ld_volatile(a.abort_flag), 0)) {
+            tc_fence_after();
+            const int64_t tk_a = lower_tile_index(m, k, a.mt), tk_b = lower_tile_index(n, k, a.mt);
+            const double sa = (double)a.scl[tk_a * a.nbs + bi];
+            const int row = warp * 32 + lane;                        // within the 128-row block
+            double *C = tile_ptr(a, m, n) + bi * BLK + row;            // column stride nbi
+            for (int c0 = 0; c0 < a.nbi; c0 += 32) {
+                float v[32];
+                tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
+                const double inv = 1.0 / (sa * (double)a.scl[tk_b * a.nbs + c0 / BLK]);   // power of two: exact
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    const int col = c0 + j;
+                    if (m != n || bi * BLK + row >= col) atomicAdd(C + (int64_t)col * a.nbi, -(double)v[j] * inv);
+                }
+            }
+            __threadfence();
+        }
+        tc_fence_before();
+    }
+    mx_it++;
+    return ok;
+}
+
+// ---------------------------------------------------------------------------
+// consumers: task loop.  Every decision to stop is taken after a barrier
+// that ORs the failure flags of all consumer warps, so no warp is ever left
+// waiting alone at a named barrier.
+// ---------------------------------------------------------------------------
+template <bool MIXED>
 __device__ void consumer_warps(const PotrfArgs &a, SmemCtl *ctl, double *ring)
 {
     const int tid = threadIdx.x;
-    uint32_t stage_it = 0, task_it = 0;
+    uint32_t stage_it = 0, task_it = 0, st16 = 0, mx_it = 0;
+    unsigned char *ring16 = MIXED ? ring16_of(ring) : nullptr;
     int executed = 0;
     while (true) {
         const uint32_t slot = task_it % TASKQ, round = task_it / TASKQ;
-        if (!warp_mbar_wait(&ctl->tfull[slot], round & 1, a.pipe_limit_ns)) {
+        const bool got = warp_mbar_wait(&ctl->tfull[slot], round & 1, a.pipe_limit_ns);
+        if (named_bar_or(1, NCONS, !got)) {
             if (tid == 0) report(a, ST_MBAR_TIMEOUT, 5, task_it, stage_it);
             break;
         }
@@ -397,25 +601,31 @@ __device__ void consumer_warps(const PotrfArgs &a, SmemCtl *ctl, double *ring)
         if (ty == T_POTRF) {
             potrf_task(a, ctl, ring, k);
             if (!ctl->fail) release = a.potrf_done + k;
+        } else if (MIXED && ty == T_GEMM) {
+            ok = mixed_update(a, ctl, ring16, t, st16, mx_it);
+            release = a.upd_done + (int64_t)m * a.mt + n;
         } else {
             const int nj = task_njobs(a, t);
-            for (int j = 0; j < nj && ok; ++j) {
+            for (int j = 0; j < nj; ++j) {
                 const Job jb = task_job(a, t, j);
-                ok = consume_job(a, ctl, ring, jb, stage_it);
-                if (ok && jb.signal) {
+                ok = consume_job<MIXED>(a, ctl, ring, jb, stage_it) && ok;
+                if (jb.signal) {
                     fence_proxy_async();
-                    named_bar_sync(1, NCONS);
+                    if (named_bar_or(1, NCONS, !ok)) {
+                        ok = false;
+                        break;
+                    }
                     if (tid == 0) mbar_arrive(&ctl->epi);
                 }
             }
+            if (MIXED && ty == T_TRSM && !named_bar_or(1, NCONS, !ok)) emit_p16_strip(a, ring, m, k, task_bi(t));
             release = (ty == T_TRSM) ? a.trsm_done + (int64_t)m * a.mt + k : a.upd_done + (int64_t)m * a.mt + n;
         }
-        if (!ok) {
+        fence_proxy_async();
+        if (named_bar_or(1, NCONS, !ok)) {
             atomicExch(a.abort_flag, 1);
             break;
         }
-        fence_proxy_async();
-        named_bar_sync(1, NCONS);
         if (tid == 0) {
             if (release) {
                 __threadfence();
@@ -438,13 +648,18 @@ __device__ void consumer_warps(const PotrfArgs &a, SmemCtl *ctl, double *ring)
 // (setmaxnreg.dec to PRODUCER_REGS) and the two consumer warpgroups take them
 // (setmaxnreg.inc to CONSUMER_REGS): 4*32*48 + 8*32*224 = 63488 <= 384*168, and
 // per sub-partition 1*32*48 + 2*32*224 = 15872 <= 16384.
-__global__ void __launch_bounds__(NTHREADS, 1) potrf_persistent_kernel(PotrfArgs a)
+// MIXED: the trailing updates run on the 16-bit tensor cores (tmap describes
+// the 16-bit panel copies); the FP64 instantiation ignores tmap.
+template <bool MIXED>
+__global__ void __launch_bounds__(NTHREADS, 1)
+    potrf_persistent_kernel(PotrfArgs a, const __grid_constant__ CUtensorMap tmap)
 {
-    extern __shared__ __align__(128) unsigned char smem_raw[];
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
     SmemCtl *ctl = reinterpret_cast<SmemCtl *>(smem_raw);
     double *ring = reinterpret_cast<double *>(smem_raw + ((sizeof(SmemCtl) + 127) / 128) * 128);
+    constexpr int NST = MIXED ? NSTAGE_MIXED : NSTAGE;
     if (threadIdx.x == 0) {
-        for (int s = 0; s < NSTAGE; ++s) {
+        for (int s = 0; s < NST; ++s) {
             mbar_init(&ctl->full[s], 1);
             mbar_init(&ctl->empty[s], NCONS / 32);
         }
@@ -452,26 +667,50 @@ __global__ void __launch_bounds__(NTHREADS, 1) potrf_persistent_kernel(PotrfArgs
             mbar_init(&ctl->tfull[s], 1);
             mbar_init(&ctl->tempty[s], 1);
         }
+        for (int s = 0; s < MX_NST; ++s) {
+            mbar_init(&ctl->full16[s], 1);
+            mbar_init(&ctl->empty16[s], 1);
+        }
+        mbar_init(&ctl->tmem_full, 1);
         mbar_init(&ctl->epi, 1);
         ctl->fail = 0;
+    }
+    if (MIXED && threadIdx.x < 32) {
+        tmem_alloc(&ctl->tmem_base, MX_TMEM_COLS);
+        tmem_relinquish();
+        tc_fence_before();
     }
     __syncthreads();
     if (threadIdx.x >= NCONS) {
         asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;\n" ::"n"(PRODUCER_REGS));
         if (threadIdx.x < NCONS + 32) {
-            producer_warp(a, ctl, ring);
+            producer_warp<MIXED>(a, ctl, ring, &tmap);
             if (a.trace && threadIdx.x == NCONS) a.trace_exit[6 * blockIdx.x] = globaltimer_ns();
         }
     } else {
         asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;\n" ::"n"(CONSUMER_REGS));
-        consumer_warps(a, ctl, ring);
+        if (MIXED) tc_fence_after();
+        consumer_warps<MIXED>(a, ctl, ring);
+        if (MIXED) {
+            // every consumer warp leaves the loop at the same point
+            tc_fence_before();
+            named_bar_sync(1, NCONS);
+            if (threadIdx.x < 32) {
+                tc_fence_after();
+                tmem_dealloc(ctl->tmem_base, MX_TMEM_COLS);
+            }
+        }
     }
 }
 
-size_t potrf_smem_bytes()
+size_t potrf_smem_bytes(bool mixed)
 {
-    return ((sizeof(SmemCtl) + 127) / 128) * 128 + (size_t)NSTAGE * STAGE_DOUBLES * sizeof(double);
+    const size_t ctl = ((sizeof(SmemCtl) + 127) / 128) * 128;
+    if (!mixed) return ctl + (size_t)NSTAGE * STAGE_DOUBLES * sizeof(double);
+    // FP64 ring, then the 16-bit ring aligned to 1024 B (worst-case padding)
+    return ctl + (size_t)NSTAGE_MIXED * STAGE_DOUBLES * sizeof(double) + 1024 + (size_t)MX_NST * MX_STAGE_BYTES;
 }
+size_t potrf_smem_bytes() { return potrf_smem_bytes(false); }
 
 // ---------------------------------------------------------------------------
 // host: ticket order
@@ -481,13 +720,16 @@ size_t potrf_smem_bytes()
 // TRSM(*,k+1), the rest of the step-k update by increasing column.  Every
 // task's dependencies precede it, so CTAs that take tickets in order always
 // make progress (no co-residency assumption).
-std::vector<uint64_t> build_potrf_tasks(int mt, int nbs, int delay)
+// In the mixed-precision variant an update task covers a 128-row block of
+// the tile and all its columns (bj = 0).
+std::vector<uint64_t> build_potrf_tasks(int mt, int nbs, int delay, bool mixed)
 {
     std::vector<uint64_t> v;
+    const int nbj = mixed ? 1 : nbs;
     auto push_update_tile = [&](int m, int n, int k) {
         for (int bi = 0; bi < nbs; ++bi)
-            for (int bj = 0; bj < nbs; ++bj) {
-                if (m == n && bj > bi) continue;
+            for (int bj = 0; bj < nbj; ++bj) {
+                if (!mixed && m == n && bj > bi) continue;
                 v.push_back(make_task(T_GEMM, k, m, n, bi, bj));
             }
     };
@@ -505,8 +747,8 @@ std::vector<uint64_t> build_potrf_tasks(int mt, int nbs, int delay)
         for (int n = k + 2; n < mt; ++n)
             for (int m = n; m < mt; ++m)
                 for (int bi = 0; bi < nbs; ++bi)
-                    for (int bj = 0; bj < nbs; ++bj) {
-                        if (m == n && bj > bi) continue;
+                    for (int bj = 0; bj < nbj; ++bj) {
+                        if (!mixed && m == n && bj > bi) continue;
                         rest.push_back(make_task(T_GEMM, k, m, n, bi, bj));
                     }
         const size_t d = std::min<size_t>(rest.size(), (size_t)std::max(delay, 0));
@@ -520,20 +762,69 @@ std::vector<uint64_t> build_potrf_tasks(int mt, int nbs, int delay)
 // ---------------------------------------------------------------------------
 // host: run one factorization of the device tiles
 // ---------------------------------------------------------------------------
+// Tensor map of the 16-bit panel copies: rows of nbi elements (K-major), one
+// row per matrix row of every lower tile, boxes of 64 x 128 with 128-byte
+// swizzle (the canonical K-major UMMA operand layout).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static int make_p16_map(Context *ctx, CUtensorMap *map, void *P16, size_t rows, int nbi, int fmt)
+{
+    static EncodeTiledFn encode = nullptr;
+    if (!encode) {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn) {
+            ctx->set_error("cuTensorMapEncodeTiled is not available from the driver");
+            return DPLASMA_ERR_UNEXPECTED;
+        }
+        encode = (EncodeTiledFn)fn;
+    }
+    const cuuint64_t dims[2] = {(cuuint64_t)nbi, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)nbi * 2};
+    const cuuint32_t box[2] = {MX_KC, BLK};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult r = encode(map, fmt ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, P16, dims,
+                              strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        ctx->set_error("cuTensorMapEncodeTiled failed (%d)", (int)r);
+        return DPLASMA_ERR_UNEXPECTED;
+    }
+    return 0;
+}
+
 int potrf_device(Context *ctx, double *dA, int mt, int nbi, int nb_user, int n_user, int *info)
 {
+    return potrf_run(ctx, dA, mt, nbi, nb_user, n_user, info, -1);
+}
+
+// p16_fmt < 0: FP64 updates; 0: FP16 updates; 1: BF16 updates.
+int potrf_run(Context *ctx, double *dA, int mt, int nbi, int nb_user, int n_user, int *info, int p16_fmt)
+{
     const int nbs = nbi / BLK;
+    const bool mixed = p16_fmt >= 0;
     cudaStream_t st = ctx->stream;
-    const int grid = ctx->potrf_grid;
+    const int grid = mixed ? ctx->potrf_grid_mixed : ctx->potrf_grid;
+    if (mixed && nbi != MX_NB) {
+        ctx->set_error("mixed-precision factorization needs a 256-wide internal tile (got %d)", nbi);
+        return DPLASMA_ERR_NOT_SUPPORTED;
+    }
+    if (grid <= 0) {
+        ctx->set_error("persistent kernel does not fit on an SM");
+        return DPLASMA_ERR_UNEXPECTED;
+    }
     // task list (cached per shape)
-    if (ctx->task_mt != mt || ctx->task_nbs != nbs || ctx->task_delay != ctx->potrf_delay) {
-        std::vector<uint64_t> tasks = build_potrf_tasks(mt, nbs, ctx->potrf_delay);
+    if (ctx->task_mt != mt || ctx->task_nbs != nbs || ctx->task_delay != ctx->potrf_delay || ctx->task_mixed != mixed) {
+        std::vector<uint64_t> tasks = build_potrf_tasks(mt, nbs, ctx->potrf_delay, mixed);
         uint64_t *dt = (uint64_t *)ctx->buffer(BUF_TASKS, tasks.size() * sizeof(uint64_t));
         if (!dt) return DPLASMA_ERR_OUT_OF_RESOURCES;
         CK(cudaMemcpyAsync(dt, tasks.data(), tasks.size() * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
         ctx->task_mt = mt;
         ctx->task_nbs = nbs;
         ctx->task_delay = ctx->potrf_delay;
+        ctx->task_mixed = mixed;
         ctx->ntasks = (int)tasks.size();
     }
     double *W = (double *)ctx->buffer(BUF_W, (size_t)mt * nbs * BLK * BLK * sizeof(double));
@@ -572,11 +863,35 @@ int potrf_device(Context *ctx, double *dA, int mt, int nbi, int nb_user, int n_u
     }
     a.dep_limit_ns = ctx->dep_limit_ns;
     a.pipe_limit_ns = ctx->pipe_limit_ns;
+    a.P16 = nullptr;
+    a.scl = nullptr;
+    a.p16_target = 0.f;
+    a.p16_fmt = 0;
+    CUtensorMap tmap;
+    memset(&tmap, 0, sizeof(tmap));
+    if (mixed) {
+        const size_t ntl = (size_t)mt * (mt + 1) / 2;
+        const size_t pbytes = ntl * (size_t)nbi * nbi * 2, sbytes = ntl * nbs * sizeof(float);
+        unsigned char *pb = (unsigned char *)ctx->buffer(BUF_P16, pbytes + sbytes + 256);
+        if (!pb) return DPLASMA_ERR_OUT_OF_RESOURCES;
+        a.P16 = pb;
+        a.scl = (float *)(pb + ((pbytes + 255) / 256) * 256);
+        a.p16_fmt = p16_fmt;
+        // fp16: headroom below 65504; bf16 has the FP32 range
+        a.p16_target = p16_fmt ? 1.0f : 16384.0f;
+        const int e = make_p16_map(ctx, &tmap, pb, ntl * (size_t)nbi, nbi, p16_fmt);
+        if (e) return e;
+    }
 
-    const size_t smem = potrf_smem_bytes();
-    CK(cudaFuncSetAttribute(potrf_persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const size_t smem = potrf_smem_bytes(mixed);
     CK(cudaEventRecord(ctx->ev0, st));
-    potrf_persistent_kernel<<<grid, NTHREADS, smem, st>>>(a);
+    if (mixed) {
+        CK(cudaFuncSetAttribute(potrf_persistent_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        potrf_persistent_kernel<true><<<grid, NTHREADS, smem, st>>>(a, tmap);
+    } else {
+        CK(cudaFuncSetAttribute(potrf_persistent_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        potrf_persistent_kernel<false><<<grid, NTHREADS, smem, st>>>(a, tmap);
+    }
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->ev1, st));
     ctx->launches += 1;
@@ -634,16 +949,20 @@ int potrf_device(Context *ctx, double *dA, int mt, int nbi, int nb_user, int n_u
 }  // namespace db2
 
 namespace db2 {
-int potrf_max_blocks_per_sm()
+template <bool MIXED>
+static int max_blocks_per_sm()
 {
-    const size_t smem = potrf_smem_bytes();
-    if (cudaFuncSetAttribute(potrf_persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+    const size_t smem = potrf_smem_bytes(MIXED);
+    if (cudaFuncSetAttribute(potrf_persistent_kernel<MIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
         cudaSuccess)
         return 0;
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, potrf_persistent_kernel, NTHREADS, smem) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, potrf_persistent_kernel<MIXED>, NTHREADS, smem) != cudaSuccess)
+        return 0;
     return n;
 }
+int potrf_max_blocks_per_sm(bool mixed) { return mixed ? max_blocks_per_sm<true>() : max_blocks_per_sm<false>(); }
+int potrf_max_blocks_per_sm() { return max_blocks_per_sm<false>(); }
 }  // namespace db2
 
 // ---------------------------------------------------------------------------
@@ -726,11 +1045,17 @@ int potrf_launch_prealloc(cudaStream_t st, double *dA, int mt, int nbi, int nb_u
     a.trace_cta = nullptr;
     a.dep_limit_ns = limit_ns;
     a.pipe_limit_ns = limit_ns;
-    const size_t smem = potrf_smem_bytes();
-    if (cudaFuncSetAttribute(potrf_persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+    a.P16 = nullptr;
+    a.scl = nullptr;
+    a.p16_target = 0.f;
+    a.p16_fmt = 0;
+    CUtensorMap tmap;
+    memset(&tmap, 0, sizeof(tmap));
+    const size_t smem = potrf_smem_bytes(false);
+    if (cudaFuncSetAttribute(potrf_persistent_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
         cudaSuccess)
         return DPLASMA_ERR_UNEXPECTED;
-    potrf_persistent_kernel<<<grid, NTHREADS, smem, st>>>(a);
+    potrf_persistent_kernel<false><<<grid, NTHREADS, smem, st>>>(a, tmap);
     if (cudaGetLastError() != cudaSuccess) return DPLASMA_ERR_UNEXPECTED;
     int hs[8];
     if (cudaMemcpyAsync(hs, ctr, sizeof(hs), cudaMemcpyDeviceToHost, st) != cudaSuccess) return DPLASMA_ERR_UNEXPECTED;

@@ -40,6 +40,19 @@ constexpr int CONSUMER_REGS = 224;
 constexpr int TASKQ = 4;         // task ring depth
 constexpr int STAGE_DOUBLES = 2 * BK * SP;
 
+// Mixed-precision variant (16-bit tensor-core updates, nbi = 256): the FP64
+// ring keeps NSTAGE_MIXED stages for the TRSM jobs, and a second ring holds
+// MX_NST stages of 16-bit operands, each A (128 rows x MX_KC) and B (256 rows
+// x MX_KC) in the 128-byte-swizzled K-major layout of the UMMA descriptors.
+constexpr int NSTAGE_MIXED = 3;
+constexpr int MX_KC = 64;                          // K per 16-bit stage (one 128-byte row)
+constexpr int MX_NST = 2;
+constexpr int MX_A_BYTES = BLK * MX_KC * 2;        // 16 KB
+constexpr int MX_B_BYTES = 2 * BLK * MX_KC * 2;    // 32 KB
+constexpr int MX_STAGE_BYTES = MX_A_BYTES + MX_B_BYTES;
+constexpr int MX_TMEM_COLS = 256;                  // 128 x 256 FP32 accumulator
+constexpr int MX_NB = 256;
+
 // Task encoding (64 bits): type[0:4) k[4:20) m[20:36) n[36:52) bi[52:56) bj[56:60)
 enum : int { T_END = 0, T_POTRF = 1, T_TRSM = 2, T_GEMM = 3 };
 __host__ __device__ __forceinline__ uint64_t make_task(int type, int k, int m, int n, int bi, int bj)
@@ -76,6 +89,12 @@ struct PotrfArgs {
     int *trace_cta;        // CTA that ran each ticket
     uint64_t dep_limit_ns; // bounded dependency waits
     uint64_t pipe_limit_ns;// bounded pipeline waits
+    // mixed precision: 16-bit K-major copies of the panel tiles and their
+    // power-of-two scales (per tile and 128-row block)
+    void *P16;
+    float *scl;
+    float p16_target;      // largest |value| a 16-bit panel block is scaled to
+    int p16_fmt;           // 1: bf16, 0: fp16
 };
 
 __device__ __forceinline__ double *tile_ptr(const PotrfArgs &a, int m, int n)
@@ -155,9 +174,13 @@ struct __align__(16) SmemCtl {
     uint64_t tempty[TASKQ];
     uint64_t epi;
     uint64_t task[TASKQ];
+    uint64_t full16[MX_NST];
+    uint64_t empty16[MX_NST];
+    uint64_t tmem_full;
     int tick[TASKQ];
     int fail;
-    int pad[3];
+    uint32_t tmem_base;
+    int pad[2];
 };
 
 }  // namespace db2

@@ -1,0 +1,598 @@
+// refine.cu -- mixed-precision solve with FP64 iterative refinement.
+//
+// The factor comes from the persistent Cholesky kernel with its trailing
+// updates on the FP16/BF16 tensor cores (FP64 diagonal factorizations and
+// panel solves, FP32 accumulation, per-block power-of-two scales).  The
+// refinement works in FP64 against an untouched copy of A, as LAPACK dsposv
+// (declared in src/include/lapacke.h:2987 of the reference) does:
+//
+//     x = L^-T L^-1 b;  repeat  r = b - A x;  converged if every column has
+//     ||r||_inf < ||x||_inf ||A||_inf eps sqrt(n);  x += L^-T L^-1 r
+//
+// with up to `itermax` (30) iterations before falling back to the FP64
+// factorization.  GMRES-IR replaces the correction solve by GMRES on
+// L^-T L^-1 A d = L^-T L^-1 r (left-preconditioned, FP64), which converges
+// for condition numbers where plain refinement stagnates.
+//
+// Device kernels here: the symmetric tile product out += alpha A x (FP64
+// DMMA, one CTA per lower tile, panels streamed by bulk copies), column norms,
+// column dot products and the small vector updates of GMRES.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "dev_common.cuh"
+#include "internal.h"
+
+namespace db2 {
+
+// ---------------------------------------------------------------------------
+// out[:, 0:nc] += alpha * A * in[:, 0:nc]   (A symmetric, lower tiles, nbi = 256)
+// ---------------------------------------------------------------------------
+constexpr int SY_NBI = 256;
+constexpr int SY_PC = 16;                 // columns per panel
+constexpr int SY_NST = 3;                 // panel stages
+constexpr int SY_PP = SY_NBI + 4;         // panel pitch (doubles), == 4 mod 16: conflict-free fragments
+constexpr int SY_NC = 16;                 // right-hand-side columns per launch
+constexpr int SY_THREADS = 256;
+constexpr size_t SY_SMEM = (size_t)(SY_NST * SY_PC * SY_PP + 2 * SY_NC * SY_PP + 2 * 8 * 256) * sizeof(double) + 64;
+
+__global__ void __launch_bounds__(SY_THREADS, 1)
+    symm_tiles_kernel(const double *__restrict__ A, int mt, const double *__restrict__ in, int ldin,
+                      double *__restrict__ out, int ldout, int nc, double alpha, int *status, uint64_t limit_ns)
+{
+    const int m = blockIdx.x, n = blockIdx.y;
+    if (m < n) return;
+    extern __shared__ __align__(16) double sy[];
+    double *P = sy;                                     // [stage][c][r]
+    double *Xn = P + SY_NST * SY_PC * SY_PP;            // [j][c]: in rows of tile column n
+    double *Xm = Xn + SY_NC * SY_PP;                    // [j][r]: in rows of tile row m
+    double *red = Xm + SY_NC * SY_PP;                   // [2][warp][lane*8]
+    uint64_t *full = reinterpret_cast<uint64_t *>(red + 2 * 8 * 256);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int g = lane >> 2, t = lane & 3;
+    const double *T = A + lower_tile_index(m, n, mt) * (int64_t)SY_NBI * SY_NBI;
+    constexpr int NP = SY_NBI / SY_PC;
+
+    if (tid == 0) {
+        for (int s = 0; s < SY_NST; ++s) mbar_init(&full[s], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (warp == 0) {
+        for (int s = 0; s < SY_NST; ++s) {
+            if (lane == 0) mbar_arrive_expect_tx(&full[s], SY_PC * SY_NBI * sizeof(double));
+            __syncwarp();
+            if (lane < SY_PC)
+                bulk_g2s(P + (s * SY_PC + lane) * SY_PP, T + (int64_t)(s * SY_PC + lane) * SY_NBI,
+                         SY_NBI * sizeof(double), &full[s]);
+        }
+    }
+    for (int e = tid; e < SY_NC * SY_NBI; e += SY_THREADS) {
+        const int j = e / SY_NBI, r = e % SY_NBI;
+        Xn[j * SY_PP + r] = j < nc ? in[(int64_t)j * ldin + (int64_t)n * SY_NBI + r] : 0.0;
+        Xm[j * SY_PP + r] = j < nc ? in[(int64_t)j * ldin + (int64_t)m * SY_NBI + r] : 0.0;
+    }
+    __syncthreads();
+
+    double ym[2][2][4];
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) ym[a][b][q] = 0.0;
+
+    for (int p = 0; p < NP; ++p) {
+        const int s = p % SY_NST;
+        const bool ok = mbar_wait(&full[s], (p / SY_NST) & 1, limit_ns);
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) {
+                atomicCAS(status, 0, 2);
+                // copies already issued must land before the CTA exits
+                for (int q = p; q < NP && q < p + SY_NST; ++q) mbar_wait(&full[q % SY_NST], (q / SY_NST) & 1, limit_ns);
+            }
+            return;
+        }
+        double *Ps = P + s * SY_PC * SY_PP;
+        const int c0 = p * SY_PC;
+        if (m == n) {
+            // symmetric use of the lower triangle: keep r > c, halve the diagonal
+            for (int e = tid; e < SY_PC * SY_NBI; e += SY_THREADS) {
+                const int c = e / SY_NBI, r = e % SY_NBI;
+                double &v = Ps[c * SY_PP + r];
+                if (r < c0 + c) v = 0.0;
+                else if (r == c0 + c) v *= 0.5;
+            }
+            __syncthreads();
+        }
+        // y_m(rows 32w..32w+31) += P(rows, 16 cols) * Xn(16 cols, j)
+#pragma unroll
+        for (int kk = 0; kk < SY_PC; kk += 4) {
+            double af[2][2], bf[2];
+#pragma unroll
+            for (int mi = 0; mi < 2; ++mi) {
+                af[mi][0] = Ps[(kk + t) * SY_PP + warp * 32 + mi * 16 + g];
+                af[mi][1] = Ps[(kk + t) * SY_PP + warp * 32 + mi * 16 + g + 8];
+            }
+#pragma unroll
+            for (int ni = 0; ni < 2; ++ni) bf[ni] = Xn[(ni * 8 + g) * SY_PP + c0 + kk + t];
+#pragma unroll
+            for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 2; ++ni) dmma_16x8x4(ym[mi][ni], af[mi][0], af[mi][1], bf[ni]);
+        }
+        // y_n(16 cols, j) partial over rows 32w..32w+31: P^T * Xm
+        double yn[2][4];
+#pragma unroll
+        for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) yn[ni][q] = 0.0;
+#pragma unroll
+        for (int kk = 0; kk < 32; kk += 4) {
+            const int r = warp * 32 + kk + t;
+            const double a0 = Ps[g * SY_PP + r], a1 = Ps[(g + 8) * SY_PP + r];
+#pragma unroll
+            for (int ni = 0; ni < 2; ++ni) dmma_16x8x4(yn[ni], a0, a1, Xm[(ni * 8 + g) * SY_PP + r]);
+        }
+        double *rb = red + (p & 1) * (8 * 256) + warp * 256 + lane * 8;
+#pragma unroll
+        for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) rb[ni * 4 + q] = yn[ni][q];
+        fence_proxy_async();   // the diagonal fix-up wrote stage s through the generic proxy
+        __syncthreads();       // stage s and this panel's partials are complete
+        if (warp == 0 && p + SY_NST < NP) {
+            const int pn = p + SY_NST;
+            if (lane == 0) mbar_arrive_expect_tx(&full[s], SY_PC * SY_NBI * sizeof(double));
+            __syncwarp();
+            if (lane < SY_PC)
+                bulk_g2s(Ps + lane * SY_PP, T + (int64_t)(pn * SY_PC + lane) * SY_NBI, SY_NBI * sizeof(double),
+                         &full[s]);
+        }
+        {
+            // thread -> (lane l, register q): output column c, rhs j
+            const int l = tid & 31, ni = (tid >> 5) & 1, q = (tid >> 6) & 3;
+            const double *rr = red + (p & 1) * (8 * 256) + l * 8 + ni * 4 + q;
+            double v = 0.0;
+#pragma unroll
+            for (int w = 0; w < 8; ++w) v += rr[w * 256];
+            const int gg = l >> 2, tt = l & 3;
+            const int c = gg + ((q & 2) ? 8 : 0), j = ni * 8 + 2 * tt + (q & 1);
+            if (j < nc) atomicAdd(out + (int64_t)j * ldout + (int64_t)n * SY_NBI + c0 + c, alpha * v);
+        }
+    }
+#pragma unroll
+    for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int r = warp * 32 + mi * 16 + g + ((q & 2) ? 8 : 0);
+                const int j = ni * 8 + 2 * t + (q & 1);
+                if (j < nc) atomicAdd(out + (int64_t)j * ldout + (int64_t)m * SY_NBI + r, alpha * ym[mi][ni][q]);
+            }
+}
+
+int symm_tiles(Context *ctx, const double *dA, const Geom &g, const double *in, int ldin, double *out, int ldout,
+               int ncols, double alpha, int *status)
+{
+    if (g.nbi != SY_NBI) {
+        ctx->set_error("symmetric tile product supports 256-wide internal tiles only");
+        return DPLASMA_ERR_NOT_SUPPORTED;
+    }
+    CK(cudaFuncSetAttribute(symm_tiles_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SY_SMEM));
+    for (int c0 = 0; c0 < ncols; c0 += SY_NC) {
+        const int nc = std::min(SY_NC, ncols - c0);
+        symm_tiles_kernel<<<dim3(g.mt, g.mt), SY_THREADS, SY_SMEM, ctx->stream>>>(
+            dA, g.mt, in + (size_t)c0 * ldin, ldin, out + (size_t)c0 * ldout, ldout, nc, alpha, status,
+            ctx->pipe_limit_ns);
+        CK(cudaGetLastError());
+        ctx->launches++;
+    }
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// column reductions and updates on (rows x ncols) column-major arrays
+// ---------------------------------------------------------------------------
+// stats[j] = {max |x_j|, sum x_j^2}; the max is an atomic on the bit pattern
+// of a non-negative double (monotone in its integer order).
+__global__ void col_stats_kernel(const double *__restrict__ X, int ld, int rows, int ncols, double *stats)
+{
+    const int j = blockIdx.y;
+    double mx = 0.0, ss = 0.0;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x) {
+        const double v = X[(int64_t)j * ld + r];
+        mx = fmax(mx, fabs(v));
+        if (v != v) mx = INFINITY;   // NaN stops the refinement
+        ss = fma(v, v, ss);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        ss += __shfl_xor_sync(0xffffffffu, ss, o);
+    }
+    __shared__ double smx[32], sss[32];
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+        smx[w] = mx;
+        sss[w] = ss;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int i = 1; i < (int)(blockDim.x >> 5); ++i) {
+            mx = fmax(mx, smx[i]);
+            ss += sss[i];
+        }
+        atomicMax(reinterpret_cast<unsigned long long *>(stats + 2 * j), (unsigned long long)__double_as_longlong(mx));
+        atomicAdd(stats + 2 * j + 1, ss);
+    }
+}
+
+// H[i*ncols + j] += sum_r V_i[r, j] * w[r, j]   for i = blockIdx.z  (V_i = V + i*vstride)
+__global__ void col_dots_kernel(const double *__restrict__ V, size_t vstride, const double *__restrict__ w, int ld,
+                                int rows, int ncols, double *H)
+{
+    const int j = blockIdx.y, i = blockIdx.z;
+    const double *v = V + (size_t)i * vstride + (size_t)j * ld;
+    const double *x = w + (size_t)j * ld;
+    double s = 0.0;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x) s = fma(v[r], x[r], s);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    __shared__ double sm[32];
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int q = 1; q < (int)(blockDim.x >> 5); ++q) s += sm[q];
+        atomicAdd(H + (size_t)i * ncols + j, s);
+    }
+}
+
+// w[:, j] = w[:, j] * ws[j] + sum_{i<nv} V_i[:, j] * c[i*ncols + j]   (ws null: 1)
+__global__ void col_combine_kernel(double *__restrict__ w, int ld, int rows, int ncols, const double *__restrict__ ws,
+                                   const double *__restrict__ V, size_t vstride, int nv, const double *__restrict__ c)
+{
+    const int j = blockIdx.y;
+    const double sw = ws ? ws[j] : 1.0;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x) {
+        double acc = w[(size_t)j * ld + r] * sw;
+        for (int i = 0; i < nv; ++i) acc = fma(V[(size_t)i * vstride + (size_t)j * ld + r], c[(size_t)i * ncols + j], acc);
+        w[(size_t)j * ld + r] = acc;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host helpers
+// ---------------------------------------------------------------------------
+struct Vec {
+    double *p;
+    int ld, rows, ncols;
+};
+
+static int col_stats(Context *ctx, const Vec &x, double *dstats, std::vector<double> &hmax, std::vector<double> &hss)
+{
+    CK(cudaMemsetAsync(dstats, 0, 2 * x.ncols * sizeof(double), ctx->stream));
+    col_stats_kernel<<<dim3(std::max(1, ctx->sms * 2 / std::max(1, x.ncols)), x.ncols), 256, 0, ctx->stream>>>(
+        x.p, x.ld, x.rows, x.ncols, dstats);
+    CK(cudaGetLastError());
+    ctx->launches++;
+    std::vector<double> h(2 * x.ncols);
+    CK(cudaMemcpyAsync(h.data(), dstats, h.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    hmax.resize(x.ncols);
+    hss.resize(x.ncols);
+    for (int j = 0; j < x.ncols; ++j) {
+        hmax[j] = h[2 * j];
+        hss[j] = h[2 * j + 1];
+    }
+    return 0;
+}
+
+static int combine(Context *ctx, const Vec &w, const double *dws, const double *V, size_t vstride, int nv,
+                   const double *dc)
+{
+    col_combine_kernel<<<dim3(std::max(1, ctx->sms * 4 / std::max(1, w.ncols)), w.ncols), 256, 0, ctx->stream>>>(
+        w.p, w.ld, w.rows, w.ncols, dws, V, vstride, nv, dc);
+    CK(cudaGetLastError());
+    ctx->launches++;
+    return 0;
+}
+
+// Mixed-precision solve driver state (all device arrays padded: rows = npad).
+struct Refine {
+    Context *ctx;
+    Geom g;
+    const double *A0;      // FP64 matrix (lower tiles)
+    const double *L;       // factor
+    const double *W;       // inverses of its 128x128 diagonal blocks
+    int npad, nc, ld;
+    double *b, *x, *r;     // right-hand sides, solution, residual / correction
+    double *small;         // device scratch for reductions
+    int *status;
+};
+
+static int apply_prec(Refine &R, double *v)
+{
+    int rc;
+    if ((rc = trsm_sweep(R.ctx, R.L, R.W, R.g, v, R.ld, R.nc, 0, 1.0))) return rc;
+    return trsm_sweep(R.ctx, R.L, R.W, R.g, v, R.ld, R.nc, 1, 1.0);
+}
+
+// r = b - A0 x
+static int residual(Refine &R)
+{
+    Context *ctx = R.ctx;
+    CK(cudaMemcpyAsync(R.r, R.b, (size_t)R.ld * R.nc * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    return symm_tiles(ctx, R.A0, R.g, R.x, R.ld, R.r, R.ld, R.nc, -1.0, R.status);
+}
+
+// GMRES on M^-1 A d = M^-1 r for all columns at once (each column its own
+// Krylov space), Arnoldi with classical Gram-Schmidt applied twice, at most
+// mmax steps.  On return R.r holds the correction d.  `tol` is relative to
+// ||M^-1 r||_2 per column.
+static int gmres_correction(Refine &R, double *Vbuf, int mmax, double tol, int *inner)
+{
+    Context *ctx = R.ctx;
+    const int nc = R.nc, ld = R.ld;
+    const size_t vs = (size_t)ld * nc;       // one basis block
+    Vec z{Vbuf, ld, R.npad, nc};
+    int rc;
+    // z = M^-1 r ; beta = ||z|| ; V_0 = z / beta
+    CK(cudaMemcpyAsync(Vbuf, R.r, vs * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    if ((rc = apply_prec(R, Vbuf))) return rc;
+    std::vector<double> mx, ss;
+    if ((rc = col_stats(ctx, z, R.small, mx, ss))) return rc;
+    std::vector<double> beta(nc), inv(nc);
+    for (int j = 0; j < nc; ++j) {
+        beta[j] = sqrt(ss[j]);
+        inv[j] = beta[j] > 0 ? 1.0 / beta[j] : 0.0;
+    }
+    double *dsc = R.small + 2 * nc;          // per-column scalars
+    double *dH = dsc + nc;                   // (mmax+1) x nc coefficients
+    CK(cudaMemcpyAsync(dsc, inv.data(), nc * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    if ((rc = combine(ctx, z, dsc, nullptr, 0, 0, nullptr))) return rc;
+
+    // Hessenberg per column (column-major (mmax+1) x mmax), Givens rotations
+    std::vector<double> H((size_t)nc * (mmax + 1) * mmax, 0.0), cs((size_t)nc * mmax), sn((size_t)nc * mmax);
+    std::vector<double> gv((size_t)nc * (mmax + 1), 0.0);
+    for (int j = 0; j < nc; ++j) gv[(size_t)j * (mmax + 1)] = beta[j];
+    std::vector<char> active(nc, 1);
+    for (int j = 0; j < nc; ++j)
+        if (beta[j] == 0.0) active[j] = 0;
+    int k = 0;
+    std::vector<double> h((size_t)(mmax + 1) * nc), h2((size_t)(mmax + 1) * nc), neg((size_t)(mmax + 1) * nc);
+    for (; k < mmax; ++k) {
+        bool any = false;
+        for (int j = 0; j < nc; ++j) any = any || active[j];
+        if (!any) break;
+        double *Vk = Vbuf + (size_t)k * vs, *Vn = Vbuf + (size_t)(k + 1) * vs;
+        // V_{k+1} = M^-1 A V_k
+        CK(cudaMemsetAsync(Vn, 0, vs * sizeof(double), ctx->stream));
+        if ((rc = symm_tiles(ctx, R.A0, R.g, Vk, ld, Vn, ld, nc, 1.0, R.status))) return rc;
+        if ((rc = apply_prec(R, Vn))) return rc;
+        Vec vn{Vn, ld, R.npad, nc};
+        std::fill(h.begin(), h.end(), 0.0);
+        for (int pass = 0; pass < 2; ++pass) {
+            CK(cudaMemsetAsync(dH, 0, (size_t)(k + 1) * nc * sizeof(double), ctx->stream));
+            col_dots_kernel<<<dim3(std::max(1, ctx->sms / std::max(1, nc)), nc, k + 1), 256, 0, ctx->stream>>>(
+                Vbuf, vs, Vn, ld, R.npad, nc, dH);
+            CK(cudaGetLastError());
+            ctx->launches++;
+            CK(cudaMemcpyAsync(h2.data(), dH, (size_t)(k + 1) * nc * sizeof(double), cudaMemcpyDeviceToHost,
+                               ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+            for (size_t q = 0; q < (size_t)(k + 1) * nc; ++q) {
+                h[q] += h2[q];
+                neg[q] = -h2[q];
+            }
+            CK(cudaMemcpyAsync(dH, neg.data(), (size_t)(k + 1) * nc * sizeof(double), cudaMemcpyHostToDevice,
+                               ctx->stream));
+            if ((rc = combine(ctx, vn, nullptr, Vbuf, vs, k + 1, dH))) return rc;
+        }
+        if ((rc = col_stats(ctx, vn, R.small, mx, ss))) return rc;
+        for (int j = 0; j < nc; ++j) {
+            double *Hj = H.data() + (size_t)j * (mmax + 1) * mmax + (size_t)k * (mmax + 1);
+            for (int i = 0; i <= k; ++i) Hj[i] = h[(size_t)i * nc + j];
+            const double hn = sqrt(ss[j]);
+            Hj[k + 1] = hn;
+            inv[j] = hn > 0 ? 1.0 / hn : 0.0;
+            // apply the previous rotations, then a new one
+            for (int i = 0; i < k; ++i) {
+                const double c = cs[(size_t)j * mmax + i], s = sn[(size_t)j * mmax + i];
+                const double t0 = c * Hj[i] + s * Hj[i + 1];
+                Hj[i + 1] = -s * Hj[i] + c * Hj[i + 1];
+                Hj[i] = t0;
+            }
+            const double a = Hj[k], b = Hj[k + 1];
+            const double d = hypot(a, b);
+            const double c = d > 0 ? a / d : 1.0, s = d > 0 ? b / d : 0.0;
+            cs[(size_t)j * mmax + k] = c;
+            sn[(size_t)j * mmax + k] = s;
+            Hj[k] = d;
+            Hj[k + 1] = 0.0;
+            double *gj = gv.data() + (size_t)j * (mmax + 1);
+            gj[k + 1] = -s * gj[k];
+            gj[k] = c * gj[k];
+            if (active[j] && (fabs(gj[k + 1]) <= tol * beta[j] || hn == 0.0)) active[j] = 0;
+        }
+        CK(cudaMemcpyAsync(dsc, inv.data(), nc * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        if ((rc = combine(ctx, vn, dsc, nullptr, 0, 0, nullptr))) return rc;
+        if (inner) ++*inner;
+    }
+    // y = H(0:k,0:k)^-1 g(0:k); d = V y.  Columns that met the tolerance
+    // early carry on with the others: more Arnoldi steps only lower their
+    // GMRES residual.
+    std::vector<double> y((size_t)k * nc, 0.0);
+    for (int j = 0; j < nc; ++j) {
+        const double *Hj = H.data() + (size_t)j * (mmax + 1) * mmax;
+        const double *gj = gv.data() + (size_t)j * (mmax + 1);
+        for (int i = k - 1; i >= 0; --i) {
+            double s = gj[i];
+            for (int l = i + 1; l < k; ++l) s -= Hj[(size_t)l * (mmax + 1) + i] * y[(size_t)l * nc + j];
+            const double d = Hj[(size_t)i * (mmax + 1) + i];
+            y[(size_t)i * nc + j] = d != 0.0 ? s / d : 0.0;
+        }
+    }
+    CK(cudaMemsetAsync(R.r, 0, vs * sizeof(double), ctx->stream));
+    if (k > 0) {
+        CK(cudaMemcpyAsync(dH, y.data(), (size_t)k * nc * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        Vec rv{R.r, ld, R.npad, nc};
+        if ((rc = combine(ctx, rv, nullptr, Vbuf, vs, k, dH))) return rc;
+    }
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// the driver
+// ---------------------------------------------------------------------------
+int refine_solve(Context *ctx, const double *A0, double *L, const Geom &g, double *b, double *x, int npad, int nc,
+                 const RefineOpts &o, RefineStats &st)
+{
+    int rc;
+    Refine R;
+    R.ctx = ctx;
+    R.g = g;
+    R.A0 = A0;
+    R.L = L;
+    R.W = nullptr;
+    R.npad = npad;
+    R.nc = nc;
+    R.ld = npad;
+    R.b = b;
+    R.x = x;
+    const size_t vs = (size_t)npad * nc;
+    const int mmax = std::max(1, o.gmres_m);
+    R.r = (double *)ctx->buffer(BUF_R, vs * sizeof(double));
+    const size_t nsmall = (size_t)(mmax + 4) * nc * 2 + 64;
+    R.small = (double *)ctx->buffer(BUF_SMALL, nsmall * sizeof(double));
+    if (!R.r || !R.small) return DPLASMA_ERR_OUT_OF_RESOURCES;
+    R.status = (int *)(R.small + nsmall - 8);
+    CK(cudaMemsetAsync(R.status, 0, sizeof(int), ctx->stream));
+
+    // own events: the factorization and the sweeps record the context's
+    struct Ev {
+        cudaEvent_t e[3] = {nullptr, nullptr, nullptr};
+        ~Ev()
+        {
+            for (auto v : e)
+                if (v) cudaEventDestroy(v);
+        }
+    } ev;
+    for (auto &v : ev.e) CK(cudaEventCreate(&v));
+    cudaEvent_t e0 = ev.e[0], e1 = ev.e[1], e2 = ev.e[2];
+    const double eps = ldexp(1.0, -53);
+    st.iter = 0;
+    st.inner_iters = 0;
+    st.fallback = 0;
+    st.solver_used = 1;
+    st.backward_error = 0.0;
+    st.factor_ms = st.refine_ms = 0.0;
+
+    // ||A||_inf of the FP64 matrix
+    double *dnorm = (double *)ctx->buffer(BUF_NORM, 64 * sizeof(double));
+    if (!dnorm) return DPLASMA_ERR_OUT_OF_RESOURCES;
+    if ((rc = lansy_inf_device(ctx, A0, g, dnorm))) return rc;
+    double anrm = 0.0;
+    CK(cudaMemcpyAsync(&anrm, dnorm, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    const double cte = anrm * eps * sqrt((double)g.n) * o.bwd_factor;
+
+    // mixed factorization of the working copy
+    CK(cudaEventRecord(e0, ctx->stream));
+    CK(cudaMemcpyAsync(L, A0, g.elems() * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    int info = 0;
+    if ((rc = potrf_run(ctx, L, g.mt, g.nbi, g.nb, g.n, &info, o.fmt))) return rc;
+    CK(cudaEventRecord(e1, ctx->stream));
+    R.W = (const double *)ctx->buffer(BUF_W, 0);
+
+    std::vector<double> xmax, xss, rmax, rss, bmax, bss;
+    Vec xv{x, npad, npad, nc}, rv{R.r, npad, npad, nc}, bv{b, npad, npad, nc};
+    if ((rc = col_stats(ctx, bv, R.small, bmax, bss))) return rc;
+    std::vector<double> ones(nc, 1.0);
+    bool converged = false;
+    double *Vbuf = nullptr;
+    if (info == 0) {
+        // x = M^-1 b
+        CK(cudaMemcpyAsync(x, b, vs * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+        if ((rc = apply_prec(R, x))) return rc;
+        int solver = o.solver == 2 ? 2 : 1;
+        double prev = INFINITY;
+        for (int it = 0; it <= o.itermax; ++it) {
+            if ((rc = residual(R))) return rc;
+            if ((rc = col_stats(ctx, xv, R.small, xmax, xss)) || (rc = col_stats(ctx, rv, R.small, rmax, rss))) return rc;
+            int ist = 0;
+            CK(cudaMemcpy(&ist, R.status, sizeof(int), cudaMemcpyDeviceToHost));
+            if (ist) {
+                ctx->set_error("symmetric tile product: pipeline wait timed out");
+                return DPLASMA_ERR_UNEXPECTED;
+            }
+            bool all = true;
+            double worst = 0.0, bwd = 0.0;
+            for (int j = 0; j < nc; ++j) {
+                if (!(rmax[j] < xmax[j] * cte) && !(rmax[j] == 0.0)) all = false;
+                const double ratio = xmax[j] > 0 ? rmax[j] / xmax[j] : rmax[j];
+                worst = std::max(worst, ratio);
+                const double den = anrm * xmax[j] + bmax[j];
+                bwd = std::max(bwd, den > 0 ? rmax[j] / den : rmax[j]);
+            }
+            st.backward_error = bwd;
+            if (all) {
+                converged = true;
+                st.iter = it;
+                break;
+            }
+            if (it == o.itermax || !(worst < INFINITY)) break;
+            // plain refinement that stops contracting switches to GMRES-IR
+            if (o.solver == 0 && solver == 1 && it > 0 && !(worst < 0.5 * prev)) solver = 2;
+            prev = worst;
+            if (solver == 1) {
+                if ((rc = apply_prec(R, R.r))) return rc;
+            } else {
+                if (!Vbuf) {
+                    Vbuf = (double *)ctx->buffer(BUF_KRYLOV, (size_t)(mmax + 1) * vs * sizeof(double));
+                    if (!Vbuf) return DPLASMA_ERR_OUT_OF_RESOURCES;
+                }
+                if ((rc = gmres_correction(R, Vbuf, mmax, o.gmres_tol, &st.inner_iters))) return rc;
+            }
+            st.solver_used = std::max(st.solver_used, solver);
+            // x += d
+            CK(cudaMemcpyAsync(R.small, ones.data(), nc * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+            if ((rc = combine(ctx, xv, nullptr, R.r, 0, 1, R.small))) return rc;
+        }
+    }
+    if (!converged) {
+        // FP64 factorization of the working copy and a plain solve
+        st.fallback = 1;
+        st.iter = info != 0 ? -3 : -(o.itermax + 1);
+        CK(cudaMemcpyAsync(L, A0, g.elems() * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+        int info64 = 0;
+        if ((rc = potrf_run(ctx, L, g.mt, g.nbi, g.nb, g.n, &info64, -1))) return rc;
+        if (info64) return info64;
+        R.W = (const double *)ctx->buffer(BUF_W, 0);
+        CK(cudaMemcpyAsync(x, b, vs * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+        if ((rc = apply_prec(R, x))) return rc;
+        if ((rc = residual(R))) return rc;
+        if ((rc = col_stats(ctx, xv, R.small, xmax, xss)) || (rc = col_stats(ctx, rv, R.small, rmax, rss))) return rc;
+        double bwd = 0.0;
+        for (int j = 0; j < nc; ++j) {
+            const double den = anrm * xmax[j] + bmax[j];
+            bwd = std::max(bwd, den > 0 ? rmax[j] / den : rmax[j]);
+        }
+        st.backward_error = bwd;
+    }
+    CK(cudaEventRecord(e2, ctx->stream));
+    CK(cudaEventSynchronize(e2));
+    float f = 0.f, r2 = 0.f;
+    cudaEventElapsedTime(&f, e0, e1);
+    cudaEventElapsedTime(&r2, e1, e2);
+    st.factor_ms = f;
+    st.refine_ms = r2;
+    return 0;
+}
+
+}  // namespace db2

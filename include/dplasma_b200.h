@@ -202,6 +202,57 @@ double dplasma_dlansy(parsec_context_t *parsec, dplasma_enum_t ntype, dplasma_en
  * device looks the scratch up and should come before any stream capture. */
 int dplasma_b200_dpotrf_noalloc(void *stream, dplasma_enum_t uplo, parsec_tiled_matrix_t *A);
 
+/* ---- mixed precision ---------------------------------------------------- */
+/* Type of the tensor-core operands of the trailing updates. */
+#define DPLASMA_B200_FP16 0
+#define DPLASMA_B200_BF16 1
+/* Correction solver of the refinement. */
+#define DPLASMA_B200_IR_AUTO  0   /* plain refinement, GMRES-IR once it stops contracting */
+#define DPLASMA_B200_IR_PLAIN 1   /* x += L^-T L^-1 r */
+#define DPLASMA_B200_IR_GMRES 2   /* GMRES on L^-T L^-1 A d = L^-T L^-1 r */
+
+typedef struct dplasma_b200_refine_opts_s {
+    int    fmt;        /* DPLASMA_B200_FP16 or DPLASMA_B200_BF16 */
+    int    solver;     /* DPLASMA_B200_IR_* */
+    int    itermax;    /* refinement iterations before the FP64 fallback (LAPACK dsposv ITERMAX = 30) */
+    int    gmres_m;    /* largest Krylov dimension of one GMRES-IR correction */
+    double gmres_tol;  /* residual reduction asked of one GMRES-IR correction */
+    double bwdmax;     /* LAPACK dsposv BWDMAX: stop when ||r_j|| < ||x_j|| ||A|| eps sqrt(n) bwdmax */
+} dplasma_b200_refine_opts_t;
+
+typedef struct dplasma_b200_refine_stats_s {
+    int    iter;           /* LAPACK dsposv ITER: refinement steps, or -3 (low-precision factorization
+                              failed) / -(itermax+1) (no convergence): FP64 factorization used */
+    int    inner_iters;    /* GMRES iterations over all corrections */
+    int    fallback;       /* 1 when the FP64 factorization produced the solution */
+    int    solver_used;    /* highest DPLASMA_B200_IR_* used (1 plain, 2 GMRES) */
+    double backward_error; /* max_j ||b_j - A x_j||_inf / (||A||_inf ||x_j||_inf + ||b_j||_inf) */
+    double factor_ms;      /* device time of the mixed factorization (with its working copy) */
+    double refine_ms;      /* device time of the solves and refinement (and of a fallback) */
+} dplasma_b200_refine_stats_t;
+
+/* Defaults: FP16, IR_AUTO, itermax 30, gmres_m 30, gmres_tol 1e-4, bwdmax 1. */
+void dplasma_b200_refine_opts_default(dplasma_b200_refine_opts_t *opts);
+
+/* dplasma_dsposv: no dplasma counterpart; the argument meaning of LAPACK
+ * dsposv (LAPACKE_dsposv, src/include/lapacke.h:2987 of the reference).
+ * Solves A X = B for symmetric positive definite A with a factorization whose
+ * trailing updates run on the FP16 tensor cores, refined in FP64 to the
+ * dsposv accuracy, falling back to the FP64 factorization after 30
+ * non-converging steps.  A (N x N, tile nb with 128 < nb <= 256) is unchanged
+ * unless the fallback ran, in which case it holds the FP64 factor, as in
+ * dsposv; B is unchanged; X (N x NRHS, same tiling as B) receives the
+ * solution.  *iter as dsposv ITER.  Returns 0, INFO > 0 when A is not
+ * positive definite, or a negative code. */
+int dplasma_dsposv(parsec_context_t *parsec, dplasma_enum_t uplo, parsec_tiled_matrix_t *A,
+                   const parsec_tiled_matrix_t *B, parsec_tiled_matrix_t *X, int *iter);
+
+/* dplasma_dsposv with explicit options (NULL: defaults) and statistics
+ * (may be NULL). */
+int dplasma_b200_dsposv_ex(parsec_context_t *parsec, dplasma_enum_t uplo, parsec_tiled_matrix_t *A,
+                           const parsec_tiled_matrix_t *B, parsec_tiled_matrix_t *X,
+                           const dplasma_b200_refine_opts_t *opts, dplasma_b200_refine_stats_t *stats);
+
 /* ---- instrumentation ---------------------------------------------------- */
 /* Device time in milliseconds of the last factorization (CUDA events around
  * the scheduler launch only) and of the last triangular-solve pair. */

@@ -125,6 +125,21 @@ def test_argument_checks_without_a_device():
     br = db.desc_general(4, 100, 32, 32)
     assert L.dplasma_dtrsm(None, db.Right, db.Lower, db.NoTrans, db.NonUnit, 1.0, pd(d), pd(br)) == db.ERR_NOT_SUPPORTED
     assert L.dplasma_dplgsy(None, 1.0, 999, pd(d), 1) == -3
+    # mixed-precision solve: uplo first, then the options, then the context
+    x = db.desc_general(100, 4, 32, 32)
+    db.attach(x, np.zeros(db.desc_elems(x)))
+    it = ctypes.c_int(7)
+    assert L.dplasma_dsposv(None, 999, pd(d), pd(b), pd(x), pd(it)) == -1
+    o = db.RefineOpts()
+    L.dplasma_b200_refine_opts_default(pd(o))
+    assert (o.fmt, o.solver, o.itermax, o.gmres_m, o.gmres_tol, o.bwdmax) == (db.FP16, db.IR_AUTO, 30, 30, 1e-4, 1.0)
+    st = db.RefineStats()
+    bad = db.RefineOpts()
+    L.dplasma_b200_refine_opts_default(pd(bad))
+    bad.fmt = 5
+    assert L.dplasma_b200_dsposv_ex(None, db.Lower, pd(d), pd(b), pd(x), pd(bad), pd(st)) == db.ERR_ILLEGAL_VALUE
+    assert L.dplasma_b200_dsposv_ex(None, db.Lower, pd(d), pd(b), pd(x), pd(o), pd(st)) == db.ERR_NOT_INITIALIZED
+    assert L.dplasma_dsposv(None, db.Lower, pd(d), pd(b), pd(x), pd(it)) == db.ERR_NOT_INITIALIZED
     # valid arguments without a context
     assert L.dplasma_dpotrf(None, db.Lower, pd(d)) == db.ERR_NOT_INITIALIZED
     assert L.dplasma_dposv(None, db.Lower, pd(d), pd(b)) == db.ERR_NOT_INITIALIZED
