@@ -493,13 +493,9 @@ int refine_solve(Context *ctx, const double *A0, double *L, const Geom &g, doubl
     st.backward_error = 0.0;
     st.factor_ms = st.refine_ms = 0.0;
 
-    // ||A||_inf of the FP64 matrix
-    double *dnorm = (double *)ctx->buffer(BUF_NORM, 64 * sizeof(double));
-    if (!dnorm) return DPLASMA_ERR_OUT_OF_RESOURCES;
-    if ((rc = lansy_inf_device(ctx, A0, g, dnorm))) return rc;
+    // ||A||_inf of the FP64 matrix (to the host)
     double anrm = 0.0;
-    CK(cudaMemcpyAsync(&anrm, dnorm, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    if ((rc = lansy_inf_device(ctx, A0, g, &anrm))) return rc;
     const double cte = anrm * eps * sqrt((double)g.n) * o.bwd_factor;
 
     // mixed factorization of the working copy
