@@ -69,7 +69,7 @@ EXPORTS = (
     "dplasma_dpotrs", "dplasma_dposv", "dplasma_dtrsm", "dplasma_dplgsy", "dplasma_dplrnt", "dplasma_dlansy",
     "dplasma_b200_last_factor_ms", "dplasma_b200_last_solve_ms", "dplasma_b200_last_launches",
     "dplasma_b200_fp64_peak_tflops", "dplasma_b200_refine_opts_default", "dplasma_dsposv",
-    "dplasma_b200_dsposv_ex",
+    "dplasma_b200_dsposv_ex", "dplasma_b200_dplgsy_cond",
 )
 
 
@@ -113,6 +113,7 @@ def lib():
     L.dplasma_b200_last_launches.argtypes = [P]
     L.dplasma_b200_fp64_peak_tflops.restype = D
     L.dplasma_b200_fp64_peak_tflops.argtypes = [P]
+    L.dplasma_b200_dplgsy_cond.argtypes = [P, D, I, I, pd, U64]
     L.dplasma_b200_refine_opts_default.argtypes = [ctypes.POINTER(RefineOpts)]
     L.dplasma_dsposv.argtypes = [P, I, pd, pd, pd, ctypes.POINTER(I)]
     L.dplasma_b200_dsposv_ex.argtypes = [P, I, pd, pd, pd, ctypes.POINTER(RefineOpts), ctypes.POINTER(RefineStats)]
@@ -251,6 +252,9 @@ class Context:
 
     def dlansy(self, ntype: int, uplo: int, A: Desc) -> float:
         return lib().dplasma_dlansy(self.h, ntype, uplo, ctypes.byref(A))
+
+    def dplgsy_cond(self, kappa: float, nrefl: int, uplo: int, A: Desc, seed: int) -> int:
+        return lib().dplasma_b200_dplgsy_cond(self.h, kappa, nrefl, uplo, ctypes.byref(A), seed)
 
     def dsposv(self, uplo: int, A: Desc, B: Desc, X: Desc, fmt: int = FP16, solver: int = IR_AUTO,
                itermax: int = 30, gmres_m: int = 30, gmres_tol: float = 1e-4, bwdmax: float = 1.0):

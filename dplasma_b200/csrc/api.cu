@@ -563,3 +563,31 @@ extern "C" int dplasma_dsposv(parsec_context_t *parsec, dplasma_enum_t uplo, par
     if (iter) *iter = st.iter;
     return rc;
 }
+
+extern "C" int dplasma_b200_dplgsy_cond(parsec_context_t *parsec, double kappa, int nrefl, dplasma_enum_t uplo,
+                                        parsec_tiled_matrix_t *A, unsigned long long int seed)
+{
+    if (!(kappa >= 1.0)) return -2;
+    if (nrefl < 0) return -3;
+    if (uplo != dplasmaUpper && uplo != dplasmaLower) return -4;
+    if (!parsec) return DPLASMA_ERR_NOT_INITIALIZED;
+    int rc;
+    if ((rc = check_square("dplasma_b200_dplgsy_cond", A))) return rc;
+    Context *ctx = &parsec->impl;
+    cudaSetDevice(ctx->device);
+    ctx->launches = 0;
+    ctx->errmsg[0] = 0;
+    if (A->m == 0) return 0;
+    Geom g = make_geom(A->m, A->mb);
+    if (g.nbi != 256) {
+        ctx->set_error("dplasma_b200_dplgsy_cond needs a tile size nb with 128 < nb <= 256 (got %d)", g.nb);
+        return DPLASMA_ERR_NOT_SUPPORTED;
+    }
+    const bool inplace = in_place_ok(A, uplo, g);
+    double *dA = inplace ? (double *)A->mat : (double *)ctx->buffer(BUF_A, g.elems() * sizeof(double));
+    if (!dA) return DPLASMA_ERR_OUT_OF_RESOURCES;
+    if ((rc = generate_cond(ctx, dA, g, kappa, nrefl, seed))) return rc;
+    if (!inplace && (rc = download_sym(ctx, A, uplo, g, dA))) return rc;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}

@@ -136,6 +136,7 @@ struct RefineStats {
 };
 int refine_solve(Context *ctx, const double *A0, double *L, const Geom &g, double *b, double *x, int npad, int nc,
                  const RefineOpts &o, RefineStats &st);
+int generate_cond(Context *ctx, double *dA, const Geom &g, double kappa, int nrefl, unsigned long long seed);
 int symm_tiles(Context *ctx, const double *dA, const Geom &g, const double *in, int ldin, double *out, int ldout,
                int ncols, double alpha, int *status);
 

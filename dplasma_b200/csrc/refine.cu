@@ -303,6 +303,133 @@ static int combine(Context *ctx, const Vec &w, const double *dws, const double *
     return 0;
 }
 
+// ---------------------------------------------------------------------------
+// test matrices of prescribed condition: A = Q diag(sigma) Q^T, Q the product
+// of nrefl Householder reflectors I - 2 v v^T with random unit v, sigma
+// geometric from 1 to kappa.  Applied as two-sided rank-2 updates
+//     A <- A - 2 (v u^T + u v^T),  w = A v,  u = w - (v^T w) v
+// on the lower tiles (O(nrefl N^2) work).
+// ---------------------------------------------------------------------------
+// Internal row m*nbi + r holds the caller's row m*nb + r when r < nb; the
+// other rows are padding (identity in A, zero in vectors).
+__global__ void cond_diag_kernel(double *A, int mt, int nb, int nbi, int n, double kappa)
+{
+    const int64_t t = blockIdx.x;
+    // tile (m, nn) of packed index t
+    int nn = 0;
+    int64_t base = 0;
+    while (base + (mt - nn) <= t) {
+        base += mt - nn;
+        ++nn;
+    }
+    const int m = nn + (int)(t - base);
+    double *T = A + t * (int64_t)nbi * nbi;
+    for (int64_t e = threadIdx.x; e < (int64_t)nbi * nbi; e += blockDim.x) {
+        const int r = (int)(e % nbi), c = (int)(e / nbi);
+        double v = 0.0;
+        if (m == nn && r == c) {
+            const int i = m * nb + r;
+            v = (r < nb && i < n) ? (n > 1 ? pow(kappa, (double)i / (double)(n - 1)) : 1.0) : 1.0;
+        }
+        T[e] = v;
+    }
+}
+
+// v[i] ~ N(0,1) for i < n (Box-Muller on a counter hash), 0 in the padding
+__device__ __forceinline__ uint64_t mix64(uint64_t z)
+{
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+__global__ void cond_vec_kernel(double *v, int npad, int nb, int nbi, int n, uint64_t seed, int refl)
+{
+    for (int ip = blockIdx.x * blockDim.x + threadIdx.x; ip < npad; ip += gridDim.x * blockDim.x) {
+        double x = 0.0;
+        const int r = ip % nbi, i = (ip / nbi) * nb + r;
+        if (r < nb && i < n) {
+            const uint64_t h = mix64(seed * 0x100000001B3ull ^ ((uint64_t)refl << 40) ^ (uint64_t)i);
+            const uint64_t h2 = mix64(h);
+            const double u1 = ((double)(h >> 11) + 1.0) * 0x1.0p-53;   // (0, 1]
+            const double u2 = (double)(h2 >> 11) * 0x1.0p-53;           // [0, 1)
+            x = sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
+        }
+        v[ip] = x;
+    }
+}
+
+// A(lower tiles) -= 2 (v u^T + u v^T)
+__global__ void rank2_tiles_kernel(double *A, int mt, int nbi, const double *__restrict__ v,
+                                   const double *__restrict__ u)
+{
+    const int m = blockIdx.x, nn = blockIdx.y;
+    if (m < nn) return;
+    double *T = A + lower_tile_index(m, nn, mt) * (int64_t)nbi * nbi;
+    const double *vm = v + (int64_t)m * nbi, *um = u + (int64_t)m * nbi;
+    const double *vn = v + (int64_t)nn * nbi, *un = u + (int64_t)nn * nbi;
+    for (int r = threadIdx.x; r < nbi; r += blockDim.x) {
+        const double a = 2.0 * vm[r], b = 2.0 * um[r];
+        for (int c = 0; c < nbi; ++c) {
+            double *p = T + (int64_t)c * nbi + r;
+            *p = *p - (a * un[c] + b * vn[c]);
+        }
+    }
+}
+
+int generate_cond(Context *ctx, double *dA, const Geom &g, double kappa, int nrefl, unsigned long long seed)
+{
+    if (g.nbi != SY_NBI) {
+        ctx->set_error("conditioned generator needs 256-wide internal tiles");
+        return DPLASMA_ERR_NOT_SUPPORTED;
+    }
+    const int npad = g.mt * g.nbi;
+    double *v = (double *)ctx->buffer(BUF_B0, (size_t)npad * 8 * sizeof(double));
+    double *w = (double *)ctx->buffer(BUF_X, (size_t)npad * 8 * sizeof(double));
+    double *small = (double *)ctx->buffer(BUF_SMALL, 4096 * sizeof(double));
+    if (!v || !w || !small) return DPLASMA_ERR_OUT_OF_RESOURCES;
+    int *status = (int *)(small + 4000);
+    CK(cudaMemsetAsync(status, 0, sizeof(int), ctx->stream));
+    cond_diag_kernel<<<(unsigned)g.ntiles(), 256, 0, ctx->stream>>>(dA, g.mt, g.nb, g.nbi, g.n, kappa);
+    CK(cudaGetLastError());
+    ctx->launches++;
+    Vec vv{v, npad, npad, 1}, wv{w, npad, npad, 1};
+    std::vector<double> mx, ss;
+    int rc;
+    for (int r = 0; r < nrefl; ++r) {
+        cond_vec_kernel<<<ctx->sms * 4, 256, 0, ctx->stream>>>(v, npad, g.nb, g.nbi, g.n, seed, r);
+        CK(cudaGetLastError());
+        ctx->launches++;
+        if ((rc = col_stats(ctx, vv, small, mx, ss))) return rc;
+        const double inv = ss[0] > 0 ? 1.0 / sqrt(ss[0]) : 0.0;
+        CK(cudaMemcpyAsync(small + 8, &inv, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        if ((rc = combine(ctx, vv, small + 8, nullptr, 0, 0, nullptr))) return rc;
+        CK(cudaMemsetAsync(w, 0, (size_t)npad * sizeof(double), ctx->stream));
+        if ((rc = symm_tiles(ctx, dA, g, v, npad, w, npad, 1, 1.0, status))) return rc;
+        CK(cudaMemsetAsync(small + 16, 0, sizeof(double), ctx->stream));
+        col_dots_kernel<<<dim3(ctx->sms, 1, 1), 256, 0, ctx->stream>>>(v, 0, w, npad, npad, 1, small + 16);
+        CK(cudaGetLastError());
+        ctx->launches++;
+        double alpha = 0.0;
+        CK(cudaMemcpyAsync(&alpha, small + 16, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        const double na = -alpha;
+        CK(cudaMemcpyAsync(small + 24, &na, sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        if ((rc = combine(ctx, wv, nullptr, v, 0, 1, small + 24))) return rc;   // u = w - alpha v
+        rank2_tiles_kernel<<<dim3(g.mt, g.mt), 256, 0, ctx->stream>>>(dA, g.mt, g.nbi, v, w);
+        CK(cudaGetLastError());
+        ctx->launches++;
+    }
+    int ist = 0;
+    CK(cudaMemcpyAsync(&ist, status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (ist) {
+        ctx->set_error("symmetric tile product: pipeline wait timed out");
+        return DPLASMA_ERR_UNEXPECTED;
+    }
+    return 0;
+}
+
 // Mixed-precision solve driver state (all device arrays padded: rows = npad).
 struct Refine {
     Context *ctx;

@@ -234,6 +234,16 @@ typedef struct dplasma_b200_refine_stats_s {
 /* Defaults: FP16, IR_AUTO, itermax 30, gmres_m 30, gmres_tol 1e-4, bwdmax 1. */
 void dplasma_b200_refine_opts_default(dplasma_b200_refine_opts_t *opts);
 
+/* dplasma_b200_dplgsy_cond: no dplasma counterpart; a test-matrix generator
+ * beside dplasma_dplgsy for the mixed-precision solve.  Fills the symmetric
+ * matrix A = Q diag(sigma) Q^T, Q the product of `nrefl` Householder
+ * reflectors of random unit vectors drawn from `seed`, sigma geometric from
+ * 1 (first row) to kappa (last row), so that cond_2(A) = kappa.  Built on the
+ * GPU in FP64 by nrefl two-sided rank-2 updates.  A: N x N, tile nb with
+ * 128 < nb <= 256, `uplo` triangle written.  Returns 0 or a negative code. */
+int dplasma_b200_dplgsy_cond(parsec_context_t *parsec, double kappa, int nrefl, dplasma_enum_t uplo,
+                             parsec_tiled_matrix_t *A, unsigned long long int seed);
+
 /* dplasma_dsposv: no dplasma counterpart; the argument meaning of LAPACK
  * dsposv (LAPACKE_dsposv, src/include/lapacke.h:2987 of the reference).
  * Solves A X = B for symmetric positive definite A with a factorization whose

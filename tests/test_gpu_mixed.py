@@ -168,3 +168,19 @@ def test_dsposv_rejects_tile_size(gpu_ctx):
     A = oracle.dplgsy(N, NB, 3872, bump=float(N))
     rc, _, _, _, _ = run_dsposv(gpu_ctx, A, np.ones((N, 1)), NB, db.Lower)
     assert rc == db.ERR_NOT_SUPPORTED
+
+
+@pytest.mark.parametrize("N,NB,uplo", [(768, 256, db.Lower), (700, 200, db.Upper)])
+def test_dplgsy_cond_spectrum(gpu_ctx, N, NB, uplo):
+    # the generated matrix is symmetric with eigenvalues geomspace(1, kappa, N)
+    kappa = 1e4
+    d = db.desc_sym(N, NB, uplo)
+    buf = np.zeros(db.desc_elems(d))
+    db.attach(d, buf)
+    assert gpu_ctx.dplgsy_cond(kappa, 64, uplo, d, 7) == 0, gpu_ctx.last_error()
+    T = db.unpack(buf, d)
+    A = np.tril(T) + np.tril(T, -1).T if uplo == db.Lower else np.triu(T) + np.triu(T, 1).T
+    ev = np.linalg.eigvalsh(A)
+    assert np.allclose(ev, np.geomspace(1.0, kappa, N), rtol=1e-9, atol=1e-9 * kappa)
+    # not diagonal: the reflectors mixed the coordinates
+    assert np.abs(A - np.diag(np.diag(A))).max() > 1e-3
