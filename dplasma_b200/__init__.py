@@ -57,7 +57,7 @@ class RefineStats(ctypes.Structure):
                 ("refine_ms", ctypes.c_double)]
 
 
-FP16, BF16 = 0, 1
+FP16, BF16, FP16_SPLIT = 0, 1, 2
 IR_AUTO, IR_PLAIN, IR_GMRES = 0, 1, 2
 
 _lib = None

@@ -140,6 +140,7 @@ extern "C" parsec_context_t *dplasma_b200_init(int device)
     }
     ctx->potrf_grid = getenv_int("DPLASMA_B200_GRID", ctx->sms * occ);
     ctx->potrf_grid_mixed = ctx->sms * potrf_max_blocks_per_sm(true);
+    ctx->mx_chunk = getenv_int("DPLASMA_B200_MX_CHUNK", 4);
     ctx->potrf_delay = getenv_int("DPLASMA_B200_DELAY", 3 * ctx->potrf_grid);
     ctx->wave_occ = getenv_int("DPLASMA_B200_NO_WAVE", 0) ? 0 : wave_max_blocks_per_sm();
     int occs = sweep_max_blocks_per_sm();
@@ -486,7 +487,7 @@ extern "C" int dplasma_b200_dsposv_ex(parsec_context_t *parsec, dplasma_enum_t u
     dplasma_b200_refine_opts_t o;
     dplasma_b200_refine_opts_default(&o);
     if (opts) o = *opts;
-    if ((o.fmt != DPLASMA_B200_FP16 && o.fmt != DPLASMA_B200_BF16) || o.solver < 0 || o.solver > 2 ||
+    if ((o.fmt != DPLASMA_B200_FP16 && o.fmt != DPLASMA_B200_BF16 && o.fmt != DPLASMA_B200_FP16_SPLIT) || o.solver < 0 || o.solver > 2 ||
         o.itermax < 0 || o.gmres_m < 1 || o.gmres_m > 200 || !(o.gmres_tol > 0.0) || !(o.bwdmax > 0.0)) {
         dplasma_error("dplasma_dsposv", "illegal options");
         return DPLASMA_ERR_ILLEGAL_VALUE;

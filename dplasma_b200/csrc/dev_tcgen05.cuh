@@ -50,6 +50,18 @@ __device__ __forceinline__ uint64_t umma_desc_k_sw128(uint32_t smem_addr)
     d |= (uint64_t)2 << 61;                               // SWIZZLE_128B
     return d;
 }
+// The same for the 64-byte swizzle: rows of 64 B (32 16-bit elements of K),
+// 8-row groups 512 B apart, layout type 4 (SWIZZLE_64B).
+__device__ __forceinline__ uint64_t umma_desc_k_sw64(uint32_t smem_addr)
+{
+    uint64_t d = 0;
+    d |= (uint64_t)((smem_addr >> 4) & 0x3FFF);
+    d |= (uint64_t)1 << 16;
+    d |= (uint64_t)(512 >> 4) << 32;
+    d |= (uint64_t)1 << 46;
+    d |= (uint64_t)4 << 61;
+    return d;
+}
 // Instruction descriptor for kind::f16: FP32 accumulator, A and B of the
 // same 16-bit type (fmt 0 = F16, 1 = BF16), both K-major, M x N.
 __host__ __device__ constexpr uint32_t umma_idesc_f16(int fmt, int M, int N)

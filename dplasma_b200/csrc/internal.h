@@ -49,7 +49,8 @@ struct Context {
     void *bufs[BUF_COUNT] = {};
     size_t bufsz[BUF_COUNT] = {};
     int task_mt = -1, task_nbs = -1, task_delay = -1, ntasks = 0;
-    bool task_mixed = false;
+    int task_mixed = 0;                      // chunk size of the cached mixed task list (0: FP64 list)
+    int mx_chunk = 4;                        // panels per mixed-precision update task
     double last_factor_ms = 0.0, last_solve_ms = 0.0;
     int launches = 0;
     long long last_tasks_executed = 0;
@@ -101,7 +102,7 @@ Geom make_geom(int n, int nb);
 
 // potrf_kernel.cu
 int potrf_device(Context *ctx, double *dA, int mt, int nbi, int nb_user, int n_user, int *info);
-// p16_fmt < 0: FP64 updates; 0/1: FP16/BF16 tensor-core updates (nbi == 256)
+// p16_fmt < 0: FP64 updates; 0/1/2: FP16/BF16/split-FP16 tensor-core updates (nbi == 256)
 int potrf_run(Context *ctx, double *dA, int mt, int nbi, int nb_user, int n_user, int *info, int p16_fmt);
 int potrf_max_blocks_per_sm(bool mixed);
 

@@ -36,8 +36,16 @@ __device__ __forceinline__ void report(const PotrfArgs &a, int code, int site, i
 template <bool MIXED>
 __device__ __forceinline__ int step_blocks(const PotrfArgs &a, int m, int n)
 {
-    if (MIXED) return a.nbs;
     return (m == n) ? a.nbs * (a.nbs + 1) / 2 : a.nbs * a.nbs;
+}
+// Update tasks tile (m,n) receives in all: FP64, nbs*nbs blocks (or the lower
+// triangle of them) per step; mixed, one per 128-row block and chunk of
+// mx_chunk panels.
+template <bool MIXED>
+__device__ __forceinline__ int all_updates(const PotrfArgs &a, int m, int n)
+{
+    if (MIXED) return ((n + a.mx_chunk - 1) / a.mx_chunk) * a.nbs;
+    return n * step_blocks<MIXED>(a, m, n);
 }
 
 template <bool MIXED>
@@ -47,13 +55,22 @@ __device__ bool wait_deps(const PotrfArgs &a, uint64_t t)
     const int nbs = a.nbs;
     switch (task_type(t)) {
     case T_POTRF:
-        return wait_geq(a.upd_done + (int64_t)k * a.mt + k, k * step_blocks<MIXED>(a, k, k), a.abort_flag, a.status,
+        return wait_geq(a.upd_done + (int64_t)k * a.mt + k, all_updates<MIXED>(a, k, k), a.abort_flag, a.status,
                         a.dep_limit_ns);
     case T_TRSM:
         return wait_geq(a.potrf_done + k, 1, a.abort_flag, a.status, a.dep_limit_ns) &&
-               wait_geq(a.upd_done + (int64_t)m * a.mt + k, k * step_blocks<MIXED>(a, m, k), a.abort_flag, a.status,
+               wait_geq(a.upd_done + (int64_t)m * a.mt + k, all_updates<MIXED>(a, m, k), a.abort_flag, a.status,
                         a.dep_limit_ns);
     case T_GEMM:
+        if (MIXED) {
+            // chunk k of panels [k*S, min(k*S+S, n)): the last panel's strips
+            // imply the earlier ones (TRSM(m,j+1) follows the update of (m,j+1)
+            // by panel j, which read TRSM(m,j)); chunks of one tile in order
+            const int kl = min(k * a.mx_chunk + a.mx_chunk, n) - 1;
+            return wait_geq(a.trsm_done + (int64_t)m * a.mt + kl, nbs, a.abort_flag, a.status, a.dep_limit_ns) &&
+                   wait_geq(a.trsm_done + (int64_t)n * a.mt + kl, nbs, a.abort_flag, a.status, a.dep_limit_ns) &&
+                   wait_geq(a.upd_done + (int64_t)m * a.mt + n, k * nbs, a.abort_flag, a.status, a.dep_limit_ns);
+        }
         return wait_geq(a.trsm_done + (int64_t)m * a.mt + k, nbs, a.abort_flag, a.status, a.dep_limit_ns) &&
                wait_geq(a.trsm_done + (int64_t)n * a.mt + k, nbs, a.abort_flag, a.status, a.dep_limit_ns) &&
                wait_geq(a.upd_done + (int64_t)m * a.mt + n, k * step_blocks<MIXED>(a, m, n), a.abort_flag, a.status,
@@ -133,27 +150,43 @@ __device__ void producer_warp(const PotrfArgs &a, SmemCtl *ctl, double *ring, co
         }
         fence_proxy_async();
         if (MIXED && ty == T_GEMM) {
-            // 16-bit operands by TMA tensor loads (128B swizzle, canonical
-            // K-major UMMA layout): A = block row bi of P16(m,k), B = P16(n,k)
-            const int k = task_k(t), m = task_m(t), n = task_n(t), bi = task_bi(t);
-            const int rowA = (int)(lower_tile_index(m, k, a.mt) * a.nbi) + bi * BLK;
-            const int rowB = (int)(lower_tile_index(n, k, a.mt) * a.nbi);
-            for (int kc = 0; kc < a.nbi; kc += MX_KC) {
-                const uint32_t s = st16 % MX_NST, r = st16 / MX_NST;
-                if (r > 0 && !warp_mbar_wait(&ctl->empty16[s], (r - 1) & 1, a.pipe_limit_ns)) {
-                    if (lane == 0) report(a, ST_MBAR_TIMEOUT, 8, st16, tk);
-                    pipe_ok = false;
-                    break;
+            // 16-bit operands by TMA tensor loads (swizzled, canonical K-major
+            // UMMA layout): for every panel j of the chunk, A = block row bi of
+            // P16(m,j), B = P16(n,j); the split form adds the lo rows.
+            const int kc = task_k(t), m = task_m(t), n = task_n(t), bi = task_bi(t);
+            const int j0 = kc * a.mx_chunk, j1 = min(j0 + a.mx_chunk, n);
+            const int KC = a.mx_split ? MX_KC_SPLIT : MX_KC;
+            for (int j = j0; j < j1 && pipe_ok; ++j) {
+                const int rowA = (int)(lower_tile_index(m, j, a.mt) * a.nbi) + bi * BLK;
+                const int rowB = (int)(lower_tile_index(n, j, a.mt) * a.nbi);
+                for (int kx = 0; kx < a.nbi; kx += KC) {
+                    const uint32_t s = st16 % MX_NST, r = st16 / MX_NST;
+                    if (r > 0 && !warp_mbar_wait(&ctl->empty16[s], (r - 1) & 1, a.pipe_limit_ns)) {
+                        if (lane == 0) report(a, ST_MBAR_TIMEOUT, 8, st16, tk);
+                        pipe_ok = false;
+                        break;
+                    }
+                    unsigned char *st = ring16 + s * MX_STAGE_BYTES;
+                    if (lane == 0) {
+                        uint64_t *bar = &ctl->full16[s];
+                        mbar_arrive_expect_tx(bar, MX_STAGE_BYTES);
+                        if (!a.mx_split) {
+                            tma_load_2d(st, tmap, kx, rowA, bar);
+                            tma_load_2d(st + MX_A_BYTES, tmap, kx, rowB, bar);
+                            tma_load_2d(st + MX_A_BYTES + BLK * MX_KC * 2, tmap, kx, rowB + BLK, bar);
+                        } else {
+                            const int R = a.p16_rows;
+                            tma_load_2d(st, tmap, kx, rowA, bar);                                // A hi
+                            tma_load_2d(st + MX_SPLIT_BLOCK, tmap, kx, rowA + R, bar);           // A lo
+                            tma_load_2d(st + 2 * MX_SPLIT_BLOCK, tmap, kx, rowB, bar);           // B hi
+                            tma_load_2d(st + 3 * MX_SPLIT_BLOCK, tmap, kx, rowB + BLK, bar);
+                            tma_load_2d(st + 4 * MX_SPLIT_BLOCK, tmap, kx, rowB + R, bar);       // B lo
+                            tma_load_2d(st + 5 * MX_SPLIT_BLOCK, tmap, kx, rowB + R + BLK, bar);
+                        }
+                    }
+                    __syncwarp();
+                    st16++;
                 }
-                unsigned char *st = ring16 + s * MX_STAGE_BYTES;
-                if (lane == 0) {
-                    mbar_arrive_expect_tx(&ctl->full16[s], MX_STAGE_BYTES);
-                    tma_load_2d(st, tmap, kc, rowA, &ctl->full16[s]);
-                    tma_load_2d(st + MX_A_BYTES, tmap, kc, rowB, &ctl->full16[s]);
-                    tma_load_2d(st + MX_A_BYTES + BLK * 128, tmap, kc, rowB + BLK, &ctl->full16[s]);
-                }
-                __syncwarp();
-                st16++;
             }
             if (!pipe_ok) break;
             continue;
@@ -438,47 +471,60 @@ __device__ void potrf_task(const PotrfArgs &a, SmemCtl *ctl, double *ring, int k
 }
 
 // ---------------------------------------------------------------------------
+// mixed precision: power-of-two scales of the 16-bit panel copies, one per
+// tile row m and 128-row block b.  Every entry of row i of the factor obeys
+// |L(i,j)| <= sqrt(A(i,i)) (the squares of a row of L add up to A(i,i)), so a
+// scale chosen from the diagonal before the factorization bounds every panel
+// of that row: scl * max_i sqrt(A(i,i)) <= target.  One scale for all panels
+// lets an update task accumulate several panels in one tensor-memory sum.
+// ---------------------------------------------------------------------------
+__global__ void p16_scale_kernel(const double *A, int mt, int nbi, float target, float *scl)
+{
+    const int m = blockIdx.x, b = threadIdx.x >> 7, r = threadIdx.x & 127;   // blockDim = nbi
+    const double *T = A + lower_tile_index(m, m, mt) * (int64_t)nbi * nbi;
+    const int i = b * BLK + r;
+    float v = (float)sqrt(fmax(T[(int64_t)i * nbi + i], 0.0));
+    if (!(v == v)) v = INFINITY;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    __shared__ float wm[16];
+    if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (r == 0) {
+        float amax = 0.f;
+        for (int w = 0; w < 4; ++w) amax = fmaxf(amax, wm[b * 4 + w]);
+        int e2 = 0;
+        if (amax > 0.f && isfinite(amax)) {
+            const float q = target / amax;
+            if (isfinite(q)) {
+                frexpf(q, &e2);
+                e2 = max(-120, min(120, e2 - 1));
+            } else {
+                e2 = 120;
+            }
+        }
+        scl[m * (nbi / BLK) + b] = ldexpf(1.f, e2);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // mixed precision: 16-bit copy of a finished TRSM strip.  The strip (128 rows
-// of tile (m,k), FP64, column-major) is scaled by a power of two so that its
-// largest magnitude is at most p16_target, rounded to bf16/fp16 and stored
-// K-major (row r holds the nbi values of row r), the operand layout of the
-// tcgen05 update.  All 256 consumer threads; the FP64 ring is scratch.
+// of tile (m,k), FP64, column-major) is multiplied by its row scale, rounded
+// to bf16/fp16 (split form: hi + lo fp16) and stored K-major (row r holds
+// the nbi values of row r), the operand layout of the tcgen05 update.  All
+// 256 consumer threads; the FP64 ring is scratch.
 // ---------------------------------------------------------------------------
 __device__ void emit_p16_strip(const PotrfArgs &a, double *ring, int m, int k, int bi)
 {
     const int tid = threadIdx.x;
     const int nbi = a.nbi;
     const double *X = tile_ptr(a, m, k) + bi * BLK;     // column stride nbi
-    double *red = ring;                                  // 8 partial maxima
-    float amax = 0.f;
-    for (int e = tid; e < BLK * nbi; e += NCONS) {
-        const int r = e % BLK, c = e / BLK;
-        amax = fmaxf(amax, (float)fabs(__ldcg(X + (int64_t)c * nbi + r)));
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) amax = fmaxf(amax, __shfl_xor_sync(0xffffffffu, amax, o));
-    if ((tid & 31) == 0) red[tid >> 5] = amax;
-    named_bar_sync(1, NCONS);
-    amax = 0.f;
-#pragma unroll
-    for (int w = 0; w < NCONS / 32; ++w) amax = fmaxf(amax, (float)red[w]);
-    // power-of-two scale with amax * scale <= target
-    int e2 = 0;
-    if (amax > 0.f && isfinite(amax)) {
-        const float q = a.p16_target / amax;
-        if (isfinite(q)) {
-            frexpf(q, &e2);
-            e2 = max(-120, min(120, e2 - 1));
-        } else {
-            e2 = 120;
-        }
-    }
-    const float scale = ldexpf(1.f, e2);
+    const float scale = a.scl[m * a.nbs + bi];
     const int64_t tile = lower_tile_index(m, k, a.mt);
-    if (tid == 0) a.scl[tile * a.nbs + bi] = scale;
     // transpose through shared memory, 32 columns at a time
-    double *buf = ring + 64;                               // 128 x 33
+    double *buf = ring;                                    // 128 x 33
     unsigned short *P = reinterpret_cast<unsigned short *>(a.P16) + (tile * nbi + bi * BLK) * (int64_t)nbi;
+    unsigned short *Plo = P + (int64_t)a.p16_rows * nbi;  // split form: lo part
     for (int c0 = 0; c0 < nbi; c0 += 32) {
         named_bar_sync(1, NCONS);
         for (int e = tid; e < BLK * 32; e += NCONS) {
@@ -488,36 +534,53 @@ __device__ void emit_p16_strip(const PotrfArgs &a, double *ring, int m, int k, i
         named_bar_sync(1, NCONS);
         for (int e = tid; e < BLK * 32; e += NCONS) {
             const int c = e % 32, r = e / 32;
-            const float v = (float)buf[r * 33 + c] * scale;
+            const double xs = buf[r * 33 + c] * (double)scale;    // exact: power of two
             unsigned short h;
-            if (a.p16_fmt) h = __bfloat16_as_ushort(__float2bfloat16_rn(v));
-            else h = __half_as_ushort(__float2half_rn(v));
+            if (a.p16_fmt) {
+                h = __bfloat16_as_ushort(__float2bfloat16_rn((float)xs));
+            } else {
+                const __half hh = __float2half_rn((float)xs);
+                h = __half_as_ushort(hh);
+                if (a.mx_split) {
+                    // split FP16 (hi + lo): lo carries the next 11 bits of xs
+                    const double rem = xs - (double)__half2float(hh);
+                    Plo[(int64_t)r * nbi + c0 + c] = __half_as_ushort(__float2half_rn((float)rem));
+                }
+            }
             P[(int64_t)r * nbi + c0 + c] = h;
         }
     }
 }
 
 // ---------------------------------------------------------------------------
-// mixed precision: one update task, C(m,n)[bi, :] -= P16(m,k)[bi] P16(n,k)^T
-// scaled back.  Warp 4 lane 0 issues tcgen05.mma (M=128, N=256, K=16) per
-// 16-bit stage and commits each stage to its empty barrier; warps 0-3 read
-// the 128x256 FP32 accumulator from TMEM (each its 32 lanes) and reduce it
-// into the FP64 tile in L2.  Returns false if a wait gave up.
+// mixed precision: one update task,
+//     C(m,n)[bi, :] -= sum_{j in chunk} P16(m,j)[bi] P16(n,j)^T   (scaled back)
+// Warp 4 lane 0 issues tcgen05.mma (M=128, N=256, K=16) per 16-bit stage and
+// commits each stage to its empty barrier; the split form issues hi*hi,
+// hi*lo and lo*hi into the same FP32 accumulator (split-FP16 products as in
+// Ootomo and Yokota, 2022).  Then all eight consumer warps read the 128x256
+// accumulator from TMEM (warp w: lanes 32*(w%4).., columns 128*(w/4)..) and
+// update the FP64 tile in place: the chunks of one tile run one after the
+// other, so the load-subtract-store needs no atomics.  One accumulation per
+// chunk of panels divides the traffic on C by the chunk size.
+// Returns false if a wait gave up.
 // ---------------------------------------------------------------------------
 __device__ bool mixed_update(const PotrfArgs &a, SmemCtl *ctl, unsigned char *ring16, uint64_t t, uint32_t &st16,
                              uint32_t &mx_it)
 {
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int k = task_k(t), m = task_m(t), n = task_n(t), bi = task_bi(t);
+    const int kc = task_k(t), m = task_m(t), n = task_n(t), bi = task_bi(t);
+    const int j0 = kc * a.mx_chunk, j1 = min(j0 + a.mx_chunk, n);
     const uint32_t tmem = ctl->tmem_base;
-    const int nchunks = a.nbi / MX_KC;
+    const int KC = a.mx_split ? MX_KC_SPLIT : MX_KC;
+    const int nst = (j1 - j0) * (a.nbi / KC);
     bool ok = true;
     if (warp == 4) {
         if (lane == 0) {
             const uint32_t idesc = umma_idesc_f16(a.p16_fmt, BLK, 256);
             tc_fence_after();
             uint32_t s16 = st16;
-            for (int kc = 0; kc < nchunks; ++kc, ++s16) {
+            for (int i = 0; i < nst; ++i, ++s16) {
                 const uint32_t s = s16 % MX_NST, r = s16 / MX_NST;
                 if (!mbar_wait(&ctl->full16[s], r & 1, a.pipe_limit_ns)) {
                     report(a, ST_MBAR_TIMEOUT, 9, s16, tid);
@@ -525,11 +588,24 @@ __device__ bool mixed_update(const PotrfArgs &a, SmemCtl *ctl, unsigned char *ri
                     break;
                 }
                 tc_fence_after();
-                const uint32_t sa = smem_u32(ring16 + s * MX_STAGE_BYTES), sb = sa + MX_A_BYTES;
+                const uint32_t base = smem_u32(ring16 + s * MX_STAGE_BYTES);
+                if (!a.mx_split) {
+                    const uint32_t sb = base + MX_A_BYTES;
 #pragma unroll
-                for (int k16 = 0; k16 < MX_KC / 16; ++k16)
-                    umma_f16(tmem, umma_desc_k_sw128(sa + k16 * 32), umma_desc_k_sw128(sb + k16 * 32), idesc,
-                             (kc | k16) != 0);
+                    for (int k16 = 0; k16 < MX_KC / 16; ++k16)
+                        umma_f16(tmem, umma_desc_k_sw128(base + k16 * 32), umma_desc_k_sw128(sb + k16 * 32), idesc,
+                                 (i | k16) != 0);
+                } else {
+                    const uint32_t ah = base, al = base + MX_SPLIT_BLOCK, bh = base + 2 * MX_SPLIT_BLOCK,
+                                   bl = base + 4 * MX_SPLIT_BLOCK;
+#pragma unroll
+                    for (int k16 = 0; k16 < MX_KC_SPLIT / 16; ++k16) {
+                        const uint32_t o = k16 * 32;
+                        umma_f16(tmem, umma_desc_k_sw64(ah + o), umma_desc_k_sw64(bh + o), idesc, (i | k16) != 0);
+                        umma_f16(tmem, umma_desc_k_sw64(ah + o), umma_desc_k_sw64(bl + o), idesc, 1);
+                        umma_f16(tmem, umma_desc_k_sw64(al + o), umma_desc_k_sw64(bh + o), idesc, 1);
+                    }
+                }
                 umma_commit(&ctl->empty16[s]);
             }
             // also on failure: the barrier then fires once the MMAs already
@@ -538,31 +614,35 @@ __device__ bool mixed_update(const PotrfArgs &a, SmemCtl *ctl, unsigned char *ri
         }
         ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
     }
-    st16 += nchunks;
-    if (warp < 4) {
-        if (!warp_mbar_wait(&ctl->tmem_full, mx_it & 1, a.pipe_limit_ns)) {
-            if (lane == 0) report(a, ST_MBAR_TIMEOUT, 10, mx_it, warp);
-            ok = false;
-        } else if (!__shfl_sync(0xffffffffu, ld_volatile(a.abort_flag), 0)) {
-            tc_fence_after();
-            const int64_t tk_a = lower_tile_index(m, k, a.mt), tk_b = lower_tile_index(n, k, a.mt);
-            const double sa = (double)a.scl[tk_a * a.nbs + bi];
-            const int row = warp * 32 + lane;                        // within the 128-row block
-            double *C = tile_ptr(a, m, n) + bi * BLK + row;            // column stride nbi
-            for (int c0 = 0; c0 < a.nbi; c0 += 32) {
-                float v[32];
-                tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0, v);
-                const double inv = 1.0 / (sa * (double)a.scl[tk_b * a.nbs + c0 / BLK]);   // power of two: exact
+    st16 += nst;
+    if (!warp_mbar_wait(&ctl->tmem_full, mx_it & 1, a.pipe_limit_ns)) {
+        if (lane == 0) report(a, ST_MBAR_TIMEOUT, 10, mx_it, warp);
+        ok = false;
+    } else if (!__shfl_sync(0xffffffffu, ld_volatile(a.abort_flag), 0)) {
+        tc_fence_after();
+        const int lb = (warp & 3) * 32, half = warp >> 2;
+        const int row = lb + lane;                                 // within the 128-row block
+        double *C = tile_ptr(a, m, n) + bi * BLK + row;            // column stride nbi
+        for (int c0 = half * 128; c0 < half * 128 + 128; c0 += 32) {
+            float v[32];
+            tmem_ld32(tmem + ((uint32_t)lb << 16) + (uint32_t)c0, v);
+            // row scales are the same for every panel: one power of two per block
+            const double inv = 1.0 / ((double)a.scl[m * a.nbs + bi] * (double)a.scl[n * a.nbs + c0 / BLK]);
+            double cv[32];
 #pragma unroll
-                for (int j = 0; j < 32; ++j) {
-                    const int col = c0 + j;
-                    if (m != n || bi * BLK + row >= col) atomicAdd(C + (int64_t)col * a.nbi, -(double)v[j] * inv);
-                }
+            for (int j = 0; j < 32; ++j) {
+                const int col = c0 + j;
+                cv[j] = (m != n || bi * BLK + row >= col) ? __ldcg(C + (int64_t)col * a.nbi) : 0.0;
             }
-            __threadfence();
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+                const int col = c0 + j;
+                if (m != n || bi * BLK + row >= col) __stcg(C + (int64_t)col * a.nbi, cv[j] - (double)v[j] * inv);
+            }
         }
-        tc_fence_before();
+        __threadfence();
     }
+    tc_fence_before();
     mx_it++;
     return ok;
 }
@@ -720,16 +800,13 @@ size_t potrf_smem_bytes() { return potrf_smem_bytes(false); }
 // TRSM(*,k+1), the rest of the step-k update by increasing column.  Every
 // task's dependencies precede it, so CTAs that take tickets in order always
 // make progress (no co-residency assumption).
-// In the mixed-precision variant an update task covers a 128-row block of
-// the tile and all its columns (bj = 0).
-std::vector<uint64_t> build_potrf_tasks(int mt, int nbs, int delay, bool mixed)
+std::vector<uint64_t> build_potrf_tasks(int mt, int nbs, int delay)
 {
     std::vector<uint64_t> v;
-    const int nbj = mixed ? 1 : nbs;
     auto push_update_tile = [&](int m, int n, int k) {
         for (int bi = 0; bi < nbs; ++bi)
-            for (int bj = 0; bj < nbj; ++bj) {
-                if (!mixed && m == n && bj > bi) continue;
+            for (int bj = 0; bj < nbs; ++bj) {
+                if (m == n && bj > bi) continue;
                 v.push_back(make_task(T_GEMM, k, m, n, bi, bj));
             }
     };
@@ -747,10 +824,46 @@ std::vector<uint64_t> build_potrf_tasks(int mt, int nbs, int delay, bool mixed)
         for (int n = k + 2; n < mt; ++n)
             for (int m = n; m < mt; ++m)
                 for (int bi = 0; bi < nbs; ++bi)
-                    for (int bj = 0; bj < nbj; ++bj) {
-                        if (!mixed && m == n && bj > bi) continue;
+                    for (int bj = 0; bj < nbs; ++bj) {
+                        if (m == n && bj > bi) continue;
                         rest.push_back(make_task(T_GEMM, k, m, n, bi, bj));
                     }
+        const size_t d = std::min<size_t>(rest.size(), (size_t)std::max(delay, 0));
+        v.insert(v.end(), rest.begin(), rest.begin() + d);
+        push_trsm(k + 1);
+        v.insert(v.end(), rest.begin() + d, rest.end());
+    }
+    return v;
+}
+
+// Mixed-precision ticket order.  An update task (k = chunk c) applies the
+// panels j in [c*S, min(c*S+S, n)) to the 128-row block bi of tile (m,n).
+// Each tile column n gets one chunk task per block and chunk: a full chunk is
+// issued in the step that finishes its last panel, the partial chunk that
+// ends at panel n-1 in step n-1 (the critical column).  Step k: the critical
+// column k+1, POTRF(k+1), then (when panel k closes a chunk) that chunk for
+// all columns n >= k+2 -- column k+2 first -- with TRSM(*,k+1) after `delay`
+// of them.
+std::vector<uint64_t> build_potrf_tasks_mixed(int mt, int nbs, int delay, int S)
+{
+    std::vector<uint64_t> v;
+    auto push_trsm = [&](int k) {
+        for (int m = k + 1; m < mt; ++m)
+            for (int bi = 0; bi < nbs; ++bi) v.push_back(make_task(T_TRSM, k, m, k, bi, 0));
+    };
+    v.push_back(make_task(T_POTRF, 0, 0, 0, 0, 0));
+    push_trsm(0);
+    std::vector<uint64_t> rest;
+    for (int k = 0; k + 1 < mt; ++k) {
+        const int c = k / S;
+        for (int m = k + 1; m < mt; ++m)
+            for (int bi = 0; bi < nbs; ++bi) v.push_back(make_task(T_GEMM, c, m, k + 1, bi, 0));
+        v.push_back(make_task(T_POTRF, k + 1, k + 1, k + 1, 0, 0));
+        rest.clear();
+        if (k == c * S + S - 1)
+            for (int n = k + 2; n < mt; ++n)
+                for (int m = n; m < mt; ++m)
+                    for (int bi = 0; bi < nbs; ++bi) rest.push_back(make_task(T_GEMM, c, m, n, bi, 0));
         const size_t d = std::min<size_t>(rest.size(), (size_t)std::max(delay, 0));
         v.insert(v.end(), rest.begin(), rest.begin() + d);
         push_trsm(k + 1);
@@ -768,7 +881,7 @@ std::vector<uint64_t> build_potrf_tasks(int mt, int nbs, int delay, bool mixed)
 typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-static int make_p16_map(Context *ctx, CUtensorMap *map, void *P16, size_t rows, int nbi, int fmt)
+static int make_p16_map(Context *ctx, CUtensorMap *map, void *P16, size_t rows, int nbi, int fmt, bool split)
 {
     static EncodeTiledFn encode = nullptr;
     if (!encode) {
@@ -783,10 +896,11 @@ static int make_p16_map(Context *ctx, CUtensorMap *map, void *P16, size_t rows, 
     }
     const cuuint64_t dims[2] = {(cuuint64_t)nbi, (cuuint64_t)rows};
     const cuuint64_t strides[1] = {(cuuint64_t)nbi * 2};
-    const cuuint32_t box[2] = {MX_KC, BLK};
+    const cuuint32_t box[2] = {(cuuint32_t)(split ? MX_KC_SPLIT : MX_KC), BLK};
     const cuuint32_t estr[2] = {1, 1};
     const CUresult r = encode(map, fmt ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, P16, dims,
-                              strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                              strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                              split ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B,
                               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) {
         ctx->set_error("cuTensorMapEncodeTiled failed (%d)", (int)r);
@@ -800,7 +914,7 @@ int potrf_device(Context *ctx, double *dA, int mt, int nbi, int nb_user, int n_u
     return potrf_run(ctx, dA, mt, nbi, nb_user, n_user, info, -1);
 }
 
-// p16_fmt < 0: FP64 updates; 0: FP16 updates; 1: BF16 updates.
+// p16_fmt < 0: FP64 updates; 0: FP16; 1: BF16; 2: split FP16 (hi + lo).
 int potrf_run(Context *ctx, double *dA, int mt, int nbi, int nb_user, int n_user, int *info, int p16_fmt)
 {
     const int nbs = nbi / BLK;
@@ -816,15 +930,17 @@ int potrf_run(Context *ctx, double *dA, int mt, int nbi, int nb_user, int n_user
         return DPLASMA_ERR_UNEXPECTED;
     }
     // task list (cached per shape)
-    if (ctx->task_mt != mt || ctx->task_nbs != nbs || ctx->task_delay != ctx->potrf_delay || ctx->task_mixed != mixed) {
-        std::vector<uint64_t> tasks = build_potrf_tasks(mt, nbs, ctx->potrf_delay, mixed);
+    const int chunk = mixed ? std::max(1, ctx->mx_chunk) : 0;
+    if (ctx->task_mt != mt || ctx->task_nbs != nbs || ctx->task_delay != ctx->potrf_delay || ctx->task_mixed != chunk) {
+        std::vector<uint64_t> tasks = mixed ? build_potrf_tasks_mixed(mt, nbs, ctx->potrf_delay, chunk)
+                                            : build_potrf_tasks(mt, nbs, ctx->potrf_delay);
         uint64_t *dt = (uint64_t *)ctx->buffer(BUF_TASKS, tasks.size() * sizeof(uint64_t));
         if (!dt) return DPLASMA_ERR_OUT_OF_RESOURCES;
         CK(cudaMemcpyAsync(dt, tasks.data(), tasks.size() * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
         ctx->task_mt = mt;
         ctx->task_nbs = nbs;
         ctx->task_delay = ctx->potrf_delay;
-        ctx->task_mixed = mixed;
+        ctx->task_mixed = chunk;
         ctx->ntasks = (int)tasks.size();
     }
     double *W = (double *)ctx->buffer(BUF_W, (size_t)mt * nbs * BLK * BLK * sizeof(double));
@@ -867,25 +983,36 @@ int potrf_run(Context *ctx, double *dA, int mt, int nbi, int nb_user, int n_user
     a.scl = nullptr;
     a.p16_target = 0.f;
     a.p16_fmt = 0;
+    a.mx_split = 0;
+    a.mx_chunk = 1;
+    a.p16_rows = 0;
     CUtensorMap tmap;
     memset(&tmap, 0, sizeof(tmap));
     if (mixed) {
+        const bool split = p16_fmt == 2;
         const size_t ntl = (size_t)mt * (mt + 1) / 2;
-        const size_t pbytes = ntl * (size_t)nbi * nbi * 2, sbytes = ntl * nbs * sizeof(float);
+        const size_t rows = ntl * (size_t)nbi;
+        const size_t pbytes = (split ? 2 : 1) * rows * nbi * 2, sbytes = (size_t)mt * nbs * sizeof(float);
         unsigned char *pb = (unsigned char *)ctx->buffer(BUF_P16, pbytes + sbytes + 256);
         if (!pb) return DPLASMA_ERR_OUT_OF_RESOURCES;
         a.P16 = pb;
         a.scl = (float *)(pb + ((pbytes + 255) / 256) * 256);
-        a.p16_fmt = p16_fmt;
+        a.p16_fmt = p16_fmt == 1 ? 1 : 0;
+        a.mx_split = split ? 1 : 0;
+        a.mx_chunk = chunk;
+        a.p16_rows = (int)rows;
         // fp16: headroom below 65504; bf16 has the FP32 range
-        a.p16_target = p16_fmt ? 1.0f : 16384.0f;
-        const int e = make_p16_map(ctx, &tmap, pb, ntl * (size_t)nbi, nbi, p16_fmt);
+        a.p16_target = p16_fmt == 1 ? 1.0f : 16384.0f;
+        const int e = make_p16_map(ctx, &tmap, pb, (split ? 2 : 1) * rows, nbi, a.p16_fmt, split);
         if (e) return e;
     }
 
     const size_t smem = potrf_smem_bytes(mixed);
     CK(cudaEventRecord(ctx->ev0, st));
     if (mixed) {
+        p16_scale_kernel<<<mt, nbi, 0, st>>>(dA, mt, nbi, a.p16_target, a.scl);
+        CK(cudaGetLastError());
+        ctx->launches += 1;
         CK(cudaFuncSetAttribute(potrf_persistent_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         potrf_persistent_kernel<true><<<grid, NTHREADS, smem, st>>>(a, tmap);
     } else {
@@ -1049,6 +1176,9 @@ int potrf_launch_prealloc(cudaStream_t st, double *dA, int mt, int nbi, int nb_u
     a.scl = nullptr;
     a.p16_target = 0.f;
     a.p16_fmt = 0;
+    a.mx_split = 0;
+    a.mx_chunk = 1;
+    a.p16_rows = 0;
     CUtensorMap tmap;
     memset(&tmap, 0, sizeof(tmap));
     const size_t smem = potrf_smem_bytes(false);

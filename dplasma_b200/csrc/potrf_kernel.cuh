@@ -42,14 +42,18 @@ constexpr int STAGE_DOUBLES = 2 * BK * SP;
 
 // Mixed-precision variant (16-bit tensor-core updates, nbi = 256): the FP64
 // ring keeps NSTAGE_MIXED stages for the TRSM jobs, and a second ring holds
-// MX_NST stages of 16-bit operands, each A (128 rows x MX_KC) and B (256 rows
-// x MX_KC) in the 128-byte-swizzled K-major layout of the UMMA descriptors.
+// MX_NST stages of 16-bit operands in the swizzled K-major layout of the UMMA
+// descriptors.  One stage is 48 KB either way:
+//   single 16-bit operands: A (128 rows x 64) and B (256 rows x 64), 128-byte swizzle;
+//   split FP16 (hi + lo):   A_hi, A_lo (128 x 32) and B_hi, B_lo (256 x 32), 64-byte swizzle.
 constexpr int NSTAGE_MIXED = 3;
-constexpr int MX_KC = 64;                          // K per 16-bit stage (one 128-byte row)
+constexpr int MX_KC = 64;                          // K per 16-bit stage, single operands
+constexpr int MX_KC_SPLIT = 32;                    // K per 16-bit stage, split operands
 constexpr int MX_NST = 2;
 constexpr int MX_A_BYTES = BLK * MX_KC * 2;        // 16 KB
 constexpr int MX_B_BYTES = 2 * BLK * MX_KC * 2;    // 32 KB
 constexpr int MX_STAGE_BYTES = MX_A_BYTES + MX_B_BYTES;
+constexpr int MX_SPLIT_BLOCK = BLK * MX_KC_SPLIT * 2;   // 8 KB: 128 rows of one split half
 constexpr int MX_TMEM_COLS = 256;                  // 128 x 256 FP32 accumulator
 constexpr int MX_NB = 256;
 
@@ -94,7 +98,10 @@ struct PotrfArgs {
     void *P16;
     float *scl;
     float p16_target;      // largest |value| a 16-bit panel block is scaled to
-    int p16_fmt;           // 1: bf16, 0: fp16
+    int p16_fmt;           // 1: bf16, 0: fp16 (also for the split form)
+    int mx_split;          // 1: each panel value is hi + lo (two fp16), lo rows follow at +p16_rows
+    int mx_chunk;          // panels accumulated in tensor memory per update task
+    int p16_rows;          // rows of the hi part of P16
 };
 
 __device__ __forceinline__ double *tile_ptr(const PotrfArgs &a, int m, int n)

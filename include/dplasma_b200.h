@@ -206,13 +206,18 @@ int dplasma_b200_dpotrf_noalloc(void *stream, dplasma_enum_t uplo, parsec_tiled_
 /* Type of the tensor-core operands of the trailing updates. */
 #define DPLASMA_B200_FP16 0
 #define DPLASMA_B200_BF16 1
+/* Each panel value as the sum of two FP16 numbers (hi + lo); three products
+ * per update (hi*hi + hi*lo + lo*hi, the split-FP16 method of Ootomo and
+ * Yokota, 2022) give about 22 bits: for condition numbers near 1e6, where a
+ * single 16-bit factorization can lose positive definiteness. */
+#define DPLASMA_B200_FP16_SPLIT 2
 /* Correction solver of the refinement. */
 #define DPLASMA_B200_IR_AUTO  0   /* plain refinement, GMRES-IR once it stops contracting */
 #define DPLASMA_B200_IR_PLAIN 1   /* x += L^-T L^-1 r */
 #define DPLASMA_B200_IR_GMRES 2   /* GMRES on L^-T L^-1 A d = L^-T L^-1 r */
 
 typedef struct dplasma_b200_refine_opts_s {
-    int    fmt;        /* DPLASMA_B200_FP16 or DPLASMA_B200_BF16 */
+    int    fmt;        /* DPLASMA_B200_FP16, DPLASMA_B200_BF16 or DPLASMA_B200_FP16_SPLIT */
     int    solver;     /* DPLASMA_B200_IR_* */
     int    itermax;    /* refinement iterations before the FP64 fallback (LAPACK dsposv ITERMAX = 30) */
     int    gmres_m;    /* largest Krylov dimension of one GMRES-IR correction */

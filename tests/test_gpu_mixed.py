@@ -83,6 +83,8 @@ def run_dposv(ctx, A0, B0, NB, uplo):
     (1000, 256, 5, db.Lower, db.FP16),      # ragged: identity-padded last tile
     (1300, 200, 3, db.Lower, db.BF16),      # nb 200 -> 256-wide internal tiles
     (256, 256, 1, db.Lower, db.FP16),       # one tile: no tensor-core update at all
+    (2048, 256, 16, db.Lower, db.FP16_SPLIT),
+    (1300, 200, 3, db.Upper, db.FP16_SPLIT),
 ])
 def test_dsposv_dplgsy(gpu_ctx, N, NB, NRHS, uplo, fmt):
     A = oracle.dplgsy(N, NB, 3872, bump=float(N))
@@ -101,7 +103,7 @@ def test_dsposv_dplgsy(gpu_ctx, N, NB, NRHS, uplo, fmt):
 
 
 @pytest.mark.parametrize("kappa", [1e2, 1e4, 1e6])
-@pytest.mark.parametrize("fmt", [db.FP16, db.BF16])
+@pytest.mark.parametrize("fmt", [db.FP16, db.BF16, db.FP16_SPLIT])
 def test_dsposv_conditioned(gpu_ctx, kappa, fmt):
     N, NB, NRHS = 2048, 256, 16
     A = householder_spd(N, kappa)
@@ -110,6 +112,8 @@ def test_dsposv_conditioned(gpu_ctx, kappa, fmt):
     B = A @ Xt
     rc, st, X, _, _ = run_dsposv(gpu_ctx, A, B, NB, db.Lower, fmt=fmt)
     assert rc == 0, gpu_ctx.last_error()
+    if fmt == db.FP16_SPLIT or kappa <= 1e4:
+        assert st["fallback"] == 0, st      # the split form keeps kappa = 1e6 positive definite
     assert st["backward_error"] < 10 * N * EPS, st
     assert daxmb_ratio(A, X, B) < 10.0
     X64 = run_dposv(gpu_ctx, A, B, NB, db.Lower)
@@ -127,6 +131,10 @@ def test_dsposv_solvers(gpu_ctx, solver):
     B = np.random.default_rng(9).standard_normal((N, NRHS))
     rc, st, X, _, _ = run_dsposv(gpu_ctx, A, B, NB, db.Lower, fmt=db.BF16, solver=solver)
     assert rc == 0, gpu_ctx.last_error()
+    # a second call on the same context (cached task list, grown buffers) agrees
+    rc2, st2, X2, _, _ = run_dsposv(gpu_ctx, A, B, NB, db.Lower, fmt=db.BF16, solver=solver)
+    assert rc2 == 0 and (st2["iter"], st2["fallback"]) == (st["iter"], st["fallback"])
+    assert np.abs(X2 - X).max() <= 1e-12 * np.abs(X).max()
     assert st["fallback"] == 0 and st["solver_used"] == solver, st
     if solver == db.IR_GMRES:
         assert st["inner_iters"] >= 1
