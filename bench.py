@@ -1,18 +1,26 @@
 #!/usr/bin/env python
 """Benchmark of the B200 tile-Cholesky path (one JSON line on stdout).
 
-Workload (one "step"): plain FP64 dplasma_dposv, lower, N=65536, NB=256,
-NRHS=16, on the dplgsy matrix (seed 3872, diagonal += N) and dplrnt
-right-hand sides (seed 3873) -- the matrix and sizes dplasma's own testers
-use, generated on the GPU bit-identically to the reference's generators.
+Metric: TFLOP/s and time to FP64 accuracy of dposv at N=65536, NRHS=16 --
+the mixed-precision solve (tensor-core FP16 trailing updates + FP64
+iterative refinement, dplasma_b200_dsposv_ex) against plain FP64
+dplasma_dposv (dpotrf + dpotrs) on the same matrix and right-hand sides.
 
-  value : TFLOP/s of the step with inputs resident in HBM (the matrix is
-          restored from a pristine device copy before every step, inside the
-          timed region; 17 GB per step, larger than L2);
-  e2e   : the same metric through the C ABI with caller-owned pinned HOST
-          buffers: host->device copy of A and B, factor, solve, copy back;
-  roofline : the persistent factorization kernel against the measured FP64
-          tensor-core (DMMA) peak of this GPU;
+Workload: A = Q diag(sigma) Q^T with Q the product of 64 Householder
+reflectors of random unit vectors (seed 7) and sigma geometric from 1 to
+kappa (default 1e6), built on the GPU (dplasma_b200_dplgsy_cond); B from
+dplasma_dplrnt (seed 3873).  One step = one mixed solve to the LAPACK dsposv
+accuracy (A and B stay resident in HBM; A is 17 GB, larger than L2).
+
+  value : effective TFLOP/s of the mixed step, (N^3/3 + 2 NRHS N^2 (iter+1)) / time;
+  fp64  : the same inputs through plain FP64 dposv (time, TFLOP/s), and the
+          speed-up of the mixed step over it;
+  e2e   : the mixed step through the C ABI with caller-owned pinned HOST
+          buffers (host->device copy of A and B and the read-back of X inside);
+  roofline : the mixed factorization kernel against the measured dense 16-bit
+          tensor peak (MEASURED_PEAKS.json); roofline_fp64 the FP64 kernel
+          against the measured FP64 DMMA peak;
+  kappa_sweep : kappa 1e2/1e4/1e6 x FP16/BF16/split-FP16 against FP64;
   cpu_baseline : the reference's own CORE kernels (compiled from its sources)
           run as the tile DAG on all host cores, on a bounded N.
 
@@ -161,6 +169,17 @@ def run_reference_arm(args):
 # ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
+FMTS = {"fp16": 0, "bf16": 1, "split": 2}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
 def run_gpu(args):
     import torch
     import dplasma_b200 as db
@@ -176,46 +195,74 @@ def run_gpu(args):
     dev = local
     torch.cuda.set_device(dev)
     N, NB, NRHS = args.n, args.nb, args.nrhs
+    fmt = FMTS[args.fmt]
     ctx = db.Context(dev)
 
-    # device-resident descriptors (sym lower tiles, general tiles for B)
-    dA = db.desc_sym(N, NB, db.Lower)
-    dB = db.desc_general(N, NRHS, NB, NB)
-    A_pristine = torch.empty(db.desc_elems(dA), dtype=torch.float64, device="cuda")
-    A = torch.empty_like(A_pristine)
-    B_pristine = torch.empty(db.desc_elems(dB), dtype=torch.float64, device="cuda")
-    B = torch.empty_like(B_pristine)
-    db.attach(dA, A_pristine)
+    def dev_buf(d):
+        return torch.empty(db.desc_elems(d), dtype=torch.float64, device="cuda")
+
+    dA, dB, dX = db.desc_sym(N, NB, db.Lower), db.desc_general(N, NRHS, NB, NB), db.desc_general(N, NRHS, NB, NB)
+    A_pristine, B_pristine = dev_buf(dA), dev_buf(dB)
+    A, B, X = torch.empty_like(A_pristine), torch.empty_like(B_pristine), dev_buf(dX)
     db.attach(dB, B_pristine)
-    assert ctx.dplgsy(float(N), db.Lower, dA, SEED_A) == 0
     assert ctx.dplrnt(0, dB, SEED_B) == 0
     db.attach(dA, A)
     db.attach(dB, B)
-    peak = ctx.fp64_peak_tflops()
+    db.attach(dX, X)
+    peak64 = ctx.fp64_peak_tflops()
+    peaks = measured_peaks()
 
-    def step():
+    def generate(kappa):
+        db.attach(dA, A_pristine)
+        rc = ctx.dplgsy_cond(kappa, 64, db.Lower, dA, 7)
+        db.attach(dA, A)
+        if rc != 0:
+            raise RuntimeError(f"dplgsy_cond rc={rc}: {ctx.last_error()}")
+
+    def fp64_solve():
+        """plain FP64 dposv on fresh copies; returns (ms, solution)"""
         A.copy_(A_pristine)
         B.copy_(B_pristine)
-        torch.cuda.current_stream().synchronize()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
         info = ctx.dposv(db.Lower, dA, dB)
+        e1.record()
+        torch.cuda.synchronize()
         if info != 0:
             raise RuntimeError(f"dposv info={info}: {ctx.last_error()}")
+        return e0.elapsed_time(e1), B.clone(), ctx.last_factor_ms(), ctx.last_solve_ms()
 
+    def mixed_solve(f):
+        """one mixed step: A and B resident (A is left unchanged by the solve)"""
+        rc, st = ctx.dsposv(db.Lower, dA, dB, dX, fmt=f)
+        if rc != 0:
+            raise RuntimeError(f"dsposv rc={rc}: {ctx.last_error()}")
+        return st
+
+    def fwd_err(Xs, X64):
+        return float((Xs - X64).abs().max() / X64.abs().max())
+
+    # ---- the headline matrix: FP64 reference leg, then the timed mixed steps
+    generate(args.kappa)
+    fp64_solve()                                   # warm-up
+    fp64 = [fp64_solve() for _ in range(2)]
+    fp64_ms = statistics.median(r[0] for r in fp64)
+    X64 = fp64[-1][1]
+    A.copy_(A_pristine)
+    B.copy_(B_pristine)
     for _ in range(args.warmup):
-        step()
+        mixed_solve(fmt)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    fac_ms, sol_ms, launches = [], [], 0
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
+    stats, launches = [], 0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(dev) as clk:
         e0.record()
         t0 = time.perf_counter()
         for _ in range(args.steps):
-            step()
-            fac_ms.append(ctx.last_factor_ms())
-            sol_ms.append(ctx.last_solve_ms())
+            stats.append(mixed_solve(fmt))
             launches += ctx.last_launches()
         e1.record()
         torch.cuda.synchronize()
@@ -228,37 +275,61 @@ def run_gpu(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
     ms_step = total_ms / args.steps
-    value = world * posv_flops(N, NRHS) / (ms_step * 1e-3) / 1e12
-    fac = statistics.median(fac_ms)
-    achieved = potrf_flops(N) / (fac * 1e-3) / 1e12
+    iters = statistics.median(st["iter"] for st in stats)
+    eff_flops = potrf_flops(N) + 2.0 * NRHS * N * N * (max(iters, 0) + 1)
+    value = world * eff_flops / (ms_step * 1e-3) / 1e12
+    fac_ms = statistics.median(st["factor_ms"] for st in stats)
+    mixed_fwd = fwd_err(X, X64)
+    clocks = clk.summary()
 
-    # end to end through the C ABI with pinned host buffers
+    # ---- end to end through the C ABI with pinned host buffers
     e2e = None
     if args.e2e_steps > 0:
         hA = torch.empty(db.desc_elems(dA), dtype=torch.float64, pin_memory=True)
         hB = torch.empty(db.desc_elems(dB), dtype=torch.float64, pin_memory=True)
-        hA_np, hB_np = hA.numpy(), hB.numpy()
-        A0h, B0h = A_pristine.cpu().numpy(), B_pristine.cpu().numpy()
-        hdA = db.desc_sym(N, NB, db.Lower)
-        hdB = db.desc_general(N, NRHS, NB, NB)
-        db.attach(hdA, hA_np)
-        db.attach(hdB, hB_np)
+        hX = torch.empty(db.desc_elems(dX), dtype=torch.float64, pin_memory=True)
+        hA.copy_(A_pristine)
+        hB.copy_(B_pristine)
+        hdA, hdB, hdX = db.desc_sym(N, NB, db.Lower), db.desc_general(N, NRHS, NB, NB), db.desc_general(N, NRHS, NB, NB)
+        db.attach(hdA, hA.numpy())
+        db.attach(hdB, hB.numpy())
+        db.attach(hdX, hX.numpy())
         times = []
         for i in range(args.e2e_steps + 1):
-            np.copyto(hA_np, A0h)
-            np.copyto(hB_np, B0h)
             t = time.perf_counter()
-            info = ctx.dposv(db.Lower, hdA, hdB)
+            rc, st = ctx.dsposv(db.Lower, hdA, hdB, hdX, fmt=fmt)
             dt = time.perf_counter() - t
-            assert info == 0, ctx.last_error()
+            assert rc == 0, ctx.last_error()
             if i > 0:
                 times.append(dt)
         e2e_s = sum(times) / len(times)
-        e2e = {"value": world * posv_flops(N, NRHS) / e2e_s / 1e12, "unit": "TFLOP/s",
-               "h2d_bytes_per_step": int(hA_np.nbytes + hB_np.nbytes),
-               "d2h_bytes_per_step": int(hA_np.nbytes + hB_np.nbytes), "s_per_step": e2e_s,
-               "steps": len(times)}
-        del hA, hB
+        e2e = {"value": world * eff_flops / e2e_s / 1e12, "unit": "TFLOP/s",
+               "h2d_bytes_per_step": int(hA.numel() * 8 + hB.numel() * 8),
+               "d2h_bytes_per_step": int(hX.numel() * 8), "s_per_step": e2e_s, "steps": len(times),
+               "fp64_dposv_speedup": (fp64_ms * 1e-3) / e2e_s}
+        del hA, hB, hX
+
+    # ---- kappa sweep (one run each; the headline kappa reuses its FP64 leg)
+    sweep = []
+    if args.sweep:
+        for kappa in (1e2, 1e4, 1e6):
+            if kappa != args.kappa:
+                generate(kappa)
+                t64, Xk, _, _ = fp64_solve()
+            else:
+                t64, Xk = fp64_ms, X64
+            A.copy_(A_pristine)
+            B.copy_(B_pristine)
+            for name, f in FMTS.items():
+                torch.cuda.synchronize()
+                ta = time.perf_counter()
+                st = mixed_solve(f)
+                torch.cuda.synchronize()
+                tm = (time.perf_counter() - ta) * 1e3
+                sweep.append({"kappa": kappa, "fmt": name, "ms": tm, "fp64_ms": t64, "speedup": t64 / tm,
+                              "iter": st["iter"], "gmres_iters": st["inner_iters"], "fallback": st["fallback"],
+                              "fmt_used": st["fmt_used"], "backward_error": st["backward_error"],
+                              "forward_error_vs_fp64": fwd_err(X, Xk), "factor_ms": st["factor_ms"]})
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -268,32 +339,49 @@ def run_gpu(args):
                "sample": f"dpotrf N={args.cpu_n} NB=256 lower, one run of {t:.2f} s: the reference's CORE_d* kernels "
                          "(compiled from its sources) as the tile DAG, OpenMP tasks over OpenBLAS on all host cores"}
 
-    # DRAM bytes of one factorization launch: an ncu capture at a smaller N
-    # (profiles/potrf_traffic_N16384.txt), scaled by (N/n)^3 at the same NB.
+    # DRAM bytes of one mixed factorization launch: an ncu capture at a
+    # smaller N, scaled to this N by the update traffic ((N/n)^3 at fixed NB)
     traffic = None
-    tpath = os.path.join(ROOT, "profiles", "potrf_traffic_N16384.txt")
+    tpath = os.path.join(ROOT, "profiles", "potrf_mixed_traffic_N16384.txt")
     if os.path.exists(tpath) and NB == 256:
         for line in open(tpath):
             if line.startswith("dram_bytes_per_launch"):
                 _, b, _, n0 = line.split()
                 traffic = float(b) * (N / float(n0)) ** 3
-
-    clocks = clk.summary()
+    peak16 = peaks.get("bf16_tflops")
+    achieved = potrf_flops(N) / (fac_ms * 1e-3) / 1e12
+    tensor_flops = potrf_flops(N) * (3.0 if fmt == 2 else 1.0)
+    fac64 = statistics.median(r[2] for r in fp64)
+    ach64 = potrf_flops(N) / (fac64 * 1e-3) / 1e12
     line = {
         "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"dposv FP64 lower N={N} NB={NB} NRHS={NRHS}: dplgsy(seed 3872, bump N) and "
-                               f"dplrnt(seed 3873); step = restore A,B in HBM + dpotrf + dpotrs",
-                   "l2": "inputs larger than L2 (A is %.1f GB per step)" % (A.numel() * 8 / 1e9),
+        "vs_baseline": None, "dtype": "f64 (refined) / fp16 tensor-core updates", "data": "synthetic",
+        "config": {"workload": f"mixed-precision dposv (dsposv), lower, N={N} NB={NB} NRHS={NRHS}, "
+                               f"{args.fmt} trailing updates, FP64 IR/GMRES-IR to the LAPACK dsposv accuracy; "
+                               f"A = Q diag(geomspace(1, {args.kappa:g})) Q^T, Q = 64 Householder reflectors "
+                               "(seed 7), B = dplrnt(seed 3873)",
+                   "l2": "inputs larger than L2 (A is %.1f GB)" % (A.numel() * 8 / 1e9),
                    "parallelism": "replicas" if world > 1 else "single GPU"},
-        "dpotrf_tflops": achieved, "dpotrf_ms": fac, "dpotrs_ms": statistics.median(sol_ms),
-        "dpotrs_gbs": 2 * (N * (N + 1) / 2 * 8 + 2 * N * NRHS * 8) / (statistics.median(sol_ms) * 1e-3) / 1e9,
-        "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": achieved / peak if peak > 0 else None, "traffic": traffic,
-                     "kernel": "potrf_persistent_kernel",
-                     "peak_source": "measured FP64 DMMA (mma.sync m16n8k4 f64) probe on this GPU; "
-                                    "MEASURED_PEAKS.json carries no FP64 figure"},
+        "time_to_accuracy_s": ms_step * 1e-3, "mixed_iter": iters,
+        "mixed_backward_error": max(st["backward_error"] for st in stats),
+        "mixed_forward_error_vs_fp64": mixed_fwd, "mixed_fallback": max(st["fallback"] for st in stats),
+        "mixed_factor_ms": fac_ms,
+        "fp64": {"dposv_ms": fp64_ms, "tflops": posv_flops(N, NRHS) / (fp64_ms * 1e-3) / 1e12,
+                 "dpotrf_ms": fac64, "dpotrs_ms": statistics.median(r[3] for r in fp64),
+                 "speedup_of_mixed": fp64_ms / ms_step},
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak16, "unit": "TFLOP/s",
+                     "frac": achieved / peak16 if peak16 else None, "traffic": traffic,
+                     "kernel": "potrf_persistent_kernel<true> (mixed factorization)",
+                     "tensor_flops_per_launch": tensor_flops,
+                     "note": "achieved counts N^3/3 (FP64-equivalent) per launch; peak = dense bf16 burst of "
+                             "measured (MEASURED_PEAKS.json); the kernel is bound by the FP64 tile traffic of "
+                             "its in-place epilogue and the FP64 critical path, not by the tensor pipe"},
+        "roofline_fp64": {"bound": "tensor", "achieved": ach64, "peak": peak64, "unit": "TFLOP/s",
+                          "frac": ach64 / peak64 if peak64 > 0 else None,
+                          "kernel": "potrf_persistent_kernel<false> (FP64 DMMA)",
+                          "peak_source": "measured FP64 DMMA (mma.sync m16n8k4 f64) probe on this GPU"},
+        "kappa_sweep": sweep,
         "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks, "wall_s": wall,
     }
     if rank == 0:
@@ -316,6 +404,9 @@ def main():
     p.add_argument("--e2e-steps", type=int, default=2)
     p.add_argument("--cpu-n", type=int, default=16384)
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--kappa", type=float, default=1e6)
+    p.add_argument("--fmt", default="split", choices=sorted(FMTS))
+    p.add_argument("--no-sweep", dest="sweep", action="store_false")
     args = p.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)

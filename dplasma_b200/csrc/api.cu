@@ -473,6 +473,7 @@ extern "C" void dplasma_b200_refine_opts_default(dplasma_b200_refine_opts_t *o)
     o->gmres_m = 30;
     o->gmres_tol = 1e-4;
     o->bwdmax = 1.0;
+    o->escalate = 1;
 }
 
 extern "C" int dplasma_b200_dsposv_ex(parsec_context_t *parsec, dplasma_enum_t uplo, parsec_tiled_matrix_t *A,
@@ -529,6 +530,7 @@ extern "C" int dplasma_b200_dsposv_ex(parsec_context_t *parsec, dplasma_enum_t u
     ro.gmres_m = o.gmres_m;
     ro.gmres_tol = o.gmres_tol;
     ro.bwd_factor = o.bwdmax;
+    ro.escalate = o.escalate != 0;
     RefineStats st;
     rc = refine_solve(ctx, A0, L, g, b, x, npad, nrhs_pad, ro, st);
     if (stats) {
@@ -536,6 +538,7 @@ extern "C" int dplasma_b200_dsposv_ex(parsec_context_t *parsec, dplasma_enum_t u
         stats->inner_iters = st.inner_iters;
         stats->fallback = st.fallback;
         stats->solver_used = st.solver_used;
+        stats->fmt_used = st.fmt_used;
         stats->backward_error = st.backward_error;
         stats->factor_ms = st.factor_ms;
         stats->refine_ms = st.refine_ms;

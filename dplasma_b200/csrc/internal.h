@@ -130,9 +130,10 @@ int wave_max_blocks_per_sm();
 struct RefineOpts {
     int fmt = 0, solver = 0, itermax = 30, gmres_m = 30;
     double gmres_tol = 1e-4, bwd_factor = 1.0;
+    bool escalate = true;
 };
 struct RefineStats {
-    int iter = 0, inner_iters = 0, fallback = 0, solver_used = 0;
+    int iter = 0, inner_iters = 0, fallback = 0, solver_used = 0, fmt_used = 0;
     double backward_error = 0.0, factor_ms = 0.0, refine_ms = 0.0;
 };
 int refine_solve(Context *ctx, const double *A0, double *L, const Geom &g, double *b, double *x, int npad, int nc,

@@ -629,7 +629,15 @@ int refine_solve(Context *ctx, const double *A0, double *L, const Geom &g, doubl
     CK(cudaEventRecord(e0, ctx->stream));
     CK(cudaMemcpyAsync(L, A0, g.elems() * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
     int info = 0;
+    st.fmt_used = o.fmt;
     if ((rc = potrf_run(ctx, L, g.mt, g.nbi, g.nb, g.n, &info, o.fmt))) return rc;
+    if (info != 0 && o.escalate && o.fmt != 2) {
+        // the 16-bit rounding of the panels broke positive definiteness:
+        // the split form (about 22 bits) before giving up on tensor cores
+        CK(cudaMemcpyAsync(L, A0, g.elems() * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+        st.fmt_used = 2;
+        if ((rc = potrf_run(ctx, L, g.mt, g.nbi, g.nb, g.n, &info, 2))) return rc;
+    }
     CK(cudaEventRecord(e1, ctx->stream));
     R.W = (const double *)ctx->buffer(BUF_W, 0);
 
@@ -691,6 +699,7 @@ int refine_solve(Context *ctx, const double *A0, double *L, const Geom &g, doubl
     if (!converged) {
         // FP64 factorization of the working copy and a plain solve
         st.fallback = 1;
+        st.fmt_used = -1;
         st.iter = info != 0 ? -3 : -(o.itermax + 1);
         CK(cudaMemcpyAsync(L, A0, g.elems() * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
         int info64 = 0;

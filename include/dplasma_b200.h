@@ -223,6 +223,8 @@ typedef struct dplasma_b200_refine_opts_s {
     int    gmres_m;    /* largest Krylov dimension of one GMRES-IR correction */
     double gmres_tol;  /* residual reduction asked of one GMRES-IR correction */
     double bwdmax;     /* LAPACK dsposv BWDMAX: stop when ||r_j|| < ||x_j|| ||A|| eps sqrt(n) bwdmax */
+    int    escalate;   /* 1: when an FP16/BF16 factorization loses positive definiteness, retry in
+                          the split-FP16 form before the FP64 fallback */
 } dplasma_b200_refine_opts_t;
 
 typedef struct dplasma_b200_refine_stats_s {
@@ -231,12 +233,13 @@ typedef struct dplasma_b200_refine_stats_s {
     int    inner_iters;    /* GMRES iterations over all corrections */
     int    fallback;       /* 1 when the FP64 factorization produced the solution */
     int    solver_used;    /* highest DPLASMA_B200_IR_* used (1 plain, 2 GMRES) */
+    int    fmt_used;       /* operand form of the factor that was refined (-1: FP64 fallback) */
     double backward_error; /* max_j ||b_j - A x_j||_inf / (||A||_inf ||x_j||_inf + ||b_j||_inf) */
     double factor_ms;      /* device time of the mixed factorization (with its working copy) */
     double refine_ms;      /* device time of the solves and refinement (and of a fallback) */
 } dplasma_b200_refine_stats_t;
 
-/* Defaults: FP16, IR_AUTO, itermax 30, gmres_m 30, gmres_tol 1e-4, bwdmax 1. */
+/* Defaults: FP16, IR_AUTO, itermax 30, gmres_m 30, gmres_tol 1e-4, bwdmax 1, escalate 1. */
 void dplasma_b200_refine_opts_default(dplasma_b200_refine_opts_t *opts);
 
 /* dplasma_b200_dplgsy_cond: no dplasma counterpart; a test-matrix generator

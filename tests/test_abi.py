@@ -132,7 +132,8 @@ def test_argument_checks_without_a_device():
     assert L.dplasma_dsposv(None, 999, pd(d), pd(b), pd(x), pd(it)) == -1
     o = db.RefineOpts()
     L.dplasma_b200_refine_opts_default(pd(o))
-    assert (o.fmt, o.solver, o.itermax, o.gmres_m, o.gmres_tol, o.bwdmax) == (db.FP16, db.IR_AUTO, 30, 30, 1e-4, 1.0)
+    assert (o.fmt, o.solver, o.itermax, o.gmres_m, o.gmres_tol, o.bwdmax, o.escalate) == \
+        (db.FP16, db.IR_AUTO, 30, 30, 1e-4, 1.0, 1)
     st = db.RefineStats()
     bad = db.RefineOpts()
     L.dplasma_b200_refine_opts_default(pd(bad))

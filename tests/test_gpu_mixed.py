@@ -112,8 +112,9 @@ def test_dsposv_conditioned(gpu_ctx, kappa, fmt):
     B = A @ Xt
     rc, st, X, _, _ = run_dsposv(gpu_ctx, A, B, NB, db.Lower, fmt=fmt)
     assert rc == 0, gpu_ctx.last_error()
-    if fmt == db.FP16_SPLIT or kappa <= 1e4:
-        assert st["fallback"] == 0, st      # the split form keeps kappa = 1e6 positive definite
+    # no FP64 fallback: a 16-bit breakdown escalates to the split form, which
+    # keeps kappa = 1e6 positive definite
+    assert st["fallback"] == 0 and st["fmt_used"] in (fmt, db.FP16_SPLIT), st
     assert st["backward_error"] < 10 * N * EPS, st
     assert daxmb_ratio(A, X, B) < 10.0
     X64 = run_dposv(gpu_ctx, A, B, NB, db.Lower)
@@ -147,7 +148,7 @@ def test_dsposv_fallback_leaves_fp64_factor(gpu_ctx):
     N, NB, NRHS = 1024, 256, 4
     A = householder_spd(N, 1e6)
     B = np.random.default_rng(10).standard_normal((N, NRHS))
-    rc, st, X, (dA, bufA), _ = run_dsposv(gpu_ctx, A, B, NB, db.Lower, fmt=db.BF16, itermax=0)
+    rc, st, X, (dA, bufA), _ = run_dsposv(gpu_ctx, A, B, NB, db.Lower, fmt=db.BF16, itermax=0, escalate=False)
     assert rc == 0, gpu_ctx.last_error()
     # -1: the refinement may not iterate; -3: the 16-bit factorization broke down
     assert st["fallback"] == 1 and st["iter"] in (-1, -3), st
@@ -168,7 +169,7 @@ def test_dsposv_not_spd_returns_info(gpu_ctx):
     dR, _ = sym_desc_with(A, NB, db.Lower)
     info = gpu_ctx.dpotrf(db.Lower, dR)
     assert info > 0 and rc == info
-    assert st["fallback"] == 1 and st["iter"] == -3
+    assert st["fallback"] == 1 and st["iter"] == -3 and st["fmt_used"] == -1
 
 
 def test_dsposv_rejects_tile_size(gpu_ctx):
