@@ -838,12 +838,15 @@ std::vector<uint64_t> build_potrf_tasks(int mt, int nbs, int delay)
 
 // Mixed-precision ticket order.  An update task (k = chunk c) applies the
 // panels j in [c*S, min(c*S+S, n)) to the 128-row block bi of tile (m,n).
-// Each tile column n gets one chunk task per block and chunk: a full chunk is
-// issued in the step that finishes its last panel, the partial chunk that
-// ends at panel n-1 in step n-1 (the critical column).  Step k: the critical
-// column k+1, POTRF(k+1), then (when panel k closes a chunk) that chunk for
-// all columns n >= k+2 -- column k+2 first -- with TRSM(*,k+1) after `delay`
-// of them.
+// Each tile column n gets one chunk task per block and chunk: the partial
+// chunk that ends at panel n-1 in step n-1 (the critical column), a full
+// chunk once its last panel is done.  A full chunk c closes in step
+// k = c*S+S-1; its tasks for the columns n >= k+2 are spread over the steps
+// k .. k+S-1 by columns, nearest first and in parts of equal work, so every
+// step has update work to hide the POTRF/TRSM chain behind (column n is
+// always issued by step n-2, before its own critical step).  Step k: the
+// critical column k+1, POTRF(k+1), `delay` tasks of the step's share,
+// TRSM(*,k+1), the rest of the share.
 std::vector<uint64_t> build_potrf_tasks_mixed(int mt, int nbs, int delay, int S)
 {
     std::vector<uint64_t> v;
@@ -851,19 +854,29 @@ std::vector<uint64_t> build_potrf_tasks_mixed(int mt, int nbs, int delay, int S)
         for (int m = k + 1; m < mt; ++m)
             for (int bi = 0; bi < nbs; ++bi) v.push_back(make_task(T_TRSM, k, m, k, bi, 0));
     };
+    // share[k]: update tasks issued in step k
+    std::vector<std::vector<uint64_t>> share(mt > 0 ? mt : 1);
+    for (int c = 0; c * S + S - 1 + 1 < mt; ++c) {
+        const int k = c * S + S - 1;                  // the chunk's last panel
+        long long work = 0;
+        for (int n = k + 2; n < mt; ++n) work += mt - n;
+        long long done = 0;
+        for (int n = k + 2; n < mt; ++n) {
+            int part = (int)((done * S) / (work > 0 ? work : 1));
+            part = std::min(part, std::min(S - 1, n - 2 - k));
+            for (int m = n; m < mt; ++m)
+                for (int bi = 0; bi < nbs; ++bi) share[k + part].push_back(make_task(T_GEMM, c, m, n, bi, 0));
+            done += mt - n;
+        }
+    }
     v.push_back(make_task(T_POTRF, 0, 0, 0, 0, 0));
     push_trsm(0);
-    std::vector<uint64_t> rest;
     for (int k = 0; k + 1 < mt; ++k) {
         const int c = k / S;
         for (int m = k + 1; m < mt; ++m)
             for (int bi = 0; bi < nbs; ++bi) v.push_back(make_task(T_GEMM, c, m, k + 1, bi, 0));
         v.push_back(make_task(T_POTRF, k + 1, k + 1, k + 1, 0, 0));
-        rest.clear();
-        if (k == c * S + S - 1)
-            for (int n = k + 2; n < mt; ++n)
-                for (int m = n; m < mt; ++m)
-                    for (int bi = 0; bi < nbs; ++bi) rest.push_back(make_task(T_GEMM, c, m, n, bi, 0));
+        const std::vector<uint64_t> &rest = share[k];
         const size_t d = std::min<size_t>(rest.size(), (size_t)std::max(delay, 0));
         v.insert(v.end(), rest.begin(), rest.begin() + d);
         push_trsm(k + 1);
@@ -1197,3 +1210,17 @@ int potrf_launch_prealloc(cudaStream_t st, double *dA, int mt, int nbi, int nb_u
 }
 
 }  // namespace db2
+
+// ---------------------------------------------------------------------------
+// Test hook (not part of the public header): the ticket order as built for a
+// launch, so host tests can replay the dependency rules on the CPU.  Returns
+// the number of tasks (those beyond `cap` are not written).
+// ---------------------------------------------------------------------------
+extern "C" int dplasma_b200_debug_task_list(int mixed_chunk, int mt, int nbs, int delay, unsigned long long *out,
+                                            int cap)
+{
+    const std::vector<uint64_t> v = mixed_chunk > 0 ? db2::build_potrf_tasks_mixed(mt, nbs, delay, mixed_chunk)
+                                                    : db2::build_potrf_tasks(mt, nbs, delay);
+    for (size_t i = 0; i < v.size() && (int)i < cap; ++i) out[i] = v[i];
+    return (int)v.size();
+}
