@@ -30,6 +30,7 @@ enum BufferId : int {
     BUF_R,            // residual / correction
     BUF_SMALL,        // per-column reductions
     BUF_KRYLOV,       // GMRES basis
+    BUF_PTRACE,       // per-POTRF phase times (opt-in trace)
     BUF_COUNT
 };
 

@@ -44,7 +44,7 @@ __device__ __forceinline__ int step_blocks(const PotrfArgs &a, int m, int n)
 template <bool MIXED>
 __device__ __forceinline__ int all_updates(const PotrfArgs &a, int m, int n)
 {
-    if (MIXED) return ((n + a.mx_chunk - 1) / a.mx_chunk) * a.nbs;
+    if (MIXED) return (n + a.mx_chunk - 1) / a.mx_chunk;
     return n * step_blocks<MIXED>(a, m, n);
 }
 
@@ -69,7 +69,7 @@ __device__ bool wait_deps(const PotrfArgs &a, uint64_t t)
             const int kl = min(k * a.mx_chunk + a.mx_chunk, n) - 1;
             return wait_geq(a.trsm_done + (int64_t)m * a.mt + kl, nbs, a.abort_flag, a.status, a.dep_limit_ns) &&
                    wait_geq(a.trsm_done + (int64_t)n * a.mt + kl, nbs, a.abort_flag, a.status, a.dep_limit_ns) &&
-                   wait_geq(a.upd_done + (int64_t)m * a.mt + n, k * nbs, a.abort_flag, a.status, a.dep_limit_ns);
+                   wait_geq(a.upd_done + (int64_t)m * a.mt + n, k, a.abort_flag, a.status, a.dep_limit_ns);
         }
         return wait_geq(a.trsm_done + (int64_t)m * a.mt + k, nbs, a.abort_flag, a.status, a.dep_limit_ns) &&
                wait_geq(a.trsm_done + (int64_t)n * a.mt + k, nbs, a.abort_flag, a.status, a.dep_limit_ns) &&
@@ -81,11 +81,11 @@ __device__ bool wait_deps(const PotrfArgs &a, uint64_t t)
     }
 }
 
-// 16-bit stages follow the FP64 stages, 1024-byte aligned in the shared
-// window (128-byte swizzle atoms of 8 rows).
+// The 16-bit stages start at the ring, 1024-byte aligned in the shared
+// window (swizzle atoms of 8 rows).
 __device__ __forceinline__ unsigned char *ring16_of(double *ring)
 {
-    unsigned char *p = reinterpret_cast<unsigned char *>(ring + NSTAGE_MIXED * STAGE_DOUBLES);
+    unsigned char *p = reinterpret_cast<unsigned char *>(ring);
     const uint32_t s = smem_u32(p);
     return p + (((s + 1023u) & ~1023u) - s);
 }
@@ -102,6 +102,7 @@ __device__ void producer_warp(const PotrfArgs &a, SmemCtl *ctl, double *ring, co
     unsigned char *ring16 = MIXED ? ring16_of(ring) : nullptr;
     if (MIXED && lane == 0) tma_prefetch_desc(tmap);
     bool pipe_ok = true;
+    int prev_mode = -1;      // MIXED: 0 FP64 ring, 1 16-bit ring (same shared memory)
     while (true) {
         int tk = -1;
         if (lane == 0) tk = ld_volatile(a.abort_flag) ? -1 : atomicAdd(a.ticket, 1);
@@ -148,16 +149,30 @@ __device__ void producer_warp(const PotrfArgs &a, SmemCtl *ctl, double *ring, co
             if (a.trace && lane == 0) a.trace_exit[6 * blockIdx.x + 2] = globaltimer_ns();
             continue;
         }
+        if (MIXED) {
+            // the FP64 ring and the 16-bit ring share memory: before the
+            // first load of the other kind, the previous task must be done
+            const int mode = ty == T_GEMM ? 1 : 0;
+            if (prev_mode >= 0 && mode != prev_mode && task_it >= 2) {
+                const uint32_t pit = task_it - 2, pslot = pit % TASKQ;
+                if (!warp_mbar_wait(&ctl->tempty[pslot], (pit / TASKQ) & 1, a.pipe_limit_ns)) {
+                    if (lane == 0) report(a, ST_MBAR_TIMEOUT, 11, task_it, tk);
+                    pipe_ok = false;
+                    break;
+                }
+            }
+            prev_mode = mode;
+        }
         fence_proxy_async();
         if (MIXED && ty == T_GEMM) {
             // 16-bit operands by TMA tensor loads (swizzled, canonical K-major
-            // UMMA layout): for every panel j of the chunk, A = block row bi of
-            // P16(m,j), B = P16(n,j); the split form adds the lo rows.
-            const int kc = task_k(t), m = task_m(t), n = task_n(t), bi = task_bi(t);
+            // UMMA layout): for every panel j of the chunk, A = P16(m,j),
+            // B = P16(n,j); the split form adds the lo rows.
+            const int kc = task_k(t), m = task_m(t), n = task_n(t);
             const int j0 = kc * a.mx_chunk, j1 = min(j0 + a.mx_chunk, n);
             const int KC = a.mx_split ? MX_KC_SPLIT : MX_KC;
             for (int j = j0; j < j1 && pipe_ok; ++j) {
-                const int rowA = (int)(lower_tile_index(m, j, a.mt) * a.nbi) + bi * BLK;
+                const int rowA = (int)(lower_tile_index(m, j, a.mt) * a.nbi);
                 const int rowB = (int)(lower_tile_index(n, j, a.mt) * a.nbi);
                 for (int kx = 0; kx < a.nbi; kx += KC) {
                     const uint32_t s = st16 % MX_NST, r = st16 / MX_NST;
@@ -171,17 +186,20 @@ __device__ void producer_warp(const PotrfArgs &a, SmemCtl *ctl, double *ring, co
                         uint64_t *bar = &ctl->full16[s];
                         mbar_arrive_expect_tx(bar, MX_STAGE_BYTES);
                         if (!a.mx_split) {
-                            tma_load_2d(st, tmap, kx, rowA, bar);
-                            tma_load_2d(st + MX_A_BYTES, tmap, kx, rowB, bar);
-                            tma_load_2d(st + MX_A_BYTES + BLK * MX_KC * 2, tmap, kx, rowB + BLK, bar);
+                            tma_load_2d(st, tmap, kx, rowA, bar);                                // A 0-127
+                            tma_load_2d(st + MX_BLOCK, tmap, kx, rowA + BLK, bar);               // A 128-255
+                            tma_load_2d(st + 2 * MX_BLOCK, tmap, kx, rowB, bar);                 // B
+                            tma_load_2d(st + 3 * MX_BLOCK, tmap, kx, rowB + BLK, bar);
                         } else {
                             const int R = a.p16_rows;
                             tma_load_2d(st, tmap, kx, rowA, bar);                                // A hi
-                            tma_load_2d(st + MX_SPLIT_BLOCK, tmap, kx, rowA + R, bar);           // A lo
-                            tma_load_2d(st + 2 * MX_SPLIT_BLOCK, tmap, kx, rowB, bar);           // B hi
-                            tma_load_2d(st + 3 * MX_SPLIT_BLOCK, tmap, kx, rowB + BLK, bar);
-                            tma_load_2d(st + 4 * MX_SPLIT_BLOCK, tmap, kx, rowB + R, bar);       // B lo
-                            tma_load_2d(st + 5 * MX_SPLIT_BLOCK, tmap, kx, rowB + R + BLK, bar);
+                            tma_load_2d(st + MX_SPLIT_BLOCK, tmap, kx, rowA + BLK, bar);
+                            tma_load_2d(st + 2 * MX_SPLIT_BLOCK, tmap, kx, rowA + R, bar);       // A lo
+                            tma_load_2d(st + 3 * MX_SPLIT_BLOCK, tmap, kx, rowA + R + BLK, bar);
+                            tma_load_2d(st + 4 * MX_SPLIT_BLOCK, tmap, kx, rowB, bar);           // B hi
+                            tma_load_2d(st + 5 * MX_SPLIT_BLOCK, tmap, kx, rowB + BLK, bar);
+                            tma_load_2d(st + 6 * MX_SPLIT_BLOCK, tmap, kx, rowB + R, bar);       // B lo
+                            tma_load_2d(st + 7 * MX_SPLIT_BLOCK, tmap, kx, rowB + R + BLK, bar);
                         }
                     }
                     __syncwarp();
@@ -348,32 +366,58 @@ __device__ void potrf_task(const PotrfArgs &a, SmemCtl *ctl, double *ring, int k
     for (int e = tid; e < a.nbs * BLK * BLK; e += NCONS) Wk[e] = 0.0;
     if (tid == 0) ctl->fail = 0;
     named_bar_sync(1, NCONS);
+    unsigned long long tp = (a.ptrace && tid == 0) ? globaltimer_ns() : 0;
+    auto phase = [&](int i) {
+        if (a.ptrace && tid == 0) {
+            const unsigned long long now = globaltimer_ns();
+            a.ptrace[8 * k + i] += now - tp;
+            tp = now;
+        }
+    };
 
     for (int p0 = 0; p0 < nbi; p0 += 32) {
         // (a) 32x32 diagonal block: unblocked Cholesky, lane i owns row i
         if (warp == 0) {
+            unsigned long long ts = (a.ptrace && lane == 0) ? globaltimer_ns() : 0;
+            auto sub = [&](int i) {
+                if (a.ptrace && lane == 0) {
+                    const unsigned long long now = globaltimer_ns();
+                    a.ptrace[8 * k + 4 + i] += now - ts;
+                    ts = now;
+                }
+            };
             double d[32];
 #pragma unroll
             for (int c = 0; c < 32; ++c) d[c] = (c <= lane) ? __ldcg(T + (int64_t)(p0 + c) * nbi + p0 + lane) : 0.0;
+            if (a.ptrace) { double z = 0; for (int c = 0; c < 32; ++c) z += d[c]; if (z == 12345.0) colb[0] = z; }
+            sub(0);
+            // Unblocked right-looking Cholesky (LAPACK dpotf2 order), lane i
+            // holding row i; the column of step j goes to the other lanes by
+            // shuffles.  sqrt and 1/sqrt are independent, so a step costs one
+            // of them rather than a square root followed by a division.  A
+            // non-positive pivot (or NaN) marks the column and the remaining
+            // steps run on harmless values: the loop stays fully unrolled.
             int failcol = -1;
+            double rdiag = 0.0;      // lane j: 1 / L(j,j)
 #pragma unroll
             for (int j = 0; j < 32; ++j) {
-                const double piv = __shfl_sync(0xffffffffu, d[j], j);
+                double piv = __shfl_sync(0xffffffffu, d[j], j);
                 if (!(piv > 0.0)) {   // LAPACK dpotf2: ajj <= 0 or NaN stops the factorization
-                    failcol = j;
-                    break;
+                    if (failcol < 0) failcol = j;
+                    piv = 1.0;
                 }
                 const double s = sqrt(piv);
-                const double rs = 1.0 / s;
+                const double rs = rsqrt(piv);
                 const double lij = (lane == j) ? s : d[j] * rs;
                 if (lane >= j) d[j] = lij;
-                colb[lane] = lij;
-                __syncwarp();
+                if (lane == j) rdiag = rs;
 #pragma unroll
-                for (int c = j + 1; c < 32; ++c)
-                    if (lane >= c) d[c] -= lij * colb[c];
-                __syncwarp();
+                for (int c = j + 1; c < 32; ++c) {
+                    const double lcj = __shfl_sync(0xffffffffu, lij, c);
+                    if (lane >= c) d[c] -= lij * lcj;
+                }
             }
+            sub(1);
             if (failcol >= 0) {
                 if (lane == 0) {
                     ctl->fail = 1;
@@ -388,16 +432,40 @@ __device__ void potrf_task(const PotrfArgs &a, SmemCtl *ctl, double *ring, int k
                     Ls[lane * 33 + c] = (c <= lane) ? d[c] : 0.0;
                 }
                 __syncwarp();
-                // inverse of the 32x32 lower block: lane c forms column c
+                sub(2);
+                // inverse of the 32x32 lower block: lane c forms column c by
+                // forward substitution, multiplying by the reciprocal pivots
+                // of the factorization, four partial sums per row
                 const int b = p0 / BLK, q0 = p0 % BLK;
                 double *Wb = Wk + (int64_t)b * BLK * BLK;
-                invert32_lower(Ls, lane, 0, [&](int i, int c, double v) {
-                    Dv[i * 33 + c] = v;
-                    Wb[(int64_t)(q0 + c) * BLK + q0 + i] = v;
-                });
+                double x[32];
+#pragma unroll
+                for (int i = 0; i < 32; ++i) {
+                    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+#pragma unroll
+                    for (int l = 0; l + 3 < i; l += 4) {
+                        s0 = fma(Ls[i * 33 + l], x[l], s0);
+                        s1 = fma(Ls[i * 33 + l + 1], x[l + 1], s1);
+                        s2 = fma(Ls[i * 33 + l + 2], x[l + 2], s2);
+                        s3 = fma(Ls[i * 33 + l + 3], x[l + 3], s3);
+                    }
+#pragma unroll
+                    for (int l = i & ~3; l < i; ++l) s0 = fma(Ls[i * 33 + l], x[l], s0);
+                    const double ri = __shfl_sync(0xffffffffu, rdiag, i);
+                    const double sum = (s0 + s1) + (s2 + s3);
+                    x[i] = (i < lane) ? 0.0 : ((i == lane) ? ri : -sum * ri);
+                }
+#pragma unroll
+                for (int i = 0; i < 32; ++i) {
+                    Dv[i * 33 + lane] = x[i];
+                    Wb[(int64_t)(q0 + lane) * BLK + q0 + i] = x[i];
+                }
+                if (a.ptrace) { __syncwarp(); if (Dv[lane * 33] == 12345.0) colb[1] = 0; }
+                sub(3);
             }
         }
         named_bar_sync(1, NCONS);
+        phase(0);
         if (ctl->fail) return;
 
         // (b) panel below the block: X = P * Dinv^T  (P = T[p0+32:, p0:p0+32])
@@ -417,6 +485,7 @@ __device__ void potrf_task(const PotrfArgs &a, SmemCtl *ctl, double *ring, int k
             }
         }
         named_bar_sync(1, NCONS);
+        phase(1);
 
         // (c) trailing update of the lower part: T22 -= X X^T (DMMA, 32x32 blocks)
         const int nb32 = R / 32;
@@ -449,6 +518,11 @@ __device__ void potrf_task(const PotrfArgs &a, SmemCtl *ctl, double *ring, int k
 #pragma unroll
                     for (int ni = 0; ni < 4; ++ni) dmma_16x8x4(acc[mi][ni], af[mi][0], af[mi][1], bf[ni]);
             }
+            // all loads first, then the stores: interleaved, every load would
+            // wait for the previous store (the compiler cannot tell the
+            // addresses apart) and the update would take one L2 round trip
+            // per element
+            double old[2][4][4];
 #pragma unroll
             for (int mi = 0; mi < 2; ++mi)
 #pragma unroll
@@ -457,17 +531,26 @@ __device__ void potrf_task(const PotrfArgs &a, SmemCtl *ctl, double *ring, int k
                     for (int q = 0; q < 4; ++q) {
                         const int r = p0 + 32 + bi * 32 + mi * 16 + g + ((q & 2) ? 8 : 0);
                         const int c = p0 + 32 + bj * 32 + ni * 8 + 2 * t + (q & 1);
-                        if (r >= c) {
-                            double *p = T + (int64_t)c * nbi + r;
-                            *p = __ldcg(p) - acc[mi][ni][q];
-                        }
+                        old[mi][ni][q] = (r >= c) ? __ldcg(T + (int64_t)c * nbi + r) : 0.0;
+                    }
+#pragma unroll
+            for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int r = p0 + 32 + bi * 32 + mi * 16 + g + ((q & 2) ? 8 : 0);
+                        const int c = p0 + 32 + bj * 32 + ni * 8 + 2 * t + (q & 1);
+                        if (r >= c) T[(int64_t)c * nbi + r] = old[mi][ni][q] - acc[mi][ni][q];
                     }
         }
         named_bar_sync(1, NCONS);
+        phase(2);
     }
 
     // Inverses of the 128x128 diagonal blocks from the 32x32 ones.
     assemble_w128(T, nbi, Wk, a.nbs, Sw, warp, lane, NCONS / 32, 1, NCONS);
+    phase(3);
 }
 
 // ---------------------------------------------------------------------------
@@ -554,22 +637,21 @@ __device__ void emit_p16_strip(const PotrfArgs &a, double *ring, int m, int k, i
 
 // ---------------------------------------------------------------------------
 // mixed precision: one update task,
-//     C(m,n)[bi, :] -= sum_{j in chunk} P16(m,j)[bi] P16(n,j)^T   (scaled back)
-// Warp 4 lane 0 issues tcgen05.mma (M=128, N=256, K=16) per 16-bit stage and
+//     C(m,n) -= sum_{j in chunk} P16(m,j) P16(n,j)^T   (scaled back)
+// Warp 4 lane 0 issues tcgen05.mma (M=128, N=256, K=16) for the two 128-row
+// halves of the tile into two TMEM accumulators (columns 0 and 256) and
 // commits each stage to its empty barrier; the split form issues hi*hi,
-// hi*lo and lo*hi into the same FP32 accumulator (split-FP16 products as in
-// Ootomo and Yokota, 2022).  Then all eight consumer warps read the 128x256
-// accumulator from TMEM (warp w: lanes 32*(w%4).., columns 128*(w/4)..) and
-// update the FP64 tile in place: the chunks of one tile run one after the
-// other, so the load-subtract-store needs no atomics.  One accumulation per
-// chunk of panels divides the traffic on C by the chunk size.
-// Returns false if a wait gave up.
+// hi*lo and lo*hi into the same FP32 accumulators (split-FP16 products as in
+// Ootomo and Yokota, 2022).  Then all eight consumer warps read the
+// accumulators (warp w: half w/4, TMEM lanes 32*(w%4)..) and update the FP64
+// tile in place: the chunks of one tile run one after the other, so the
+// load-subtract-store needs no atomics.  Returns false if a wait gave up.
 // ---------------------------------------------------------------------------
 __device__ bool mixed_update(const PotrfArgs &a, SmemCtl *ctl, unsigned char *ring16, uint64_t t, uint32_t &st16,
                              uint32_t &mx_it)
 {
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int kc = task_k(t), m = task_m(t), n = task_n(t), bi = task_bi(t);
+    const int kc = task_k(t), m = task_m(t), n = task_n(t);
     const int j0 = kc * a.mx_chunk, j1 = min(j0 + a.mx_chunk, n);
     const uint32_t tmem = ctl->tmem_base;
     const int KC = a.mx_split ? MX_KC_SPLIT : MX_KC;
@@ -590,20 +672,28 @@ __device__ bool mixed_update(const PotrfArgs &a, SmemCtl *ctl, unsigned char *ri
                 tc_fence_after();
                 const uint32_t base = smem_u32(ring16 + s * MX_STAGE_BYTES);
                 if (!a.mx_split) {
-                    const uint32_t sb = base + MX_A_BYTES;
+                    const uint32_t b = base + 2 * MX_BLOCK;
 #pragma unroll
-                    for (int k16 = 0; k16 < MX_KC / 16; ++k16)
-                        umma_f16(tmem, umma_desc_k_sw128(base + k16 * 32), umma_desc_k_sw128(sb + k16 * 32), idesc,
-                                 (i | k16) != 0);
+                    for (int k16 = 0; k16 < MX_KC / 16; ++k16) {
+                        const uint32_t o = k16 * 32, acc = (i | k16) != 0;
+                        const uint64_t bd = umma_desc_k_sw128(b + o);
+                        umma_f16(tmem, umma_desc_k_sw128(base + o), bd, idesc, acc);
+                        umma_f16(tmem + 256, umma_desc_k_sw128(base + MX_BLOCK + o), bd, idesc, acc);
+                    }
                 } else {
-                    const uint32_t ah = base, al = base + MX_SPLIT_BLOCK, bh = base + 2 * MX_SPLIT_BLOCK,
-                                   bl = base + 4 * MX_SPLIT_BLOCK;
+                    const uint32_t ah = base, al = base + 2 * MX_SPLIT_BLOCK, bh = base + 4 * MX_SPLIT_BLOCK,
+                                   bl = base + 6 * MX_SPLIT_BLOCK;
 #pragma unroll
                     for (int k16 = 0; k16 < MX_KC_SPLIT / 16; ++k16) {
-                        const uint32_t o = k16 * 32;
-                        umma_f16(tmem, umma_desc_k_sw64(ah + o), umma_desc_k_sw64(bh + o), idesc, (i | k16) != 0);
-                        umma_f16(tmem, umma_desc_k_sw64(ah + o), umma_desc_k_sw64(bl + o), idesc, 1);
-                        umma_f16(tmem, umma_desc_k_sw64(al + o), umma_desc_k_sw64(bh + o), idesc, 1);
+                        const uint32_t o = k16 * 32, acc = (i | k16) != 0;
+                        const uint64_t bhd = umma_desc_k_sw64(bh + o), bld = umma_desc_k_sw64(bl + o);
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            const uint32_t d = tmem + 256 * h, ho = h * MX_SPLIT_BLOCK;
+                            umma_f16(d, umma_desc_k_sw64(ah + ho + o), bhd, idesc, acc);
+                            umma_f16(d, umma_desc_k_sw64(ah + ho + o), bld, idesc, 1);
+                            umma_f16(d, umma_desc_k_sw64(al + ho + o), bhd, idesc, 1);
+                        }
                     }
                 }
                 umma_commit(&ctl->empty16[s]);
@@ -621,23 +711,25 @@ __device__ bool mixed_update(const PotrfArgs &a, SmemCtl *ctl, unsigned char *ri
     } else if (!__shfl_sync(0xffffffffu, ld_volatile(a.abort_flag), 0)) {
         tc_fence_after();
         const int lb = (warp & 3) * 32, half = warp >> 2;
-        const int row = lb + lane;                                 // within the 128-row block
-        double *C = tile_ptr(a, m, n) + bi * BLK + row;            // column stride nbi
-        for (int c0 = half * 128; c0 < half * 128 + 128; c0 += 32) {
+        const int row = half * BLK + lb + lane;                    // within the tile
+        double *C = tile_ptr(a, m, n) + row;                       // column stride nbi
+        const double sr = (double)a.scl[m * a.nbs + half];
+        for (int c0 = 0; c0 < a.nbi; c0 += 32) {
+            if (m == n && c0 > row - lane + 31) break;             // above the diagonal
             float v[32];
-            tmem_ld32(tmem + ((uint32_t)lb << 16) + (uint32_t)c0, v);
-            // row scales are the same for every panel: one power of two per block
-            const double inv = 1.0 / ((double)a.scl[m * a.nbs + bi] * (double)a.scl[n * a.nbs + c0 / BLK]);
+            tmem_ld32(tmem + ((uint32_t)lb << 16) + (uint32_t)(256 * half + c0), v);
+            // row and column scales are the same for every panel
+            const double inv = 1.0 / (sr * (double)a.scl[n * a.nbs + c0 / BLK]);
             double cv[32];
 #pragma unroll
             for (int j = 0; j < 32; ++j) {
                 const int col = c0 + j;
-                cv[j] = (m != n || bi * BLK + row >= col) ? __ldcg(C + (int64_t)col * a.nbi) : 0.0;
+                cv[j] = (m != n || row >= col) ? __ldcg(C + (int64_t)col * a.nbi) : 0.0;
             }
 #pragma unroll
             for (int j = 0; j < 32; ++j) {
                 const int col = c0 + j;
-                if (m != n || bi * BLK + row >= col) __stcg(C + (int64_t)col * a.nbi, cv[j] - (double)v[j] * inv);
+                if (m != n || row >= col) __stcg(C + (int64_t)col * a.nbi, cv[j] - (double)v[j] * inv);
             }
         }
         __threadfence();
@@ -788,7 +880,10 @@ size_t potrf_smem_bytes(bool mixed)
     const size_t ctl = ((sizeof(SmemCtl) + 127) / 128) * 128;
     if (!mixed) return ctl + (size_t)NSTAGE * STAGE_DOUBLES * sizeof(double);
     // FP64 ring, then the 16-bit ring aligned to 1024 B (worst-case padding)
-    return ctl + (size_t)NSTAGE_MIXED * STAGE_DOUBLES * sizeof(double) + 1024 + (size_t)MX_NST * MX_STAGE_BYTES;
+    // one region for the FP64 ring, POTRF scratch and the 1024-aligned 16-bit ring
+    const size_t fp64 = (size_t)NSTAGE_MIXED * STAGE_DOUBLES * sizeof(double);
+    const size_t r16 = 1024 + (size_t)MX_NST * MX_STAGE_BYTES;
+    return ctl + (fp64 > r16 ? fp64 : r16);
 }
 size_t potrf_smem_bytes() { return potrf_smem_bytes(false); }
 
@@ -837,8 +932,8 @@ std::vector<uint64_t> build_potrf_tasks(int mt, int nbs, int delay)
 }
 
 // Mixed-precision ticket order.  An update task (k = chunk c) applies the
-// panels j in [c*S, min(c*S+S, n)) to the 128-row block bi of tile (m,n).
-// Each tile column n gets one chunk task per block and chunk: the partial
+// panels j in [c*S, min(c*S+S, n)) to the whole tile (m,n).  Each tile
+// column n gets one task per tile and chunk: the partial
 // chunk that ends at panel n-1 in step n-1 (the critical column), a full
 // chunk once its last panel is done.  A full chunk c closes in step
 // k = c*S+S-1; its tasks for the columns n >= k+2 are spread over the steps
@@ -864,8 +959,7 @@ std::vector<uint64_t> build_potrf_tasks_mixed(int mt, int nbs, int delay, int S)
         for (int n = k + 2; n < mt; ++n) {
             int part = (int)((done * S) / (work > 0 ? work : 1));
             part = std::min(part, std::min(S - 1, n - 2 - k));
-            for (int m = n; m < mt; ++m)
-                for (int bi = 0; bi < nbs; ++bi) share[k + part].push_back(make_task(T_GEMM, c, m, n, bi, 0));
+            for (int m = n; m < mt; ++m) share[k + part].push_back(make_task(T_GEMM, c, m, n, 0, 0));
             done += mt - n;
         }
     }
@@ -873,8 +967,7 @@ std::vector<uint64_t> build_potrf_tasks_mixed(int mt, int nbs, int delay, int S)
     push_trsm(0);
     for (int k = 0; k + 1 < mt; ++k) {
         const int c = k / S;
-        for (int m = k + 1; m < mt; ++m)
-            for (int bi = 0; bi < nbs; ++bi) v.push_back(make_task(T_GEMM, c, m, k + 1, bi, 0));
+        for (int m = k + 1; m < mt; ++m) v.push_back(make_task(T_GEMM, c, m, k + 1, 0, 0));
         v.push_back(make_task(T_POTRF, k + 1, k + 1, k + 1, 0, 0));
         const std::vector<uint64_t> &rest = share[k];
         const size_t d = std::min<size_t>(rest.size(), (size_t)std::max(delay, 0));
@@ -982,6 +1075,7 @@ int potrf_run(Context *ctx, double *dA, int mt, int nbi, int nb_user, int n_user
     a.task_count = a.upd_done + (size_t)mt * mt;
     a.diag = ctr + 4;
     a.trace = nullptr;
+    a.ptrace = nullptr;
     if (ctx->trace_path[0]) {
         const size_t tbytes = ((size_t)a.ntasks * 4 + 6 * (size_t)grid) * sizeof(unsigned long long) + (size_t)a.ntasks * sizeof(int);
         a.trace = (unsigned long long *)ctx->buffer(BUF_TRACE, tbytes);
@@ -989,6 +1083,9 @@ int potrf_run(Context *ctx, double *dA, int mt, int nbi, int nb_user, int n_user
         a.trace_exit = a.trace + (size_t)a.ntasks * 4;
         a.trace_cta = (int *)(a.trace_exit + 6 * (size_t)grid);
         CK(cudaMemsetAsync(a.trace, 0, tbytes, st));
+        a.ptrace = (unsigned long long *)ctx->buffer(BUF_PTRACE, (size_t)mt * 8 * sizeof(unsigned long long));
+        if (!a.ptrace) return DPLASMA_ERR_OUT_OF_RESOURCES;
+        CK(cudaMemsetAsync(a.ptrace, 0, (size_t)mt * 8 * sizeof(unsigned long long), st));
     }
     a.dep_limit_ns = ctx->dep_limit_ns;
     a.pipe_limit_ns = ctx->pipe_limit_ns;
@@ -1076,6 +1173,12 @@ int potrf_run(Context *ctx, double *dA, int mt, int nbi, int nb_user, int n_user
                         task_n(t), task_bi(t), task_bj(t), rel(tr[4 * i]), rel(tr[4 * i + 1]), rel(tr[4 * i + 2]),
                         rel(tr[4 * i + 3]), tc[i]);
             }
+            std::vector<unsigned long long> pt((size_t)mt * 8);
+            cudaMemcpy(pt.data(), a.ptrace, pt.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost);
+            for (int k = 0; k < mt; ++k)
+                fprintf(f, "# potrf %d diag_ns %llu panel_ns %llu update_ns %llu inverse_ns %llu load_ns %llu chol_ns %llu "
+                           "store_ns %llu inv32_ns %llu\n", k, pt[8 * k], pt[8 * k + 1], pt[8 * k + 2], pt[8 * k + 3],
+                        pt[8 * k + 4], pt[8 * k + 5], pt[8 * k + 6], pt[8 * k + 7]);
             for (int c = 0; c < grid; ++c)
                 fprintf(f, "# cta %d producer_exit %lld consumer_exit %lld potrf_wait_done %lld end_pushed %lld end_seen %lld\n", c,
                         rel(tx[6 * c]), rel(tx[6 * c + 1]), rel(tx[6 * c + 2]), rel(tx[6 * c + 3]), rel(tx[6 * c + 4]));
@@ -1183,6 +1286,7 @@ int potrf_launch_prealloc(cudaStream_t st, double *dA, int mt, int nbi, int nb_u
     a.trace = nullptr;
     a.trace_exit = nullptr;
     a.trace_cta = nullptr;
+    a.ptrace = nullptr;
     a.dep_limit_ns = limit_ns;
     a.pipe_limit_ns = limit_ns;
     a.P16 = nullptr;

@@ -40,21 +40,26 @@ constexpr int CONSUMER_REGS = 224;
 constexpr int TASKQ = 4;         // task ring depth
 constexpr int STAGE_DOUBLES = 2 * BK * SP;
 
-// Mixed-precision variant (16-bit tensor-core updates, nbi = 256): the FP64
-// ring keeps NSTAGE_MIXED stages for the TRSM jobs, and a second ring holds
-// MX_NST stages of 16-bit operands in the swizzled K-major layout of the UMMA
-// descriptors.  One stage is 48 KB either way:
-//   single 16-bit operands: A (128 rows x 64) and B (256 rows x 64), 128-byte swizzle;
-//   split FP16 (hi + lo):   A_hi, A_lo (128 x 32) and B_hi, B_lo (256 x 32), 64-byte swizzle.
+// Mixed-precision variant (16-bit tensor-core updates, nbi = 256).  An update
+// task covers a whole 256x256 tile: two 128x256 FP32 accumulators in tensor
+// memory share the B operand.  The 16-bit ring holds MX_NST stages of 64 KB
+// in the swizzled K-major layout of the UMMA descriptors, made of 8 KB
+// blocks of 128 rows:
+//   single 16-bit operands (K = 64 per stage, 128-byte swizzle, 16 KB blocks):
+//       A rows 0-127 | A rows 128-255 | B rows 0-255
+//   split FP16 (K = 32, 64-byte swizzle, 8 KB blocks):
+//       A_hi 0-127 | A_hi 128-255 | A_lo 0-127 | A_lo 128-255 | B_hi 0-255 | B_lo 0-255
+// The same shared memory serves as the FP64 ring (NSTAGE_MIXED stages) of
+// the TRSM jobs and as POTRF scratch: the producer drains one use before it
+// starts the other.
 constexpr int NSTAGE_MIXED = 3;
 constexpr int MX_KC = 64;                          // K per 16-bit stage, single operands
 constexpr int MX_KC_SPLIT = 32;                    // K per 16-bit stage, split operands
-constexpr int MX_NST = 2;
-constexpr int MX_A_BYTES = BLK * MX_KC * 2;        // 16 KB
-constexpr int MX_B_BYTES = 2 * BLK * MX_KC * 2;    // 32 KB
-constexpr int MX_STAGE_BYTES = MX_A_BYTES + MX_B_BYTES;
+constexpr int MX_NST = 3;
+constexpr int MX_STAGE_BYTES = 64 * 1024;
+constexpr int MX_BLOCK = BLK * MX_KC * 2;          // 16 KB: 128 rows of a single operand
 constexpr int MX_SPLIT_BLOCK = BLK * MX_KC_SPLIT * 2;   // 8 KB: 128 rows of one split half
-constexpr int MX_TMEM_COLS = 256;                  // 128 x 256 FP32 accumulator
+constexpr int MX_TMEM_COLS = 512;                  // two 128 x 256 FP32 accumulators
 constexpr int MX_NB = 256;
 
 // Task encoding (64 bits): type[0:4) k[4:20) m[20:36) n[36:52) bi[52:56) bj[56:60)
@@ -91,6 +96,7 @@ struct PotrfArgs {
     unsigned long long *trace; // opt-in, 4 per ticket: fetched, dependencies met, started, finished (ns); may be null
     unsigned long long *trace_exit; // 2 per CTA: producer and consumer exit times
     int *trace_cta;        // CTA that ran each ticket
+    unsigned long long *ptrace; // opt-in, 4 per POTRF(k): ns spent in its diagonal blocks, panels, updates, inverses
     uint64_t dep_limit_ns; // bounded dependency waits
     uint64_t pipe_limit_ns;// bounded pipeline waits
     // mixed precision: 16-bit K-major copies of the panel tiles and their

@@ -6,7 +6,7 @@ every task's dependencies are produced by tasks earlier in the order.  The
 rules replayed here are the ones the kernel waits on (the dataflow of
 src/zpotrf_L.jdf as per-tile completion counts), for the FP64 list (one task
 per 128x128 block and panel) and the mixed-precision list (one task per
-128-row block and chunk of S panels)."""
+tile and chunk of S panels)."""
 import ctypes
 
 import numpy as np
@@ -35,7 +35,7 @@ def replay(tl, mt, nbs, S):
 
     def all_updates(m, n):
         if S:
-            return -(-n // S) * nbs
+            return -(-n // S)
         return n * (nbs * (nbs + 1) // 2 if m == n else nbs * nbs)
 
     for i, (ty, k, m, n, bi, bj) in enumerate(tl):
@@ -49,7 +49,7 @@ def replay(tl, mt, nbs, S):
             assert ty == T_GEMM
             if S:
                 kl = min(k * S + S, n) - 1
-                assert trsm[m, kl] == nbs and trsm[n, kl] == nbs and upd[m, n] >= k * nbs, (i, k, m, n)
+                assert trsm[m, kl] == nbs and trsm[n, kl] == nbs and upd[m, n] >= k, (i, k, m, n)
             else:
                 assert trsm[m, k] == nbs and trsm[n, k] == nbs, (i, k, m, n)
                 step = nbs * (nbs + 1) // 2 if m == n else nbs * nbs
