@@ -313,7 +313,8 @@ def run_gpu(args):
     sweep = []
     if args.sweep:
         for kappa in (1e2, 1e4, 1e6):
-            if kappa != args.kappa:
+            # A_pristine holds the headline matrix until the first regeneration
+            if kappa != args.kappa or sweep:
                 generate(kappa)
                 t64, Xk, _, _ = fp64_solve()
             else:

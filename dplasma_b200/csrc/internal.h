@@ -2,6 +2,7 @@
 // GPU, one stream, grow-only device buffers, cached task lists) and the
 // functions the C ABI layer calls.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdarg.h>
 #include <stdint.h>
@@ -106,6 +107,8 @@ int potrf_device(Context *ctx, double *dA, int mt, int nbi, int nb_user, int n_u
 // p16_fmt < 0: FP64 updates; 0/1/2: FP16/BF16/split-FP16 tensor-core updates (nbi == 256)
 int potrf_run(Context *ctx, double *dA, int mt, int nbi, int nb_user, int n_user, int *info, int p16_fmt);
 int potrf_max_blocks_per_sm(bool mixed);
+int encode_map_2d(Context *ctx, CUtensorMap *map, CUtensorMapDataType type, void *base, uint64_t dim0, uint64_t dim1,
+                  uint64_t stride1, uint32_t box0, uint32_t box1, CUtensorMapSwizzle swz);
 
 // layout.cu : caller layout <-> device tiles
 int upload_sym(Context *ctx, const parsec_tiled_matrix_t *A, dplasma_enum_t uplo, const Geom &g, double *dA);

@@ -341,6 +341,35 @@ __device__ __forceinline__ bool consume_job(const PotrfArgs &a, SmemCtl *ctl, co
     return true;
 }
 
+// One step j of the unblocked right-looking Cholesky of a 32x32 block held
+// by one warp, lane i holding row i in d[]: the recursion over j is resolved
+// at compile time, so every d[] index is a constant and the row stays in
+// registers (a runtime loop of this size may be left rolled, which moves d[]
+// to local memory).  LAPACK dpotf2 order; sqrt and 1/sqrt are independent,
+// so a step costs one of them rather than a square root and a division.  A
+// non-positive pivot (or NaN) marks the column and the remaining steps run
+// on harmless values.
+template <int J>
+__device__ __forceinline__ void chol32_step(double (&d)[32], int lane, int &failcol, double &rdiag)
+{
+    double piv = __shfl_sync(0xffffffffu, d[J], J);
+    if (!(piv > 0.0)) {   // LAPACK dpotf2: ajj <= 0 or NaN stops the factorization
+        if (failcol < 0) failcol = J;
+        piv = 1.0;
+    }
+    const double s = sqrt(piv);
+    const double rs = rsqrt(piv);
+    const double lij = (lane == J) ? s : d[J] * rs;
+    if (lane >= J) d[J] = lij;
+    if (lane == J) rdiag = rs;
+#pragma unroll
+    for (int c = J + 1; c < 32; ++c) {
+        const double lcj = __shfl_sync(0xffffffffu, lij, c);
+        if (lane >= c) d[c] -= lij * lcj;
+    }
+    if constexpr (J + 1 < 32) chol32_step<J + 1>(d, lane, failcol, rdiag);
+}
+
 // ---------------------------------------------------------------------------
 // consumers: POTRF(k) of one diagonal tile + inverses of its 128x128 diagonal
 // blocks (src/zpotrf_L.jdf:194-206 computes the factor with
@@ -391,32 +420,9 @@ __device__ void potrf_task(const PotrfArgs &a, SmemCtl *ctl, double *ring, int k
             for (int c = 0; c < 32; ++c) d[c] = (c <= lane) ? __ldcg(T + (int64_t)(p0 + c) * nbi + p0 + lane) : 0.0;
             if (a.ptrace) { double z = 0; for (int c = 0; c < 32; ++c) z += d[c]; if (z == 12345.0) colb[0] = z; }
             sub(0);
-            // Unblocked right-looking Cholesky (LAPACK dpotf2 order), lane i
-            // holding row i; the column of step j goes to the other lanes by
-            // shuffles.  sqrt and 1/sqrt are independent, so a step costs one
-            // of them rather than a square root followed by a division.  A
-            // non-positive pivot (or NaN) marks the column and the remaining
-            // steps run on harmless values: the loop stays fully unrolled.
             int failcol = -1;
             double rdiag = 0.0;      // lane j: 1 / L(j,j)
-#pragma unroll
-            for (int j = 0; j < 32; ++j) {
-                double piv = __shfl_sync(0xffffffffu, d[j], j);
-                if (!(piv > 0.0)) {   // LAPACK dpotf2: ajj <= 0 or NaN stops the factorization
-                    if (failcol < 0) failcol = j;
-                    piv = 1.0;
-                }
-                const double s = sqrt(piv);
-                const double rs = rsqrt(piv);
-                const double lij = (lane == j) ? s : d[j] * rs;
-                if (lane >= j) d[j] = lij;
-                if (lane == j) rdiag = rs;
-#pragma unroll
-                for (int c = j + 1; c < 32; ++c) {
-                    const double lcj = __shfl_sync(0xffffffffu, lij, c);
-                    if (lane >= c) d[c] -= lij * lcj;
-                }
-            }
+            chol32_step<0>(d, lane, failcol, rdiag);
             sub(1);
             if (failcol >= 0) {
                 if (lane == 0) {
@@ -987,7 +993,11 @@ std::vector<uint64_t> build_potrf_tasks_mixed(int mt, int nbs, int delay, int S)
 typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-static int make_p16_map(Context *ctx, CUtensorMap *map, void *P16, size_t rows, int nbi, int fmt, bool split)
+
+// 2-D tiled tensor map (the driver's encoder, fetched through the runtime):
+// dim0 contiguous elements, dim1 rows `stride1` bytes apart, boxes box0 x box1.
+int encode_map_2d(Context *ctx, CUtensorMap *map, CUtensorMapDataType type, void *base, uint64_t dim0, uint64_t dim1,
+                  uint64_t stride1, uint32_t box0, uint32_t box1, CUtensorMapSwizzle swz)
 {
     static EncodeTiledFn encode = nullptr;
     if (!encode) {
@@ -1000,19 +1010,24 @@ static int make_p16_map(Context *ctx, CUtensorMap *map, void *P16, size_t rows, 
         }
         encode = (EncodeTiledFn)fn;
     }
-    const cuuint64_t dims[2] = {(cuuint64_t)nbi, (cuuint64_t)rows};
-    const cuuint64_t strides[1] = {(cuuint64_t)nbi * 2};
-    const cuuint32_t box[2] = {(cuuint32_t)(split ? MX_KC_SPLIT : MX_KC), BLK};
+    const cuuint64_t dims[2] = {(cuuint64_t)dim0, (cuuint64_t)dim1};
+    const cuuint64_t strides[1] = {(cuuint64_t)stride1};
+    const cuuint32_t box[2] = {box0, box1};
     const cuuint32_t estr[2] = {1, 1};
-    const CUresult r = encode(map, fmt ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16, 2, P16, dims,
-                              strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                              split ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B,
+    const CUresult r = encode(map, type, 2, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, swz,
                               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) {
         ctx->set_error("cuTensorMapEncodeTiled failed (%d)", (int)r);
         return DPLASMA_ERR_UNEXPECTED;
     }
     return 0;
+}
+
+static int make_p16_map(Context *ctx, CUtensorMap *map, void *P16, size_t rows, int nbi, int fmt, bool split)
+{
+    return encode_map_2d(ctx, map, fmt ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16, P16,
+                         (uint64_t)nbi, (uint64_t)rows, (uint64_t)nbi * 2, split ? MX_KC_SPLIT : MX_KC, BLK,
+                         split ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B);
 }
 
 int potrf_device(Context *ctx, double *dA, int mt, int nbi, int nb_user, int n_user, int *info)

@@ -15,9 +15,23 @@
 // path per block is one flag, one 128x128 update and the diagonal multiply,
 // while the bulk of L streams from HBM on all SMs at once.  CTAs wait on one
 // another, hence the cooperative launch.
+//
+// L and W arrive by TMA tensor loads with the 128-byte swizzle (a stage of
+// 32 KB takes 8 or 2 loads).  The stage holds 16-row slabs of 128-byte lines
+// [line][16 doubles], whose 16-byte chunks are XOR-ed with the line index
+// modulo 8.  To read the FP64 MMA fragments (a0 = A[g][t], a1 = A[g+8][t])
+// without bank conflicts, the 16 rows of a warp's m-tile are visited in a
+// permuted order: MMA row i stands for row pi(i) of the tile (forward: the
+// rows are the slab's elements, pi = 0,1,8,9,4,5,12,13, 2,3,10,11,6,7,14,15)
+// or sigma(i) (backward: the rows are the slab's lines,
+// sigma = 0,2,4,6,8,10,12,14, 1,3,5,7,9,11,13,15); every half-warp then
+// touches 16 distinct bank pairs.  Accumulators, staging and stores follow
+// the same permutation.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "dev_common.cuh"
+#include "dev_tcgen05.cuh"
 #include "internal.h"
 
 namespace db2 {
@@ -25,9 +39,7 @@ namespace db2 {
 constexpr int WV_RMAX = 4;
 constexpr int WV_KS = 32;
 constexpr int WV_NST = 3;
-constexpr int WV_APF = 132;            // forward stage: As[kk][r]
-constexpr int WV_APB = 36;             // backward stage: As[r][kk]
-constexpr int WV_A_DOUBLES = 128 * 36; // >= 32 * 132
+constexpr int WV_A_DOUBLES = 128 * 32;  // one stage: 32 KB of swizzled slabs
 constexpr int WV_YP = 132;             // Y stage [n][k], k < 128 (two of them)
 constexpr int WV_THREADS = 384;
 
@@ -49,11 +61,32 @@ struct __align__(16) WaveCtl {
     uint64_t empty[WV_NST];
 };
 
-__device__ __forceinline__ const double *wv_lblock(const WaveArgs &a, int p, int q)
+// Tensor-map coordinates of the 128x128 block (p, q) of L: x = row within
+// the tile column, y = tile * nbi + column.
+__device__ __forceinline__ void wv_lcoord(const WaveArgs &a, int p, int q, int &x, int &y)
 {
     const int tp = p / a.nbs, tq = q / a.nbs;
-    return a.A + lower_tile_index(tp, tq, a.mt) * (int64_t)a.nbi * a.nbi + (int64_t)(q % a.nbs) * 128 * a.nbi +
-           (p % a.nbs) * 128;
+    x = (p % a.nbs) * 128;
+    y = (int)(lower_tile_index(tp, tq, a.mt) * a.nbi) + (q % a.nbs) * 128;
+}
+
+// MMA row i of a warp's 16-row m-tile -> row of the tile (see above)
+template <bool TRANS>
+__device__ __forceinline__ int wv_perm(int i)
+{
+    return TRANS ? 2 * (i & 3) + 8 * ((i >> 2) & 1) + (i >> 3)
+                 : (i & 1) + 8 * ((i >> 1) & 1) + 4 * ((i >> 2) & 1) + 2 * (i >> 3);
+}
+// Element (row r of the stage's A operand, k) in a swizzled stage.
+//   forward:  slab = r / 16 (16 rows), line = k (32 lines of 16 rows)
+//   backward: slab = k / 16 (16 k), line = r (128 lines of 16 k)
+template <bool TRANS>
+__device__ __forceinline__ int wv_aidx(int r, int k)
+{
+    const int slab = TRANS ? (k >> 4) : (r >> 4);
+    const int line = TRANS ? r : k;
+    const int j = TRANS ? (k & 15) : (r & 15);
+    return (TRANS ? slab * 2048 : slab * 512) + line * 16 + ((((j >> 1) ^ (line & 7)) << 1) | (j & 1));
 }
 
 // Solve order position qi -> block q, and its successor.
@@ -61,11 +94,14 @@ template <bool TRANS>
 __device__ __forceinline__ int wv_block(int qi, int P) { return TRANS ? P - 1 - qi : qi; }
 
 template <int NC, bool TRANS>
-__global__ void __launch_bounds__(WV_THREADS, 1) trsm_wave_kernel(WaveArgs a)
+__global__ void __launch_bounds__(WV_THREADS, 1)
+    trsm_wave_kernel(WaveArgs a, const __grid_constant__ CUtensorMap lmap, const __grid_constant__ CUtensorMap wmap)
 {
-    extern __shared__ __align__(128) unsigned char smraw[];
+    extern __shared__ __align__(1024) unsigned char smraw[];
     WaveCtl *ctl = reinterpret_cast<WaveCtl *>(smraw);
-    double *ring = reinterpret_cast<double *>(smraw + 128);
+    // stages 1024-byte aligned in the shared window (swizzle atoms)
+    const uint32_t sbase = smem_u32(smraw);
+    double *ring = reinterpret_cast<double *>(smraw + ((((sbase + 128 + 1023u) & ~1023u)) - sbase));
     double *Ybuf = ring + WV_NST * WV_A_DOUBLES;   // two Y stages of 32 x WV_YP
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int c = blockIdx.x, G = gridDim.x, P = a.nblk;
@@ -86,7 +122,14 @@ __global__ void __launch_bounds__(WV_THREADS, 1) trsm_wave_kernel(WaveArgs a)
         if (warp != 8) return;
         uint32_t it = 0;
         bool ok = true;
-        auto issue = [&](const double *src, int ld) {
+        if (lane == 0) {
+            tma_prefetch_desc(&lmap);
+            tma_prefetch_desc(&wmap);
+        }
+        // one 128x128 block whose element (row, col) of the A operand is at
+        // map coordinates: forward (x0 + row, y0 + col), backward
+        // (x0 + col, y0 + row) -- op(A) is the transpose
+        auto issue = [&](const CUtensorMap *map, int x0, int y0) {
             for (int s0 = 0; s0 < 128 && ok; s0 += WV_KS) {
                 const uint32_t s = it % WV_NST, r = it / WV_NST;
                 if (r > 0 && !warp_mbar_wait(&ctl->empty[s], (r - 1) & 1, a.limit_ns)) {
@@ -95,33 +138,41 @@ __global__ void __launch_bounds__(WV_THREADS, 1) trsm_wave_kernel(WaveArgs a)
                     break;
                 }
                 double *As = ring + s * WV_A_DOUBLES;
-                if (lane == 0) mbar_arrive_expect_tx(&ctl->full[s], 128 * WV_KS * (uint32_t)sizeof(double));
-                __syncwarp();
-                if (!TRANS) {
-                    bulk_g2s(As + lane * WV_APF, src + (int64_t)(s0 + lane) * ld, 128 * sizeof(double), &ctl->full[s]);
-                } else {
+                if (lane == 0) {
+                    mbar_arrive_expect_tx(&ctl->full[s], 128 * WV_KS * (uint32_t)sizeof(double));
+                    if (!TRANS) {
 #pragma unroll
-                    for (int j = 0; j < 4; ++j) {
-                        const int r2 = lane + 32 * j;
-                        bulk_g2s(As + r2 * WV_APB, src + (int64_t)r2 * ld + s0, WV_KS * sizeof(double), &ctl->full[s]);
+                        for (int slab = 0; slab < 8; ++slab)     // 16 rows x 32 columns each
+                            tma_load_2d(As + slab * 512, map, x0 + slab * 16, y0 + s0, &ctl->full[s]);
+                    } else {
+#pragma unroll
+                        for (int slab = 0; slab < 2; ++slab)     // 16 k x 128 columns each
+                            tma_load_2d(As + slab * 2048, map, x0 + s0 + slab * 16, y0, &ctl->full[s]);
                     }
                 }
+                __syncwarp();
                 ++it;
             }
         };
+        auto issue_l = [&](int p, int q) {   // op(L)_pq
+            int x, y;
+            if (TRANS) wv_lcoord(a, q, p, x, y);
+            else wv_lcoord(a, p, q, x, y);
+            issue(&lmap, x, y);
+        };
         const int first = wv_block<TRANS>(0, P);
-        if (first % G == c) issue(a.W + (int64_t)first * 128 * 128, 128);
+        if (first % G == c) issue(&wmap, 0, first * 128);
         for (int qi = 0; qi < P && ok; ++qi) {
             const int q = wv_block<TRANS>(qi, P);
             const int nq = (qi + 1 < P) ? wv_block<TRANS>(qi + 1, P) : -1;
             if (nq >= 0 && nq % G == c) {
-                issue(TRANS ? wv_lblock(a, q, nq) : wv_lblock(a, nq, q), a.nbi);
-                issue(a.W + (int64_t)nq * 128 * 128, 128);
+                issue_l(nq, q);
+                issue(&wmap, 0, nq * 128);
             }
             for (int i = 0; i < WV_RMAX && ok; ++i) {
                 const int p = c + i * G;
                 if (p >= P || p == nq || !(TRANS ? p < q : p > q)) continue;
-                issue(TRANS ? wv_lblock(a, q, p) : wv_lblock(a, p, q), a.nbi);
+                issue_l(p, q);
             }
         }
         const uint32_t fst = it > WV_NST ? it - WV_NST : 0;
@@ -132,6 +183,7 @@ __global__ void __launch_bounds__(WV_THREADS, 1) trsm_wave_kernel(WaveArgs a)
     asm volatile("setmaxnreg.inc.sync.aligned.u32 224;\n");
     constexpr int NT = NC / 8;
     const int g = lane >> 2, t = lane & 3;
+    const int ra = warp * 16 + wv_perm<TRANS>(g), rb = warp * 16 + wv_perm<TRANS>(g + 8);   // fragment rows
     double acc[WV_RMAX][NT][4];
 #pragma unroll
     for (int i = 0; i < WV_RMAX; ++i) {
@@ -140,7 +192,7 @@ __global__ void __launch_bounds__(WV_THREADS, 1) trsm_wave_kernel(WaveArgs a)
         for (int ni = 0; ni < NT; ++ni)
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
-                const int r = warp * 16 + g + ((e & 2) ? 8 : 0);
+                const int r = warp * 16 + wv_perm<TRANS>(g + ((e & 2) ? 8 : 0));
                 const int col = ni * 8 + 2 * t + (e & 1);
                 acc[i][ni][e] = (p < P) ? a.alpha * __ldcg(a.Y + (int64_t)(a.c0 + col) * a.ldy + (int64_t)p * 128 + r)
                                         : 0.0;
@@ -161,14 +213,8 @@ __global__ void __launch_bounds__(WV_THREADS, 1) trsm_wave_kernel(WaveArgs a)
             const double *As = ring + s * WV_A_DOUBLES;
 #pragma unroll
             for (int kk = 0; kk < WV_KS; kk += 4) {
-                double a0, a1;
-                if (!TRANS) {
-                    a0 = As[(kk + t) * WV_APF + warp * 16 + g];
-                    a1 = As[(kk + t) * WV_APF + warp * 16 + g + 8];
-                } else {
-                    a0 = As[(warp * 16 + g) * WV_APB + kk + t];
-                    a1 = As[(warp * 16 + g + 8) * WV_APB + kk + t];
-                }
+                const double a0 = As[wv_aidx<TRANS>(ra, kk + t)];
+                const double a1 = As[wv_aidx<TRANS>(rb, kk + t)];
 #pragma unroll
                 for (int ni = 0; ni < NT; ++ni) dmma_16x8x4(ac[ni], -a0, -a1, Yst[(ni * 8 + g) * WV_YP + s0 + kk + t]);
             }
@@ -183,7 +229,7 @@ __global__ void __launch_bounds__(WV_THREADS, 1) trsm_wave_kernel(WaveArgs a)
         for (int ni = 0; ni < NT; ++ni)
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
-                const int r = warp * 16 + g + ((e & 2) ? 8 : 0);
+                const int r = (e & 2) ? rb : ra;
                 const int col = ni * 8 + 2 * t + (e & 1);
                 Yst[col * WV_YP + r] = ac[ni][e];
                 ac[ni][e] = 0.0;
@@ -203,15 +249,9 @@ __global__ void __launch_bounds__(WV_THREADS, 1) trsm_wave_kernel(WaveArgs a)
             }
             const double *As = ring + s * WV_A_DOUBLES;
 #pragma unroll
-            for (int kk = 0; kk < WV_KS; kk += 4) {
-                double a0, a1;
-                if (!TRANS) {   // A = W: rows of W are the ring's columns
-                    a0 = As[(kk + t) * WV_APF + warp * 16 + g];
-                    a1 = As[(kk + t) * WV_APF + warp * 16 + g + 8];
-                } else {        // A = W^T
-                    a0 = As[(warp * 16 + g) * WV_APB + kk + t];
-                    a1 = As[(warp * 16 + g + 8) * WV_APB + kk + t];
-                }
+            for (int kk = 0; kk < WV_KS; kk += 4) {   // A = W (forward) or W^T (backward)
+                const double a0 = As[wv_aidx<TRANS>(ra, kk + t)];
+                const double a1 = As[wv_aidx<TRANS>(rb, kk + t)];
 #pragma unroll
                 for (int ni = 0; ni < NT; ++ni) dmma_16x8x4(res[ni], a0, a1, Yst[(ni * 8 + g) * WV_YP + s0 + kk + t]);
             }
@@ -225,7 +265,7 @@ __global__ void __launch_bounds__(WV_THREADS, 1) trsm_wave_kernel(WaveArgs a)
         for (int ni = 0; ni < NT; ++ni)
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
-                const int r = warp * 16 + g + ((e & 2) ? 8 : 0);
+                const int r = (e & 2) ? rb : ra;
                 const int col = ni * 8 + 2 * t + (e & 1);
                 Yst[col * WV_YP + r] = res[ni][e];
                 Yq[(int64_t)col * a.ldy + r] = res[ni][e];
@@ -286,12 +326,18 @@ __global__ void __launch_bounds__(WV_THREADS, 1) trsm_wave_kernel(WaveArgs a)
     }
 }
 
-template <int NC, bool TRANS>
-static int launch_wave(Context *ctx, WaveArgs &a, int grid)
+static size_t wave_smem_bytes()
 {
-    const size_t smem = 128 + (size_t)(WV_NST * WV_A_DOUBLES + 2 * 32 * WV_YP) * sizeof(double);
+    // control block, worst-case alignment of the stages, stages, Y stages
+    return 128 + 1024 + (size_t)(WV_NST * WV_A_DOUBLES + 2 * 32 * WV_YP) * sizeof(double);
+}
+
+template <int NC, bool TRANS>
+static int launch_wave(Context *ctx, WaveArgs &a, int grid, CUtensorMap &lmap, CUtensorMap &wmap)
+{
+    const size_t smem = wave_smem_bytes();
     CK(cudaFuncSetAttribute(trsm_wave_kernel<NC, TRANS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    void *args[] = {&a};
+    void *args[] = {&a, &lmap, &wmap};
     CK(cudaLaunchCooperativeKernel((const void *)trsm_wave_kernel<NC, TRANS>, dim3(grid), dim3(WV_THREADS), args, smem,
                                    ctx->stream));
     ctx->launches++;
@@ -300,7 +346,7 @@ static int launch_wave(Context *ctx, WaveArgs &a, int grid)
 
 int wave_max_blocks_per_sm()
 {
-    const size_t smem = 128 + (size_t)(WV_NST * WV_A_DOUBLES + 2 * 32 * WV_YP) * sizeof(double);
+    const size_t smem = wave_smem_bytes();
     int best = 1 << 30;
     const void *fns[] = {(const void *)trsm_wave_kernel<32, false>, (const void *)trsm_wave_kernel<32, true>};
     for (const void *fn : fns) {
@@ -326,6 +372,18 @@ int trsm_wave(Context *ctx, const double *dA, const double *W, const Geom &g, do
     int *ctr = (int *)ctx->buffer(BUF_SOLVE_CTR, per * nchunks * sizeof(int));
     if (!ctr) return DPLASMA_ERR_OUT_OF_RESOURCES;
     CK(cudaMemsetAsync(ctr, 0, per * nchunks * sizeof(int), ctx->stream));
+    // L: rows of the tiles contiguous (nbi), one line per tile column;
+    // W: 128x128 column-major blocks.  Boxes of 16 doubles (128 bytes, the
+    // swizzle span) by 32 (forward: k columns) or 128 (backward: columns).
+    CUtensorMap lmap, wmap;
+    const uint32_t box1 = transposed ? 128 : WV_KS;
+    int rc0 = encode_map_2d(ctx, &lmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, (void *)dA, (uint64_t)g.nbi,
+                            (uint64_t)g.ntiles() * g.nbi, (uint64_t)g.nbi * sizeof(double), 16, box1,
+                            CU_TENSOR_MAP_SWIZZLE_128B);
+    if (!rc0)
+        rc0 = encode_map_2d(ctx, &wmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, (void *)W, 128, (uint64_t)nblk * 128,
+                            128 * sizeof(double), 16, box1, CU_TENSOR_MAP_SWIZZLE_128B);
+    if (rc0) return rc0;
     for (int ch = 0; ch < nchunks; ++ch) {
         WaveArgs a;
         a.A = dA;
@@ -344,11 +402,15 @@ int trsm_wave(Context *ctx, const double *dA, const double *W, const Geom &g, do
         const int nc = (nrhs - a.c0) < 32 ? (nrhs - a.c0) : 32;   // nrhs is a multiple of 8
         int rc;
         if (transposed)
-            rc = nc <= 8 ? launch_wave<8, true>(ctx, a, grid) : nc <= 16 ? launch_wave<16, true>(ctx, a, grid)
-                 : nc <= 24 ? launch_wave<24, true>(ctx, a, grid) : launch_wave<32, true>(ctx, a, grid);
+            rc = nc <= 8    ? launch_wave<8, true>(ctx, a, grid, lmap, wmap)
+                 : nc <= 16 ? launch_wave<16, true>(ctx, a, grid, lmap, wmap)
+                 : nc <= 24 ? launch_wave<24, true>(ctx, a, grid, lmap, wmap)
+                            : launch_wave<32, true>(ctx, a, grid, lmap, wmap);
         else
-            rc = nc <= 8 ? launch_wave<8, false>(ctx, a, grid) : nc <= 16 ? launch_wave<16, false>(ctx, a, grid)
-                 : nc <= 24 ? launch_wave<24, false>(ctx, a, grid) : launch_wave<32, false>(ctx, a, grid);
+            rc = nc <= 8    ? launch_wave<8, false>(ctx, a, grid, lmap, wmap)
+                 : nc <= 16 ? launch_wave<16, false>(ctx, a, grid, lmap, wmap)
+                 : nc <= 24 ? launch_wave<24, false>(ctx, a, grid, lmap, wmap)
+                            : launch_wave<32, false>(ctx, a, grid, lmap, wmap);
         if (rc) return rc;
     }
     int st = 0;
