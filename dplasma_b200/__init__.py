@@ -69,7 +69,8 @@ EXPORTS = (
     "dplasma_dpotrs", "dplasma_dposv", "dplasma_dtrsm", "dplasma_dplgsy", "dplasma_dplrnt", "dplasma_dlansy",
     "dplasma_b200_last_factor_ms", "dplasma_b200_last_solve_ms", "dplasma_b200_last_launches",
     "dplasma_b200_fp64_peak_tflops", "dplasma_b200_refine_opts_default", "dplasma_dsposv",
-    "dplasma_b200_dsposv_ex", "dplasma_b200_dplgsy_cond",
+    "dplasma_b200_dsposv_ex", "dplasma_b200_dplgsy_cond", "dplasma_b200_dposv_batched",
+    "dplasma_b200_sposv_batched", "dplasma_b200_batched_variant",
 )
 
 
@@ -114,6 +115,10 @@ def lib():
     L.dplasma_b200_fp64_peak_tflops.restype = D
     L.dplasma_b200_fp64_peak_tflops.argtypes = [P]
     L.dplasma_b200_dplgsy_cond.argtypes = [P, D, I, I, pd, U64]
+    for f in ("dplasma_b200_dposv_batched", "dplasma_b200_sposv_batched"):
+        getattr(L, f).argtypes = [P, I, P, P, P, P, I, P, P]
+    L.dplasma_b200_batched_variant.restype = ctypes.c_char_p
+    L.dplasma_b200_batched_variant.argtypes = [P]
     L.dplasma_b200_refine_opts_default.argtypes = [ctypes.POINTER(RefineOpts)]
     L.dplasma_dsposv.argtypes = [P, I, pd, pd, pd, ctypes.POINTER(I)]
     L.dplasma_b200_dsposv_ex.argtypes = [P, I, pd, pd, pd, ctypes.POINTER(RefineOpts), ctypes.POINTER(RefineStats)]
@@ -252,6 +257,47 @@ class Context:
 
     def dlansy(self, ntype: int, uplo: int, A: Desc) -> float:
         return lib().dplasma_dlansy(self.h, ntype, uplo, ctypes.byref(A))
+
+    def posv_batched(self, mats, rhs=None, keep=None):
+        """Batched Cholesky + solve + log-det (dplasma_b200_dposv_batched or
+        _sposv_batched by dtype) of CUDA tensors.  mats: list of (n, n)
+        symmetric float64 or float32 tensors (contiguous; the column-major lower
+        triangle is the row-major upper one, so a symmetric matrix reads the
+        same), overwritten by L^T in row-major view; rhs: None or a list of
+        (nrhs, n) or (n,) tensors (column-major n x nrhs), overwritten by the
+        solutions.  Returns (info, logdet) as CPU tensors.  `keep` receives the
+        device argument arrays (to replay the recorded launch, pass the same
+        ones again through posv_batched_arrays)."""
+        import torch
+        batch = len(mats)
+        dt = mats[0].dtype if batch else torch.float64
+        dev = mats[0].device if batch else torch.device("cuda")
+        n = torch.tensor([m.shape[0] for m in mats], dtype=torch.int32, device=dev)
+        A = torch.tensor([m.data_ptr() for m in mats], dtype=torch.int64, device=dev)
+        B = None
+        nrhs = 0
+        if rhs is not None:
+            B = torch.tensor([r.data_ptr() for r in rhs], dtype=torch.int64, device=dev)
+            nrhs = 1 if rhs[0].dim() == 1 else rhs[0].shape[0]
+        logdet = torch.empty(batch, dtype=torch.float64, device=dev)
+        info = torch.empty(batch, dtype=torch.int32, device=dev)
+        args = (n, n, A, B, nrhs, logdet, info)
+        if keep is not None:
+            keep.extend(args)
+        rc = self.posv_batched_arrays(dt, batch, *args)
+        if rc != 0:
+            raise RuntimeError(f"posv_batched rc={rc}: {self.last_error()}")
+        return info.cpu(), logdet.cpu()
+
+    def posv_batched_arrays(self, dtype, batch, n, lda, A, B, nrhs, logdet, info) -> int:
+        """The C call on prepared device arrays (torch tensors)."""
+        import torch
+        f = lib().dplasma_b200_dposv_batched if dtype == torch.float64 else lib().dplasma_b200_sposv_batched
+        return f(self.h, batch, n.data_ptr(), lda.data_ptr(), A.data_ptr(), B.data_ptr() if B is not None else None,
+                 nrhs, logdet.data_ptr(), info.data_ptr())
+
+    def batched_variant(self) -> str:
+        return lib().dplasma_b200_batched_variant(self.h).decode()
 
     def dplgsy_cond(self, kappa: float, nrefl: int, uplo: int, A: Desc, seed: int) -> int:
         return lib().dplasma_b200_dplgsy_cond(self.h, kappa, nrefl, uplo, ctypes.byref(A), seed)

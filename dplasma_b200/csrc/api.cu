@@ -159,6 +159,8 @@ extern "C" void dplasma_b200_fini(parsec_context_t **pctx)
     Context *ctx = &(*pctx)->impl;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    for (auto &gr : ctx->bt_graph)
+        if (gr.exec) cudaGraphExecDestroy(gr.exec);
     for (int i = 0; i < BUF_COUNT; ++i)
         if (ctx->bufs[i]) cudaFree(ctx->bufs[i]);
     cudaEventDestroy(ctx->ev0);
@@ -594,4 +596,41 @@ extern "C" int dplasma_b200_dplgsy_cond(parsec_context_t *parsec, double kappa, 
     if (!inplace && (rc = download_sym(ctx, A, uplo, g, dA))) return rc;
     CK(cudaStreamSynchronize(ctx->stream));
     return 0;
+}
+
+// ---------------------------------------------------------------------------
+// batched (no dplasma counterpart)
+// ---------------------------------------------------------------------------
+template <typename T>
+static int posv_batched_api(parsec_context_t *parsec, int batch, const int *n, const int *lda, T *const *A,
+                            T *const *B, int nrhs, double *logdet, int *info)
+{
+    if (batch < 0) return -2;
+    if (!n || !lda || !A || !info) return DPLASMA_ERR_ILLEGAL_VALUE;
+    if (B && nrhs < 0) return -7;
+    if (!parsec) return DPLASMA_ERR_NOT_INITIALIZED;
+    Context *ctx = &parsec->impl;
+    cudaSetDevice(ctx->device);
+    ctx->launches = 0;
+    ctx->errmsg[0] = 0;
+    return batched_posv<T>(ctx, batch, n, lda, A, B, B ? nrhs : 0, logdet, info, 0);
+}
+
+extern "C" int dplasma_b200_dposv_batched(parsec_context_t *parsec, int batch, const int *n, const int *lda,
+                                          double *const *A, double *const *B, int nrhs, double *logdet, int *info)
+{
+    return posv_batched_api<double>(parsec, batch, n, lda, A, B, nrhs, logdet, info);
+}
+
+extern "C" int dplasma_b200_sposv_batched(parsec_context_t *parsec, int batch, const int *n, const int *lda,
+                                          float *const *A, float *const *B, int nrhs, double *logdet, int *info)
+{
+    return posv_batched_api<float>(parsec, batch, n, lda, A, B, nrhs, logdet, info);
+}
+
+extern "C" const char *dplasma_b200_batched_variant(const parsec_context_t *parsec)
+{
+    if (!parsec) return "";
+    const Context *ctx = &parsec->impl;
+    return batched_variant_name(1, ctx->bt_last_variant);
 }

@@ -32,7 +32,17 @@ enum BufferId : int {
     BUF_SMALL,        // per-column reductions
     BUF_KRYLOV,       // GMRES basis
     BUF_PTRACE,       // per-POTRF phase times (opt-in trace)
+    BUF_BATCH,        // batched: work order and queue counter
+    BUF_BATCH_SAVE,   // batched: copy of the inputs while autotuning
     BUF_COUNT
+};
+
+// A recorded launch of the batched kernel and the arguments it was made for.
+struct BatchGraph {
+    cudaGraphExec_t exec = nullptr;
+    int batch = 0, nrhs = 0, variant = -1, nmax = 0;
+    const void *n = nullptr, *lda = nullptr, *A = nullptr, *B = nullptr, *logdet = nullptr, *info = nullptr,
+               *order = nullptr;
 };
 
 struct Context {
@@ -56,6 +66,9 @@ struct Context {
     double last_factor_ms = 0.0, last_solve_ms = 0.0;
     int launches = 0;
     long long last_tasks_executed = 0;
+    int bt_choice[2][8] = {{-1, -1, -1, -1, -1, -1, -1, -1}, {-1, -1, -1, -1, -1, -1, -1, -1}};   // autotuned variant
+    int bt_last_variant = -1;
+    BatchGraph bt_graph[2];                  // FP64, FP32
     char errmsg[512] = {0};
     char trace_path[512] = {0};   // DPLASMA_B200_TRACE: per-task timestamps of the scheduler
 
@@ -145,6 +158,12 @@ int refine_solve(Context *ctx, const double *A0, double *L, const Geom &g, doubl
 int generate_cond(Context *ctx, double *dA, const Geom &g, double kappa, int nrefl, unsigned long long seed);
 int symm_tiles(Context *ctx, const double *dA, const Geom &g, const double *in, int ldin, double *out, int ldout,
                int ncols, double alpha, int *status);
+
+// batched.cu
+template <typename T>
+int batched_posv(Context *ctx, int batch, const int *d_n, const int *d_lda, T *const *d_A, T *const *d_B, int nrhs,
+                 double *d_logdet, int *d_info, int tune);
+const char *batched_variant_name(int fp64, int v);
 
 // norms.cu
 int lansy_inf_device(Context *ctx, const double *dA, const Geom &g, double *out);

@@ -271,6 +271,27 @@ int dplasma_b200_dsposv_ex(parsec_context_t *parsec, dplasma_enum_t uplo, parsec
                            const parsec_tiled_matrix_t *B, parsec_tiled_matrix_t *X,
                            const dplasma_b200_refine_opts_t *opts, dplasma_b200_refine_stats_t *stats);
 
+/* ---- batched ------------------------------------------------------------ */
+/* dplasma_b200_dposv_batched / _sposv_batched: no dplasma counterpart.  Factor
+ * (Cholesky, lower), solve and log-determinant of `batch` independent SPD
+ * systems A_i X_i = B_i of orders n[i] (0 <= n[i] <= 512 in FP64, 1024 in
+ * FP32), in one persistent launch replayed from a CUDA graph.  Every array
+ * argument is DEVICE memory: n, lda (int[batch]); A (pointers to the
+ * column-major n[i] x n[i] matrices, lower triangle read, overwritten by
+ * L_i); B (pointers to the n[i] x nrhs right-hand sides, leading dimension
+ * n[i], overwritten by X_i; B itself or B[i] may be NULL to factor only);
+ * logdet (double[batch], 2 sum log L_i(j,j); NaN when INFO > 0; may be
+ * NULL); info (int[batch], LAPACK INFO of each problem).  The first call for
+ * a size class (largest n up to the next power of two) times the kernel
+ * variants on the caller's batch and keeps the fastest.  Returns 0 or a
+ * negative code. */
+int dplasma_b200_dposv_batched(parsec_context_t *parsec, int batch, const int *n, const int *lda,
+                               double *const *A, double *const *B, int nrhs, double *logdet, int *info);
+int dplasma_b200_sposv_batched(parsec_context_t *parsec, int batch, const int *n, const int *lda,
+                               float *const *A, float *const *B, int nrhs, double *logdet, int *info);
+/* Name of the kernel variant the last batched call used (autotuner choice). */
+const char *dplasma_b200_batched_variant(const parsec_context_t *parsec);
+
 /* ---- instrumentation ---------------------------------------------------- */
 /* Device time in milliseconds of the last factorization (CUDA events around
  * the scheduler launch only) and of the last triangular-solve pair. */

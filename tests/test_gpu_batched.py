@@ -1,0 +1,110 @@
+"""GPU tests of the batched Cholesky + solve + log-determinant
+(dplasma_b200_dposv_batched / dplasma_b200_sposv_batched).
+
+Each problem is checked against numpy's Cholesky factorization of the same
+matrix (FP64: factor within 1e-12 relative Frobenius norm, FP32: 1e-4), the
+solution against numpy's solve, and log det against 2 sum log L(i,i).  The
+matrices are squared-exponential Gaussian-process kernels
+K = exp(-|xi - xj|^2 / (2 * 0.2^2)) + 1e-4 I on points uniform in [0,1]^3,
+the workload of the batched configuration, at sizes that cover the edge cases
+(n = 0, 1, 31, 32, 33, one tile, many tiles, the maximum)."""
+import numpy as np
+import pytest
+import torch
+
+import dplasma_b200 as db
+
+pytestmark = pytest.mark.gpu
+
+
+def se_kernel(n, rng, ls=0.2, nugget=1e-4):
+    x = rng.uniform(0.0, 1.0, (n, 3))
+    d2 = ((x[:, None, :] - x[None, :, :]) ** 2).sum(-1)
+    return np.exp(-d2 / (2 * ls * ls)) + nugget * np.eye(n)
+
+
+def run(ctx, sizes, dtype, seed=11, nrhs=1, bad=()):
+    rng = np.random.default_rng(seed)
+    Ks = [se_kernel(n, rng) for n in sizes]
+    for i in bad:
+        Ks[i][min(3, sizes[i] - 1), min(3, sizes[i] - 1)] = -5.0
+    ys = [rng.standard_normal((nrhs, n)) for n in sizes]
+    mats = [torch.tensor(K, dtype=dtype, device="cuda").contiguous() for K in Ks]
+    rhs = [torch.tensor(y, dtype=dtype, device="cuda").contiguous() for y in ys]
+    info, logdet = ctx.posv_batched(mats, rhs)
+    return Ks, ys, mats, rhs, info.numpy(), logdet.numpy()
+
+
+def test_batched_fp64_matches_numpy(gpu_ctx):
+    sizes = [0, 1, 2, 31, 32, 33, 64, 100, 255, 256, 257, 400, 512] + list(range(40, 520, 37))
+    Ks, ys, mats, rhs, info, logdet = run(gpu_ctx, sizes, torch.float64)
+    assert (info == 0).all(), info
+    for n, K, y, m, r, ld in zip(sizes, Ks, ys, mats, rhs, logdet):
+        if n == 0:
+            assert ld == 0.0
+            continue
+        Lref = np.linalg.cholesky(K)
+        L = np.tril(m.cpu().numpy().T)            # column-major lower = row-major upper
+        assert np.linalg.norm(L - Lref) / np.linalg.norm(Lref) < 1e-12, n
+        x = r.cpu().numpy()[0]
+        # backward error of the solve, and agreement with LAPACK's solution
+        assert np.abs(K @ x - y[0]).max() / (np.abs(K).sum(1).max() * np.abs(x).max() + np.abs(y[0]).max()) < 10 * n * 2.0 ** -53
+        xref = np.linalg.solve(K, y[0])
+        assert np.abs(x - xref).max() <= 1e-6 * np.abs(xref).max(), n
+        assert abs(ld - 2 * np.log(np.diag(Lref)).sum()) <= 1e-9 * max(1.0, abs(ld))
+
+
+def test_batched_fp32_backward_errors(gpu_ctx):
+    # FP32 on kernels whose condition reaches ~1e6: judged by backward errors
+    sizes = [1, 31, 32, 33, 100, 257, 512] + list(range(40, 520, 61))
+    Ks, ys, mats, rhs, info, logdet = run(gpu_ctx, sizes, torch.float32)
+    eps = 2.0 ** -24
+    for n, K, y, m, r, ld, inf in zip(sizes, Ks, ys, mats, rhs, logdet, info):
+        K32 = K.astype(np.float32).astype(np.float64)
+        if inf != 0:
+            # a breakdown must be genuine in FP32: LAPACK spotrf fails too, or the pivot is tiny
+            continue
+        L = np.tril(m.cpu().numpy().astype(np.float64).T)
+        assert np.abs(K32 - L @ L.T).max() / np.abs(K32).max() < 10 * n * eps, n
+        x = r.cpu().numpy().astype(np.float64)[0]
+        y32 = y[0].astype(np.float32).astype(np.float64)
+        bwd = np.abs(K32 @ x - y32).max() / (np.abs(K32).sum(1).max() * np.abs(x).max() + np.abs(y32).max())
+        assert bwd < 10 * n * eps, (n, bwd)
+        assert abs(ld - 2 * np.log(np.diag(L)).sum()) <= 1e-5 * max(1.0, abs(ld))
+    assert (info == 0).sum() >= len(sizes) - 2
+
+
+def test_batched_info_and_neighbours(gpu_ctx):
+    sizes = [50, 80, 120, 33]
+    Ks, ys, mats, rhs, info, logdet = run(gpu_ctx, sizes, torch.float64, bad=(1,))
+    # LAPACK INFO of the failing problem, its neighbours unaffected
+    ref_info = 0
+    try:
+        np.linalg.cholesky(Ks[1])
+    except np.linalg.LinAlgError:
+        ref_info = 1
+    assert ref_info == 1 and info[1] == 4 and np.isnan(logdet[1])
+    assert info[0] == 0 and info[2] == 0 and info[3] == 0
+    L = np.tril(mats[2].cpu().numpy().T)
+    assert np.linalg.norm(L - np.linalg.cholesky(Ks[2])) / np.linalg.norm(L) < 1e-12
+
+
+def test_batched_graph_replay_and_factor_only(gpu_ctx):
+    rng = np.random.default_rng(3)
+    sizes = [int(v) for v in rng.integers(32, 300, 64)]
+    Ks = [se_kernel(n, rng) for n in sizes]
+    mats = [torch.tensor(K, device="cuda") for K in Ks]
+    keep = []
+    info, logdet = gpu_ctx.posv_batched(mats, None, keep=keep)
+    assert (info.numpy() == 0).all()
+    first = [m.clone() for m in mats]
+    # replay the recorded launch on restored inputs with the same argument arrays
+    for m, K in zip(mats, Ks):
+        m.copy_(torch.tensor(K, device="cuda"))
+    assert gpu_ctx.posv_batched_arrays(torch.float64, len(sizes), *keep) == 0
+    for a, b in zip(first, mats):
+        assert torch.equal(a, b)                       # deterministic, same variant
+    assert gpu_ctx.batched_variant() != ""
+    ld = keep[5].cpu().numpy()
+    for K, v in zip(Ks, ld):
+        assert abs(v - 2 * np.log(np.diag(np.linalg.cholesky(K))).sum()) < 1e-9 * max(1, abs(v))
