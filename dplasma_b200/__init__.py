@@ -70,7 +70,7 @@ EXPORTS = (
     "dplasma_b200_last_factor_ms", "dplasma_b200_last_solve_ms", "dplasma_b200_last_launches",
     "dplasma_b200_fp64_peak_tflops", "dplasma_b200_refine_opts_default", "dplasma_dsposv",
     "dplasma_b200_dsposv_ex", "dplasma_b200_dplgsy_cond", "dplasma_b200_dposv_batched",
-    "dplasma_b200_sposv_batched", "dplasma_b200_batched_variant",
+    "dplasma_b200_sposv_batched", "dplasma_b200_batched_variant", "dplasma_dpotrf_adjoint",
 )
 
 
@@ -117,6 +117,7 @@ def lib():
     L.dplasma_b200_dplgsy_cond.argtypes = [P, D, I, I, pd, U64]
     for f in ("dplasma_b200_dposv_batched", "dplasma_b200_sposv_batched"):
         getattr(L, f).argtypes = [P, I, P, P, P, P, I, P, P]
+    L.dplasma_dpotrf_adjoint.argtypes = [P, I, pd, pd]
     L.dplasma_b200_batched_variant.restype = ctypes.c_char_p
     L.dplasma_b200_batched_variant.argtypes = [P]
     L.dplasma_b200_refine_opts_default.argtypes = [ctypes.POINTER(RefineOpts)]
@@ -298,6 +299,9 @@ class Context:
 
     def batched_variant(self) -> str:
         return lib().dplasma_b200_batched_variant(self.h).decode()
+
+    def dpotrf_adjoint(self, uplo: int, L: Desc, Lbar: Desc) -> int:
+        return lib().dplasma_dpotrf_adjoint(self.h, uplo, ctypes.byref(L), ctypes.byref(Lbar))
 
     def dplgsy_cond(self, kappa: float, nrefl: int, uplo: int, A: Desc, seed: int) -> int:
         return lib().dplasma_b200_dplgsy_cond(self.h, kappa, nrefl, uplo, ctypes.byref(A), seed)

@@ -634,3 +634,42 @@ extern "C" const char *dplasma_b200_batched_variant(const parsec_context_t *pars
     const Context *ctx = &parsec->impl;
     return batched_variant_name(1, ctx->bt_last_variant);
 }
+
+// ---------------------------------------------------------------------------
+// adjoint (no dplasma counterpart)
+// ---------------------------------------------------------------------------
+extern "C" int dplasma_dpotrf_adjoint(parsec_context_t *parsec, dplasma_enum_t uplo, const parsec_tiled_matrix_t *L,
+                                      parsec_tiled_matrix_t *Lbar)
+{
+    if (uplo != dplasmaUpper && uplo != dplasmaLower) {
+        dplasma_error("dplasma_dpotrf_adjoint", "illegal value of uplo");
+        return -1;
+    }
+    if (!parsec) return DPLASMA_ERR_NOT_INITIALIZED;
+    int rc;
+    if ((rc = check_square("dplasma_dpotrf_adjoint", L)) || (rc = check_square("dplasma_dpotrf_adjoint", Lbar))) return rc;
+    if (Lbar->m != L->m || Lbar->mb != L->mb) {
+        dplasma_error("dplasma_dpotrf_adjoint", "L and Lbar differ in size or tiling");
+        return -4;
+    }
+    Context *ctx = &parsec->impl;
+    cudaSetDevice(ctx->device);
+    ctx->launches = 0;
+    ctx->errmsg[0] = 0;
+    if (L->m == 0) return 0;
+    Geom g = make_geom(L->m, L->mb);
+    if (g.mt > 65535 || g.nbi > 512) return DPLASMA_ERR_INTERNAL_LIMIT;
+    double *Lt = (double *)ctx->buffer(BUF_A, g.elems() * sizeof(double));
+    double *Lbt = (double *)ctx->buffer(BUF_A0, g.elems() * sizeof(double));
+    if (!Lt || !Lbt) return DPLASMA_ERR_OUT_OF_RESOURCES;
+    // L first, then Lbar: a host Lbar's staging copy must be the last upload
+    if ((rc = upload_sym(ctx, L, uplo, g, Lt)) || (rc = upload_sym(ctx, Lbar, uplo, g, Lbt))) return rc;
+    CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    if ((rc = potrf_adjoint_tiles(ctx, Lt, Lbt, g))) return rc;
+    CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    if ((rc = download_sym(ctx, Lbar, uplo, g, Lbt))) return rc;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    ctx->last_factor_ms = ms;
+    return 0;
+}

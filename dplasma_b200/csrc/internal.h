@@ -34,6 +34,7 @@ enum BufferId : int {
     BUF_PTRACE,       // per-POTRF phase times (opt-in trace)
     BUF_BATCH,        // batched: work order and queue counter
     BUF_BATCH_SAVE,   // batched: copy of the inputs while autotuning
+    BUF_ADJ,          // adjoint: dense L, W = L^-1 and two products
     BUF_COUNT
 };
 
@@ -158,6 +159,9 @@ int refine_solve(Context *ctx, const double *A0, double *L, const Geom &g, doubl
 int generate_cond(Context *ctx, double *dA, const Geom &g, double kappa, int nrefl, unsigned long long seed);
 int symm_tiles(Context *ctx, const double *dA, const Geom &g, const double *in, int ldin, double *out, int ldout,
                int ncols, double alpha, int *status);
+
+// adjoint.cu: Abar from L and Lbar (device tiles, lower); Lbt is overwritten
+int potrf_adjoint_tiles(Context *ctx, const double *Lt, double *Lbt, const Geom &g);
 
 // batched.cu
 template <typename T>

@@ -271,6 +271,20 @@ int dplasma_b200_dsposv_ex(parsec_context_t *parsec, dplasma_enum_t uplo, parsec
                            const parsec_tiled_matrix_t *B, parsec_tiled_matrix_t *X,
                            const dplasma_b200_refine_opts_t *opts, dplasma_b200_refine_stats_t *stats);
 
+/* ---- adjoint ------------------------------------------------------------ */
+/* dplasma_dpotrf_adjoint: no dplasma counterpart; the reverse-mode derivative
+ * of dplasma_dpotrf.  L holds the factor of A = L L^T (uplo Lower) or
+ * A = U^T U (uplo Upper: the Upper triangle holds U = L^T), as dplasma_dpotrf
+ * leaves it; Lbar holds dF/dL (resp. dF/dU) of a scalar F in the same
+ * triangle and is overwritten there by the symmetric dF/dA,
+ *     Abar = sym( L^-T Phi(L^T Lbar) L^-1 ),  Phi = lower triangle, diagonal halved.
+ * The log-determinant adjoint is the case Lbar = diag(2 dF/dlogdet / L(i,i))
+ * (Abar = dF/dlogdet * A^-1); the adjoint of x = A^-1 b is
+ * Abar = -sym(bbar x^T) with bbar = A^-1 xbar, a dplasma_dpotrs.  Same tile
+ * sizes and storages as dplasma_dpotrf.  Returns 0 or a negative code. */
+int dplasma_dpotrf_adjoint(parsec_context_t *parsec, dplasma_enum_t uplo, const parsec_tiled_matrix_t *L,
+                           parsec_tiled_matrix_t *Lbar);
+
 /* ---- batched ------------------------------------------------------------ */
 /* dplasma_b200_dposv_batched / _sposv_batched: no dplasma counterpart.  Factor
  * (Cholesky, lower), solve and log-determinant of `batch` independent SPD
