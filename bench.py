@@ -21,6 +21,9 @@ accuracy (A and B stay resident in HBM; A is 17 GB, larger than L2).
           tensor peak (MEASURED_PEAKS.json); roofline_fp64 the FP64 kernel
           against the measured FP64 DMMA peak;
   kappa_sweep : kappa 1e2/1e4/1e6 x FP16/BF16/split-FP16 against FP64;
+  batched : 4096 GP-kernel systems (n in [32, 512]) factored, solved and
+          log-det'ed in one graph-replayed launch, FP64 and FP32;
+  adjoint : GP log-marginal likelihood at N=16384, forward vs forward+backward;
   cpu_baseline : the reference's own CORE kernels (compiled from its sources)
           run as the tile DAG on all host cores, on a bounded N.
 
@@ -180,6 +183,87 @@ def measured_peaks():
         return {}
 
 
+def bench_batched(ctx, db, torch, peak64):
+    """4096 GP-kernel systems, n uniform in [32, 512] (seed 11), NRHS=1, FP64 and
+    FP32: Cholesky + solve + log-det in one graph-replayed persistent launch."""
+    B = 4096
+    rng = np.random.default_rng(11)
+    sizes = [int(v) for v in rng.integers(32, 513, B)]
+    g = torch.Generator(device="cuda").manual_seed(11)
+    base = []
+    for n in sizes:
+        x = torch.rand(n, 3, dtype=torch.float64, device="cuda", generator=g)
+        d2 = ((x[:, None, :] - x[None, :, :]) ** 2).sum(-1)
+        base.append(torch.exp(-d2 / (2 * 0.2 ** 2)) + 1e-4 * torch.eye(n, dtype=torch.float64, device="cuda"))
+    ys = [torch.randn(n, dtype=torch.float64, device="cuda", generator=g) for n in sizes]
+    flops = sum(n ** 3 / 3.0 + 2.0 * n * n + n for n in sizes)
+    out = {"problems": B, "n": "uniform integer in [32, 512], seed 11", "nrhs": 1,
+           "flops_per_batch": flops}
+    for name, dt in (("fp64", torch.float64), ("fp32", torch.float32)):
+        mats = [K.to(dt).clone() for K in base]
+        rhs = [y.to(dt).clone() for y in ys]
+        keep = []
+        info, _ = ctx.posv_batched(mats, rhs, keep=keep)       # autotunes, records the graph
+        times = []
+        for _ in range(3):
+            for m, K in zip(mats, base):
+                m.copy_(K)
+            for r, y in zip(rhs, ys):
+                r.copy_(y)
+            torch.cuda.synchronize()
+            assert ctx.posv_batched_arrays(dt, B, *keep) == 0
+            times.append(ctx.last_factor_ms())
+        ms = min(times)
+        bytes_ = sum(8.0 * n * n * 1.5 for n in sizes) * (0.5 if dt == torch.float32 else 1.0)
+        out[name] = {"ms": ms, "tflops": flops / (ms * 1e-3) / 1e12, "gbs": bytes_ / (ms * 1e-3) / 1e9,
+                     "variant": ctx.batched_variant(), "info_nonzero": int((keep[6].cpu() != 0).sum()),
+                     "launches": 1}
+        if dt == torch.float64:
+            out[name]["frac_of_fp64_peak"] = out[name]["tflops"] / peak64 if peak64 > 0 else None
+        del mats, rhs
+    return out
+
+
+def bench_adjoint(torch):
+    """GP log-marginal likelihood at N=16384 (SE kernel, 3-D points, lengthscale
+    0.2, nugget 1e-4, seed 13): forward (factor + solve + log-det) against
+    forward + backward (gradient in K and the lengthscale)."""
+    from dplasma_b200 import autograd as dag
+    n = 16384
+    g = torch.Generator(device="cuda").manual_seed(13)
+    x = torch.rand(n, 3, dtype=torch.float64, device="cuda", generator=g)
+    y = torch.randn(n, dtype=torch.float64, device="cuda", generator=g)
+
+    def fwd(ls):
+        return dag.gp_log_marginal_likelihood(dag.se_kernel(x, ls), y)
+
+    ls = torch.tensor(0.2, dtype=torch.float64, device="cuda", requires_grad=True)
+    fwd(ls.detach())
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    with torch.no_grad():
+        v = fwd(ls.detach())
+    e1.record()
+    torch.cuda.synchronize()
+    t_f = e0.elapsed_time(e1)
+    val = fwd(ls)
+    val.backward()
+    torch.cuda.synchronize()
+    ls.grad = None
+    e0.record()
+    val = fwd(ls)
+    val.backward()
+    e1.record()
+    torch.cuda.synchronize()
+    t_fb = e0.elapsed_time(e1)
+    flops_f = n ** 3 / 3.0 + 2.0 * n * n
+    return {"n": n, "forward_ms": t_f, "forward_backward_ms": t_fb, "backward_over_forward": t_fb / t_f - 1.0,
+            "forward_tflops": flops_f / (t_f * 1e-3) / 1e12, "value": float(v), "dlengthscale": float(ls.grad),
+            "note": "backward = dplasma_dpotrf_adjoint for K^-1 (about 1.3 N^3 FP64 tensor-core flops) "
+                    "and rank-1 terms; forward = dplasma_dpotrf + dplasma_dpotrs"}
+
+
 def run_gpu(args):
     import torch
     import dplasma_b200 as db
@@ -332,6 +416,11 @@ def run_gpu(args):
                               "fmt_used": st["fmt_used"], "backward_error": st["backward_error"],
                               "forward_error_vs_fp64": fwd_err(X, Xk), "factor_ms": st["factor_ms"]})
 
+    batched = adjoint = None
+    if args.extras:
+        batched = bench_batched(ctx, db, torch, peak64)
+        adjoint = bench_adjoint(torch)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         threads = os.cpu_count() or 1
@@ -382,7 +471,7 @@ def run_gpu(args):
                           "frac": ach64 / peak64 if peak64 > 0 else None,
                           "kernel": "potrf_persistent_kernel<false> (FP64 DMMA)",
                           "peak_source": "measured FP64 DMMA (mma.sync m16n8k4 f64) probe on this GPU"},
-        "kappa_sweep": sweep,
+        "kappa_sweep": sweep, "batched": batched, "adjoint": adjoint,
         "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks, "wall_s": wall,
     }
     if rank == 0:
@@ -408,6 +497,8 @@ def main():
     p.add_argument("--kappa", type=float, default=1e6)
     p.add_argument("--fmt", default="split", choices=sorted(FMTS))
     p.add_argument("--no-sweep", dest="sweep", action="store_false")
+    p.add_argument("--no-extras", dest="extras", action="store_false",
+                   help="skip the batched and adjoint measurements")
     args = p.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)

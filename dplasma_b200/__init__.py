@@ -285,6 +285,7 @@ class Context:
         args = (n, n, A, B, nrhs, logdet, info)
         if keep is not None:
             keep.extend(args)
+        torch_ready(*mats, *(rhs or []), n, A, B)
         rc = self.posv_batched_arrays(dt, batch, *args)
         if rc != 0:
             raise RuntimeError(f"posv_batched rc={rc}: {self.last_error()}")
@@ -293,6 +294,7 @@ class Context:
     def posv_batched_arrays(self, dtype, batch, n, lda, A, B, nrhs, logdet, info) -> int:
         """The C call on prepared device arrays (torch tensors)."""
         import torch
+        torch_ready(n, A)
         f = lib().dplasma_b200_dposv_batched if dtype == torch.float64 else lib().dplasma_b200_sposv_batched
         return f(self.h, batch, n.data_ptr(), lda.data_ptr(), A.data_ptr(), B.data_ptr() if B is not None else None,
                  nrhs, logdet.data_ptr(), info.data_ptr())
@@ -318,6 +320,20 @@ class Context:
         rc = lib().dplasma_b200_dsposv_ex(self.h, uplo, ctypes.byref(A), ctypes.byref(B), ctypes.byref(X),
                                           ctypes.byref(o), ctypes.byref(st))
         return rc, {f: getattr(st, f) for f, _ in RefineStats._fields_}
+
+
+def torch_ready(*tensors):
+    """The library runs on its own CUDA stream: wait for the work torch has
+    queued on the tensors' current streams (the producers of our inputs)
+    before a call.  The library's calls return with their results complete."""
+    import torch
+    seen = set()
+    for t in tensors:
+        if t is not None and getattr(t, "is_cuda", False):
+            dev = t.device.index if t.device.index is not None else torch.cuda.current_device()
+            if dev not in seen:
+                seen.add(dev)
+                torch.cuda.current_stream(dev).synchronize()
 
 
 def attach(d: Desc, buf) -> Desc:

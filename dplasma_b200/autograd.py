@@ -24,7 +24,7 @@ import math
 
 import torch
 
-from . import Context, desc_general, attach, Lower, STORAGE_LAPACK
+from . import Context, desc_general, attach, Lower, STORAGE_LAPACK, torch_ready
 
 _ctx = {}
 
@@ -53,6 +53,7 @@ def _factor(A: torch.Tensor):
     """column-major lower factor in a row-major buffer (its upper triangle)"""
     n = A.shape[0]
     buf = A.detach().contiguous().clone()
+    torch_ready(buf)
     ctx = context(A.device)
     info = ctx.dpotrf(Lower, _lapack_desc(buf, n))
     if info != 0:
@@ -67,6 +68,7 @@ def _adjoint(Lrow: torch.Tensor, Lbar: torch.Tensor) -> torch.Tensor:
     ctx = context(Lrow.device)
     Lc = Lrow.t().contiguous()              # column-major L
     Bc = torch.tril(Lbar).t().contiguous()  # column-major Lbar (lower)
+    torch_ready(Lc, Bc)
     rc = ctx.dpotrf_adjoint(Lower, _lapack_desc(Lc, n), _lapack_desc(Bc, n))
     if rc != 0:
         raise RuntimeError(f"dplasma_dpotrf_adjoint: {rc} {ctx.last_error()}")
@@ -106,6 +108,7 @@ class _GPLogML(torch.autograd.Function):
         # m x n row-major = n x m column-major; a copy (for one column the
         # transpose is already contiguous and would alias y)
         rhs = Y.detach().t().contiguous().clone()
+        torch_ready(rhs)
         rc = ctx.dpotrs(Lower, _lapack_desc(buf, n), _lapack_desc(rhs, n, Y.shape[1]))
         if rc != 0:
             raise RuntimeError(f"dplasma_dpotrs: {rc} {ctx.last_error()}")
