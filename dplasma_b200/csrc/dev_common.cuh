@@ -96,6 +96,12 @@ __device__ __forceinline__ void bulk_g2s(void *dst_smem, const void *src_gmem, u
         : "memory");
 }
 
+// Hint: bring `bytes` (multiple of 16) of global memory into L2, no completion.
+__device__ __forceinline__ void bulk_prefetch_l2(const void *src_gmem, uint32_t bytes)
+{
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src_gmem), "r"(bytes) : "memory");
+}
+
 // Order this thread's generic-proxy accesses (global and shared) before later
 // async-proxy (bulk copy) accesses of the same memory, by this or another CTA.
 __device__ __forceinline__ void fence_proxy_async()

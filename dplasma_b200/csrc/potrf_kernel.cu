@@ -133,7 +133,7 @@ __device__ void producer_warp(const PotrfArgs &a, SmemCtl *ctl, double *ring, co
         if (lane == 0) {
             ctl->task[slot] = end ? (uint64_t)T_END : t;
             ctl->tick[slot] = tk;
-            if (a.trace && end) a.trace_exit[6 * blockIdx.x + 3] = globaltimer_ns();
+            if (a.trace && end) a.trace_exit[8 * blockIdx.x + 3] = globaltimer_ns();
             mbar_arrive(&ctl->tfull[slot]);
         }
         task_it++;
@@ -146,7 +146,7 @@ __device__ void producer_warp(const PotrfArgs &a, SmemCtl *ctl, double *ring, co
                 pipe_ok = false;
                 break;
             }
-            if (a.trace && lane == 0) a.trace_exit[6 * blockIdx.x + 2] = globaltimer_ns();
+            if (a.trace && lane == 0) a.trace_exit[8 * blockIdx.x + 2] = globaltimer_ns();
             continue;
         }
         if (MIXED) {
@@ -711,34 +711,51 @@ __device__ bool mixed_update(const PotrfArgs &a, SmemCtl *ctl, unsigned char *ri
         ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
     }
     st16 += nst;
+    const unsigned long long tq0 = (a.trace && tid == 0) ? globaltimer_ns() : 0;
     if (!warp_mbar_wait(&ctl->tmem_full, mx_it & 1, a.pipe_limit_ns)) {
         if (lane == 0) report(a, ST_MBAR_TIMEOUT, 10, mx_it, warp);
         ok = false;
     } else if (!__shfl_sync(0xffffffffu, ld_volatile(a.abort_flag), 0)) {
+        const unsigned long long tq1 = (a.trace && tid == 0) ? globaltimer_ns() : 0;
         tc_fence_after();
         const int lb = (warp & 3) * 32, half = warp >> 2;
         const int row = half * BLK + lb + lane;                    // within the tile
         double *C = tile_ptr(a, m, n) + row;                       // column stride nbi
         const double sr = (double)a.scl[m * a.nbs + half];
-        for (int c0 = 0; c0 < a.nbi; c0 += 32) {
+        // 64 columns per round: both halves' loads are issued before either
+        // is used, so twice as many C reads are in flight
+        for (int c0 = 0; c0 < a.nbi; c0 += 64) {
             if (m == n && c0 > row - lane + 31) break;             // above the diagonal
-            float v[32];
-            tmem_ld32(tmem + ((uint32_t)lb << 16) + (uint32_t)(256 * half + c0), v);
-            // row and column scales are the same for every panel
-            const double inv = 1.0 / (sr * (double)a.scl[n * a.nbs + c0 / BLK]);
-            double cv[32];
+            double cv[2][32];
 #pragma unroll
-            for (int j = 0; j < 32; ++j) {
-                const int col = c0 + j;
-                cv[j] = (m != n || row >= col) ? __ldcg(C + (int64_t)col * a.nbi) : 0.0;
-            }
+            for (int h = 0; h < 2; ++h)
 #pragma unroll
-            for (int j = 0; j < 32; ++j) {
-                const int col = c0 + j;
-                if (m != n || row >= col) __stcg(C + (int64_t)col * a.nbi, cv[j] - (double)v[j] * inv);
+                for (int j = 0; j < 32; ++j) {
+                    const int col = c0 + 32 * h + j;
+                    cv[h][j] = (m != n || row >= col) ? __ldcg(C + (int64_t)col * a.nbi) : 0.0;
+                }
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int cb = c0 + 32 * h;
+                float v[32];
+                tmem_ld32(tmem + ((uint32_t)lb << 16) + (uint32_t)(256 * half + cb), v);
+                // row and column scales are the same for every panel
+                const double inv = 1.0 / (sr * (double)a.scl[n * a.nbs + cb / BLK]);
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    const int col = cb + j;
+                    if (m != n || row >= col) __stcg(C + (int64_t)col * a.nbi, cv[h][j] - (double)v[j] * inv);
+                }
             }
         }
         __threadfence();
+        if (a.trace && tid == 0) {
+            // per CTA: ns until the accumulators were ready, ns of the epilogue, tasks
+            const unsigned long long tq2 = globaltimer_ns();
+            a.trace_exit[8 * blockIdx.x + 5] += tq2 - tq1;
+            a.trace_exit[8 * blockIdx.x + 6] += tq2 - tq0;
+            a.trace_exit[8 * blockIdx.x + 7] += 1;
+        }
     }
     tc_fence_before();
     mx_it++;
@@ -769,7 +786,7 @@ __device__ void consumer_warps(const PotrfArgs &a, SmemCtl *ctl, double *ring)
         task_it++;
         const int ty = task_type(t);
         if (ty == T_END) {
-            if (a.trace && tid == 0) a.trace_exit[6 * blockIdx.x + 4] = globaltimer_ns();
+            if (a.trace && tid == 0) a.trace_exit[8 * blockIdx.x + 4] = globaltimer_ns();
             break;
         }
         if (a.trace && tid == 0) a.trace[4 * (int64_t)tk + 2] = globaltimer_ns();
@@ -818,7 +835,7 @@ __device__ void consumer_warps(const PotrfArgs &a, SmemCtl *ctl, double *ring)
         executed++;
     }
     if (tid == 0 && a.task_count) a.task_count[blockIdx.x] = executed;
-    if (tid == 0 && a.trace) a.trace_exit[6 * blockIdx.x + 1] = globaltimer_ns();
+    if (tid == 0 && a.trace) a.trace_exit[8 * blockIdx.x + 1] = globaltimer_ns();
 }
 
 // Registers are allocated per SM sub-partition, so a CTA of 12 warps launches
@@ -863,7 +880,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;\n" ::"n"(PRODUCER_REGS));
         if (threadIdx.x < NCONS + 32) {
             producer_warp<MIXED>(a, ctl, ring, &tmap);
-            if (a.trace && threadIdx.x == NCONS) a.trace_exit[6 * blockIdx.x] = globaltimer_ns();
+            if (a.trace && threadIdx.x == NCONS) a.trace_exit[8 * blockIdx.x] = globaltimer_ns();
         }
     } else {
         asm volatile("setmaxnreg.inc.sync.aligned.u32 %0;\n" ::"n"(CONSUMER_REGS));
@@ -1092,11 +1109,11 @@ int potrf_run(Context *ctx, double *dA, int mt, int nbi, int nb_user, int n_user
     a.trace = nullptr;
     a.ptrace = nullptr;
     if (ctx->trace_path[0]) {
-        const size_t tbytes = ((size_t)a.ntasks * 4 + 6 * (size_t)grid) * sizeof(unsigned long long) + (size_t)a.ntasks * sizeof(int);
+        const size_t tbytes = ((size_t)a.ntasks * 4 + 8 * (size_t)grid) * sizeof(unsigned long long) + (size_t)a.ntasks * sizeof(int);
         a.trace = (unsigned long long *)ctx->buffer(BUF_TRACE, tbytes);
         if (!a.trace) return DPLASMA_ERR_OUT_OF_RESOURCES;
         a.trace_exit = a.trace + (size_t)a.ntasks * 4;
-        a.trace_cta = (int *)(a.trace_exit + 6 * (size_t)grid);
+        a.trace_cta = (int *)(a.trace_exit + 8 * (size_t)grid);
         CK(cudaMemsetAsync(a.trace, 0, tbytes, st));
         a.ptrace = (unsigned long long *)ctx->buffer(BUF_PTRACE, (size_t)mt * 8 * sizeof(unsigned long long));
         if (!a.ptrace) return DPLASMA_ERR_OUT_OF_RESOURCES;
@@ -1168,7 +1185,7 @@ int potrf_run(Context *ctx, double *dA, int mt, int nbi, int nb_user, int n_user
     }
     if (a.trace) {
         // one line per ticket: type k m n bi bj fetched deps_met started finished cta (ns, relative)
-        std::vector<unsigned long long> tr((size_t)a.ntasks * 4), tx(6 * (size_t)grid);
+        std::vector<unsigned long long> tr((size_t)a.ntasks * 4), tx(8 * (size_t)grid);
         std::vector<int> tc(a.ntasks);
         std::vector<uint64_t> tl(a.ntasks);
         CK(cudaMemcpy(tr.data(), a.trace, tr.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
@@ -1195,8 +1212,10 @@ int potrf_run(Context *ctx, double *dA, int mt, int nbi, int nb_user, int n_user
                            "store_ns %llu inv32_ns %llu\n", k, pt[8 * k], pt[8 * k + 1], pt[8 * k + 2], pt[8 * k + 3],
                         pt[8 * k + 4], pt[8 * k + 5], pt[8 * k + 6], pt[8 * k + 7]);
             for (int c = 0; c < grid; ++c)
-                fprintf(f, "# cta %d producer_exit %lld consumer_exit %lld potrf_wait_done %lld end_pushed %lld end_seen %lld\n", c,
-                        rel(tx[6 * c]), rel(tx[6 * c + 1]), rel(tx[6 * c + 2]), rel(tx[6 * c + 3]), rel(tx[6 * c + 4]));
+                fprintf(f, "# cta %d producer_exit %lld consumer_exit %lld potrf_wait_done %lld end_pushed %lld end_seen %lld "
+                           "mixed_tasks %llu mixed_wait_plus_epilogue_ns %llu mixed_epilogue_ns %llu\n", c,
+                        rel(tx[8 * c]), rel(tx[8 * c + 1]), rel(tx[8 * c + 2]), rel(tx[8 * c + 3]), rel(tx[8 * c + 4]),
+                        tx[8 * c + 7], tx[8 * c + 6], tx[8 * c + 5]);
             fclose(f);
         }
     }
