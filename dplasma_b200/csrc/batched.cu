@@ -12,8 +12,10 @@
 //   2. every thread turns one row of the panel below into L (row x D^-T),
 //      storing it to global memory and to a shared panel;
 //   3. the lower triangle of the trailing matrix is updated from the shared
-//      panel in TILE x TILE tiles, each thread owning a block of the tile.
-// The CTA size and TILE are picked per size class by timing the variants on
+//      panel in 32x32 tiles, one warp per tile (FP64 tensor cores; FP32 on
+//      the FMA pipes), the next panel's columns first so that warp 0 factors
+//      the next diagonal block while the others finish the update.
+// The number of warps per problem is picked per size class by timing the variants on
 // the caller's own batch the first time (autotuning), and the launch is
 // recorded once as a CUDA graph and replayed while the arguments stay the
 // same.
@@ -32,8 +34,9 @@
 namespace db2 {
 
 constexpr int BT_NB = 32;
-constexpr int BT_PP = 33;          // shared pitch of panel rows
+constexpr int BT_PP = 36;          // shared pitch of panel rows (== 4 mod 16: conflict-free FP64 fragments)
 constexpr int BT_NMAX = 4096;      // largest n of one problem (panel rows in shared memory)
+constexpr int BT_MAXRHS = 16;      // right-hand sides per problem
 
 template <typename T>
 struct BatchArgs {
@@ -47,6 +50,7 @@ struct BatchArgs {
     int *info;            // per problem
     const int *order;     // problems by decreasing n
     int *ticket;
+    T *dscr;              // per CTA: inverses of the 32x32 diagonal blocks of its current problem
 };
 
 template <typename T>
@@ -79,65 +83,180 @@ __device__ __forceinline__ void bt_chol_step(T (&d)[32], int lane, int &failcol,
     if constexpr (J + 1 < 32) bt_chol_step<T, J + 1>(d, lane, failcol, rdiag);
 }
 
-// One problem, whole CTA.  Returns INFO (0 or the 1-based failing column).
+// Diagonal block j0 (jb <= 32 columns) of one problem by warp 0: factor in
+// registers, write L back, accumulate log det, form the inverse into Dinv.
+// Returns the failing column within the block or -1.
+template <typename T>
+__device__ int bt_diag(T *A, int lda, int j0, int jb, T *Dinv, T *Ls, double &ld_acc, int lane)
+{
+    T d[32];
+#pragma unroll
+    for (int c = 0; c < 32; ++c)
+        d[c] = (lane < jb && c < jb) ? ((c <= lane) ? A[(int64_t)(j0 + c) * lda + j0 + lane] : T(0))
+                                     : (c == lane ? T(1) : T(0));
+    int failcol = -1;
+    T rdiag = T(0);
+    bt_chol_step<T, 0>(d, lane, failcol, rdiag);
+    if (failcol >= jb) failcol = -1;      // padding rows are the identity
+    if (failcol >= 0) return failcol;
+    if (lane < jb) {
+#pragma unroll
+        for (int c = 0; c < 32; ++c)
+            if (c <= lane && c < jb) A[(int64_t)(j0 + c) * lda + j0 + lane] = d[c];
+        ld_acc -= 2.0 * log((double)rdiag);   // rdiag = 1 / L(i,i); no d[lane]: keeps d in registers
+    }
+#pragma unroll
+    for (int c = 0; c < 32; ++c) Ls[lane * BT_PP + c] = (c <= lane) ? d[c] : T(0);
+    __syncwarp();
+    T x[32];
+#pragma unroll
+    for (int i = 0; i < 32; ++i) {
+        T s0 = T(0), s1 = T(0);
+#pragma unroll
+        for (int l = 0; l + 1 < i; l += 2) {
+            s0 = fma(Ls[i * BT_PP + l], x[l], s0);
+            s1 = fma(Ls[i * BT_PP + l + 1], x[l + 1], s1);
+        }
+        if (i & 1) s0 = fma(Ls[i * BT_PP + i - 1], x[i - 1], s0);
+        const T ri = __shfl_sync(0xffffffffu, rdiag, i);
+        x[i] = (i < lane) ? T(0) : ((i == lane) ? ri : -(s0 + s1) * ri);
+    }
+#pragma unroll
+    for (int i = 0; i < 32; ++i) Dinv[i * BT_PP + lane] = x[i];   // Dinv[i][c], lower
+    return -1;
+}
+
+// One 32x32 tile (rb, cb), rb >= cb, of the trailing update C -= P P^T by one
+// warp; C is the trailing matrix (origin at A(o, o)), m its order.  The C
+// values are loaded before the products, so their latency overlaps them.
+__device__ __forceinline__ void bt_tile(double *A, int lda, int o, int m, const double *P, int rb, int cb, int lane)
+{
+    const int g = lane >> 2, t = lane & 3;
+    double old[2][4][4];
+#pragma unroll
+    for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int r = rb * 32 + mi * 16 + g + ((q & 2) ? 8 : 0);
+                const int c = cb * 32 + ni * 8 + 2 * t + (q & 1);
+                old[mi][ni][q] = (r < m && c < m && r >= c) ? A[(int64_t)(o + c) * lda + o + r] : 0.0;
+            }
+    double acc[2][4][4];
+#pragma unroll
+    for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[mi][ni][q] = 0.0;
+#pragma unroll
+    for (int kk = 0; kk < 32; kk += 4) {
+        double af[2][2], bf[4];
+#pragma unroll
+        for (int mi = 0; mi < 2; ++mi) {
+            af[mi][0] = P[(rb * 32 + mi * 16 + g) * BT_PP + kk + t];
+            af[mi][1] = P[(rb * 32 + mi * 16 + g + 8) * BT_PP + kk + t];
+        }
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni) bf[ni] = P[(cb * 32 + ni * 8 + g) * BT_PP + kk + t];
+#pragma unroll
+        for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni) dmma_16x8x4(acc[mi][ni], af[mi][0], af[mi][1], bf[ni]);
+    }
+#pragma unroll
+    for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int r = rb * 32 + mi * 16 + g + ((q & 2) ? 8 : 0);
+                const int c = cb * 32 + ni * 8 + 2 * t + (q & 1);
+                if (r < m && c < m && r >= c) A[(int64_t)(o + c) * lda + o + r] = old[mi][ni][q] - acc[mi][ni][q];
+            }
+}
+// FP32: lane = row of the tile, 32 columns per lane (the panel values of the
+// columns are shared-memory broadcasts)
+__device__ __forceinline__ void bt_tile(float *A, int lda, int o, int m, const float *P, int rb, int cb, int lane)
+{
+    const int r = rb * 32 + lane;
+    float old[32], acc[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+        const int c = cb * 32 + j;
+        old[j] = (r < m && c < m && r >= c) ? A[(int64_t)(o + c) * lda + o + r] : 0.f;
+        acc[j] = 0.f;
+    }
+#pragma unroll 4
+    for (int k = 0; k < 32; ++k) {
+        const float pr = P[r * BT_PP + k];
+#pragma unroll
+        for (int j = 0; j < 32; ++j) acc[j] = fmaf(pr, P[(cb * 32 + j) * BT_PP + k], acc[j]);
+    }
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+        const int c = cb * 32 + j;
+        if (r < m && c < m && r >= c) A[(int64_t)(o + c) * lda + o + r] = old[j] - acc[j];
+    }
+}
+
+// One problem, whole CTA.  Right-looking in 32-column panels with one step of
+// look-ahead: after the panel, the warps first update the next panel's
+// columns; then warp 0 factors the next diagonal block while the other warps
+// update the rest of the trailing matrix.  Returns INFO (0 or the 1-based
+// failing column).
+// Warp 0, after the diagonal block j0 was factored and inverted: keep the
+// inverse for the backward solve and apply it to the right-hand sides,
+// y_j = D^-1 b_j (forward substitution with the block inverse), y_j kept in
+// ybuf for the panel update of the rows below and stored in place in B.
+template <typename T>
+__device__ __forceinline__ void bt_diag_rhs(const T *Dinv, T *dscr, int j0, int jb, T *B, int ldb, int nrhs,
+                                            T *ybuf, int lane)
+{
+    T *Dk = dscr + (int64_t)(j0 / BT_NB) * 32 * 32;
+#pragma unroll 4
+    for (int i = 0; i < 32; ++i) Dk[i * 32 + lane] = Dinv[i * BT_PP + lane];
+    for (int col = 0; col < nrhs; ++col) {
+        T *b = B + (int64_t)col * ldb + j0;
+        const T bl = lane < jb ? b[lane] : T(0);
+        T y = T(0);
+#pragma unroll
+        for (int l = 0; l < 32; ++l) y = fma(Dinv[lane * BT_PP + l], __shfl_sync(0xffffffffu, bl, l), y);
+        if (lane < jb) b[lane] = y;
+        ybuf[col * 32 + lane] = lane < jb ? y : T(0);
+    }
+}
+
 template <typename T, int NT, int TILE>
-__device__ int bt_factor(T *A, int n, int lda, T *Dinv, T *P, int *sflag, double *logdet_out)
+__device__ int bt_factor(T *A, int n, int lda, T *Dinv, T *Ls, T *P, int *sflag, double *logdet_out, T *B,
+                         int nrhs, T *dscr, T *ybuf)
 {
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    constexpr int NW = NT / 32;
     double ld_acc = 0.0;
     int info = 0;
-    for (int j0 = 0; j0 < n; j0 += BT_NB) {
+    if (warp == 0) {
+        const int f = bt_diag<T>(A, lda, 0, min(BT_NB, n), Dinv, Ls, ld_acc, lane);
+        if (lane == 0) sflag[0] = f;
+        if (f < 0 && B) bt_diag_rhs<T>(Dinv, dscr, 0, min(BT_NB, n), B, n, nrhs, ybuf, lane);
+    }
+    __syncthreads();
+    if (sflag[0] >= 0) info = sflag[0] + 1;
+    for (int j0 = 0; j0 < n && info == 0; j0 += BT_NB) {
         const int jb = min(BT_NB, n - j0);
-        // (1) diagonal block
-        if (warp == 0) {
-            T d[32];
+        const int o = j0 + jb, m = n - o;
+        if (m <= 0) break;
+        // panel rows below: L = A D^-T, to global and to the shared panel
+        // (rows up to the next multiple of 32 are zero-filled)
+        const int m32 = (m + 31) & ~31;
+        for (int rr = tid; rr < m32; rr += NT) {
+            if (rr >= m) {
 #pragma unroll
-            for (int c = 0; c < 32; ++c)
-                d[c] = (lane < jb && c < jb) ? ((c <= lane) ? A[(int64_t)(j0 + c) * lda + j0 + lane] : T(0))
-                                             : (c == lane ? T(1) : T(0));
-            int failcol = -1;
-            T rdiag = T(0);
-            bt_chol_step<T, 0>(d, lane, failcol, rdiag);
-            if (failcol >= jb) failcol = -1;      // padding rows are the identity
-            if (lane == 0) sflag[0] = failcol;
-            if (failcol < 0) {
-                if (lane < jb) {
-#pragma unroll
-                    for (int c = 0; c < 32; ++c)
-                        if (c <= lane && c < jb) A[(int64_t)(j0 + c) * lda + j0 + lane] = d[c];
-                    ld_acc -= 2.0 * log((double)rdiag);   // rdiag = 1 / L(i,i); no d[lane]: keeps d in registers
-                }
-                // inverse of the diagonal block: lane c forms column c
-                T *Ls = P;   // staging: row i at Ls[i * BT_PP]
-#pragma unroll
-                for (int c = 0; c < 32; ++c) Ls[lane * BT_PP + c] = (c <= lane) ? d[c] : T(0);
-                __syncwarp();
-                T x[32];
-#pragma unroll
-                for (int i = 0; i < 32; ++i) {
-                    T s0 = T(0), s1 = T(0);
-#pragma unroll
-                    for (int l = 0; l + 1 < i; l += 2) {
-                        s0 = fma(Ls[i * BT_PP + l], x[l], s0);
-                        s1 = fma(Ls[i * BT_PP + l + 1], x[l + 1], s1);
-                    }
-                    if (i & 1) s0 = fma(Ls[i * BT_PP + i - 1], x[i - 1], s0);
-                    const T ri = __shfl_sync(0xffffffffu, rdiag, i);
-                    x[i] = (i < lane) ? T(0) : ((i == lane) ? ri : -(s0 + s1) * ri);
-                }
-#pragma unroll
-                for (int i = 0; i < 32; ++i) Dinv[i * BT_PP + lane] = x[i];   // Dinv[i][c], lower
+                for (int c = 0; c < 32; ++c) P[rr * BT_PP + c] = T(0);
+                continue;
             }
-        }
-        __syncthreads();
-        if (sflag[0] >= 0) {
-            info = j0 + sflag[0] + 1;
-            break;
-        }
-        // (2) panel rows below: L = A D^-T, to global and to the shared panel
-        const int m = n - j0 - jb;
-        for (int rr = tid; rr < m; rr += NT) {
-            const int r = j0 + jb + rr;
+            const int r = o + rr;
             T a[32];
 #pragma unroll
             for (int c = 0; c < 32; ++c) a[c] = (c < jb) ? A[(int64_t)(j0 + c) * lda + r] : T(0);
@@ -149,67 +268,42 @@ __device__ int bt_factor(T *A, int n, int lda, T *Dinv, T *P, int *sflag, double
                 if (c < jb) A[(int64_t)(j0 + c) * lda + r] = x;
                 P[rr * BT_PP + c] = (c < jb) ? x : T(0);
             }
-        }
-        __syncthreads();
-        // (3) trailing update of the lower triangle, TILE x TILE tiles; thread
-        // (ty, tx) of a 16 x NT/16 grid owns rows ty + 16 q and columns
-        // tx + (NT/16) q2 of the tile
-        constexpr int TXN = NT / 16;
-        constexpr int RPT = TILE / 16;          // rows per thread
-        constexpr int CPT = TILE / TXN;         // columns per thread
-        static_assert(RPT >= 1 && CPT >= 1 && RPT * 16 == TILE && CPT * TXN == TILE, "tile shape");
-        const int ty = tid & 15, tx = tid >> 4;
-        const int ntl = (m + TILE - 1) / TILE;
-        const int nitems = ntl * (ntl + 1) / 2;
-        for (int it = 0; it < nitems; ++it) {
-            int bi = (int)((sqrtf(8.0f * it + 1.0f) - 1.0f) * 0.5f);
-            while ((bi + 1) * (bi + 2) / 2 <= it) ++bi;
-            while (bi * (bi + 1) / 2 > it) --bi;
-            const int bj = it - bi * (bi + 1) / 2;
-            {
-                T acc[RPT][CPT];
-#pragma unroll
-                for (int q = 0; q < RPT; ++q)
-#pragma unroll
-                    for (int q2 = 0; q2 < CPT; ++q2) acc[q][q2] = T(0);
+            // forward solve of the rows below: b_r -= L(r, panel) y_panel
+            if (B) {
+                for (int col = 0; col < nrhs; ++col) {
+                    T acc = T(0);
 #pragma unroll 8
-                for (int k = 0; k < BT_NB; ++k) {
-                    T pr[RPT], pc[CPT];
-#pragma unroll
-                    for (int q = 0; q < RPT; ++q) {
-                        const int r = bi * TILE + ty + 16 * q;
-                        pr[q] = r < m ? P[r * BT_PP + k] : T(0);
-                    }
-#pragma unroll
-                    for (int q2 = 0; q2 < CPT; ++q2) {
-                        const int c = bj * TILE + tx + TXN * q2;
-                        pc[q2] = c < m ? P[c * BT_PP + k] : T(0);
-                    }
-#pragma unroll
-                    for (int q = 0; q < RPT; ++q)
-#pragma unroll
-                        for (int q2 = 0; q2 < CPT; ++q2) acc[q][q2] = fma(pr[q], pc[q2], acc[q][q2]);
+                    for (int c = 0; c < 32; ++c) acc = fma(P[rr * BT_PP + c], ybuf[col * 32 + c], acc);
+                    B[(int64_t)col * n + r] -= acc;
                 }
-                // loads first, then stores (see the FP64 POTRF trailing update)
-                T old[RPT][CPT];
-#pragma unroll
-                for (int q = 0; q < RPT; ++q)
-#pragma unroll
-                    for (int q2 = 0; q2 < CPT; ++q2) {
-                        const int r = bi * TILE + ty + 16 * q, c = bj * TILE + tx + TXN * q2;
-                        old[q][q2] = (r < m && c < m && r >= c) ? A[(int64_t)(j0 + jb + c) * lda + j0 + jb + r] : T(0);
-                    }
-#pragma unroll
-                for (int q = 0; q < RPT; ++q)
-#pragma unroll
-                    for (int q2 = 0; q2 < CPT; ++q2) {
-                        const int r = bi * TILE + ty + 16 * q, c = bj * TILE + tx + TXN * q2;
-                        if (r < m && c < m && r >= c)
-                            A[(int64_t)(j0 + jb + c) * lda + j0 + jb + r] = old[q][q2] - acc[q][q2];
-                    }
             }
         }
         __syncthreads();
+        const int mb = m32 / 32;
+        // (a) the next panel's columns: tiles (rb, 0)
+        for (int rb = warp; rb < mb; rb += NW) bt_tile(A, lda, o, m, P, rb, 0, lane);
+        __syncthreads();
+        // (b) warp 0: next diagonal block; the others: tiles (rb, cb), cb >= 1
+        if (warp == 0) {
+            // the rows of B in this block were final after the panel above
+            __threadfence_block();
+            const int f = bt_diag<T>(A, lda, o, min(BT_NB, m), Dinv, Ls, ld_acc, lane);
+            if (lane == 0) sflag[0] = f;
+            if (f < 0 && B) bt_diag_rhs<T>(Dinv, dscr, o, min(BT_NB, m), B, n, nrhs, ybuf, lane);
+        } else {
+            const int nrest = mb * (mb + 1) / 2 - mb;   // tiles with cb >= 1
+            for (int it = warp - 1; it < nrest; it += NW - 1) {
+                // tiles with cb >= 1 enumerated column by column
+                int cb = 1, rem = it;
+                while (rem >= mb - cb) {
+                    rem -= mb - cb;
+                    ++cb;
+                }
+                bt_tile(A, lda, o, m, P, cb + rem, cb, lane);
+            }
+        }
+        __syncthreads();
+        if (sflag[0] >= 0) info = o + sflag[0] + 1;
     }
     // log-determinant: lanes of warp 0 hold the pieces
     if (warp == 0) {
@@ -220,67 +314,41 @@ __device__ int bt_factor(T *A, int n, int lda, T *Dinv, T *P, int *sflag, double
     return info;
 }
 
-// Solve L L^T X = B in place for one problem (factor in A), whole CTA.
+// Backward solve L^T X = Y in place (Y from the fused forward solve), whole
+// CTA, with the stored inverses of the diagonal blocks: for each block j from
+// the last, s = L(below, j)^T x_below (one warp per column, lanes over rows),
+// then x_j = D_j^-T (y_j - s).  No serial substitution chain.
 template <typename T, int NT>
-__device__ void bt_solve(const T *A, int n, int lda, T *B, int ldb, int nrhs, T *red)
+__device__ void bt_backward(const T *A, int n, int lda, T *B, int nrhs, const T *dscr, T *red)
 {
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     constexpr int NW = NT / 32;
     for (int col = 0; col < nrhs; ++col) {
-        T *b = B + (int64_t)col * ldb;
-        // forward: L y = b
-        for (int j0 = 0; j0 < n; j0 += BT_NB) {
-            const int jb = min(BT_NB, n - j0);
-            if (warp == 0) {
-                T row[32];
-#pragma unroll
-                for (int c = 0; c < 32; ++c) row[c] = (lane < jb && c <= lane) ? A[(int64_t)(j0 + c) * lda + j0 + lane] : T(0);
-                T y = lane < jb ? b[j0 + lane] : T(0);
-#pragma unroll
-                for (int i = 0; i < 32; ++i) {
-                    const T lii = __shfl_sync(0xffffffffu, row[i], i);
-                    if (lane == i && i < jb) y = y / lii;
-                    const T yi = __shfl_sync(0xffffffffu, y, i);
-                    if (lane > i && lane < jb) y -= row[i] * yi;
-                }
-                if (lane < jb) b[j0 + lane] = y;
-                red[lane] = lane < jb ? y : T(0);
-            }
-            __syncthreads();
-            for (int r = j0 + jb + tid; r < n; r += NT) {
-                T s = T(0);
-#pragma unroll 8
-                for (int c = 0; c < jb; ++c) s = fma(A[(int64_t)(j0 + c) * lda + r], red[c], s);
-                b[r] -= s;
-            }
-            __syncthreads();
-        }
-        // backward: L^T x = y
+        T *b = B + (int64_t)col * n;
         const int nblk = (n + BT_NB - 1) / BT_NB;
         for (int bk = nblk - 1; bk >= 0; --bk) {
             const int j0 = bk * BT_NB, jb = min(BT_NB, n - j0);
-            // b[j0 + c] -= sum_{r >= j0 + jb} L(r, j0 + c) x_r: warp w takes columns w, w+NW, ...
             for (int c = warp; c < jb; c += NW) {
-                T s = T(0);
-                for (int r = j0 + jb + lane; r < n; r += 32) s = fma(A[(int64_t)(j0 + c) * lda + r], b[r], s);
+                T s0 = T(0), s1 = T(0);
+                const T *Lc = A + (int64_t)(j0 + c) * lda;
+                int r = j0 + jb + lane;
+                for (; r + 32 < n; r += 64) {
+                    s0 = fma(Lc[r], b[r], s0);
+                    s1 = fma(Lc[r + 32], b[r + 32], s1);
+                }
+                if (r < n) s0 = fma(Lc[r], b[r], s0);
+                T s = s0 + s1;
 #pragma unroll
                 for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
                 if (lane == 0) red[c] = s;
             }
             __syncthreads();
             if (warp == 0) {
-                // L_jj^T x = b - red: lane i holds column i of L_jj (rows >= i)
-                T colv[32];
+                const T *Dk = dscr + (int64_t)bk * 32 * 32;   // Dk[i * 32 + c] = D^-1(i, c)
+                const T tl = lane < jb ? b[j0 + lane] - red[lane] : T(0);
+                T x = T(0);
 #pragma unroll
-                for (int r = 0; r < 32; ++r) colv[r] = (lane < jb && r < jb && r >= lane) ? A[(int64_t)(j0 + lane) * lda + j0 + r] : T(0);
-                T x = lane < jb ? b[j0 + lane] - red[lane] : T(0);
-#pragma unroll
-                for (int i = 31; i >= 0; --i) {
-                    if (lane == i && i < jb) x = x / colv[i];
-                    const T xi = __shfl_sync(0xffffffffu, x, i);
-                    // lane l < i: x_l -= L(i, l) x_i = colv_l[i]
-                    if (lane < i) x -= colv[i] * xi;
-                }
+                for (int i = 0; i < 32; ++i) x = fma(Dk[i * 32 + lane], __shfl_sync(0xffffffffu, tl, i), x);
                 if (lane < jb) b[j0 + lane] = x;
             }
             __syncthreads();
@@ -293,8 +361,11 @@ __global__ void __launch_bounds__(NT) batched_posv_kernel(BatchArgs<T> a)
 {
     extern __shared__ __align__(16) unsigned char bsm[];
     T *Dinv = reinterpret_cast<T *>(bsm);
-    T *P = Dinv + 32 * BT_PP;                 // panel rows, BT_PP pitch
+    T *Ls = Dinv + 32 * BT_PP;                // diagonal-block staging
+    T *P = Ls + 32 * BT_PP;                   // panel rows, BT_PP pitch
     __shared__ int sflag[2];
+    __shared__ T ybuf[32 * BT_MAXRHS];
+    T *dscr = a.dscr + (int64_t)blockIdx.x * (BT_NMAX / BT_NB) * 32 * 32;
     while (true) {
         __syncthreads();
         if (threadIdx.x == 0) sflag[1] = atomicAdd(a.ticket, 1);
@@ -305,8 +376,10 @@ __global__ void __launch_bounds__(NT) batched_posv_kernel(BatchArgs<T> a)
         const int n = a.n[i], lda = a.lda[i];
         int info = 0;
         if (n > 0) {
-            info = bt_factor<T, NT, TILE>(a.A[i], n, lda, Dinv, P, sflag, a.logdet ? a.logdet + i : nullptr);
-            if (info == 0 && a.B && a.B[i]) bt_solve<T, NT>(a.A[i], n, lda, a.B[i], n, a.nrhs, P);
+            T *Bi = (a.B && a.nrhs > 0) ? a.B[i] : nullptr;
+            info = bt_factor<T, NT, TILE>(a.A[i], n, lda, Dinv, Ls, P, sflag, a.logdet ? a.logdet + i : nullptr, Bi,
+                                          a.nrhs, dscr, ybuf);
+            if (info == 0 && Bi) bt_backward<T, NT>(a.A[i], n, lda, Bi, a.nrhs, dscr, P);
         } else if (threadIdx.x == 0 && a.logdet) {
             a.logdet[i] = 0.0;
         }
@@ -320,7 +393,7 @@ __global__ void __launch_bounds__(NT) batched_posv_kernel(BatchArgs<T> a)
 template <typename T, int NT, int TILE>
 static size_t bt_smem(int nmax)
 {
-    return (size_t)(32 * BT_PP + (size_t)std::max(nmax, 32) * BT_PP) * sizeof(T);
+    return (size_t)(64 * BT_PP + (size_t)((std::max(nmax, 32) + 31) & ~31) * BT_PP) * sizeof(T);
 }
 
 // prepare: shared-memory attribute and grid (not stream work, so it runs
@@ -343,7 +416,7 @@ static int bt_launch(Context *ctx, const BatchArgs<T> &a, int nmax, cudaStream_t
             ctx->set_error("batched kernel does not fit (n max %d)", nmax);
             return DPLASMA_ERR_INTERNAL_LIMIT;
         }
-        grid_cache[key] = ctx->sms * occ;
+        grid_cache[key] = ctx->sms * std::min(occ, 4);   // the diagonal-inverse scratch holds 4 CTAs per SM
         return 0;
     }
     batched_posv_kernel<T, NT, TILE><<<grid_cache[key], NT, smem, st>>>(a);
@@ -361,10 +434,8 @@ template <typename T>
 static const BtVariant<T> *bt_variants(int &count)
 {
     static const BtVariant<T> v[] = {
-        {"128 threads, 32x32 tiles", bt_launch<T, 128, 32>},
-        {"128 threads, 64x64 tiles", bt_launch<T, 128, 64>},
-        {"256 threads, 32x32 tiles", bt_launch<T, 256, 32>},
-        {"256 threads, 64x64 tiles", bt_launch<T, 256, 64>},
+        {"4 warps per problem", bt_launch<T, 128, 32>},
+        {"8 warps per problem", bt_launch<T, 256, 32>},
     };
     count = (int)(sizeof(v) / sizeof(v[0]));
     return v;
@@ -400,7 +471,7 @@ int batched_posv(Context *ctx, int batch, const int *d_n, const int *d_lda, T *c
         }
         nmax = std::max(nmax, v);
     }
-    if (nmax > BT_NMAX || (size_t)(nmax + 32) * BT_PP * sizeof(T) > 220 * 1024) {
+    if (nmax > BT_NMAX || (size_t)(nmax + 96) * BT_PP * sizeof(T) > 220 * 1024) {
         ctx->set_error("batched problems of order %d exceed the limit", nmax);
         return DPLASMA_ERR_INTERNAL_LIMIT;
     }
@@ -412,7 +483,15 @@ int batched_posv(Context *ctx, int batch, const int *d_n, const int *d_lda, T *c
     int *ticket = dord + batch + 32;
     CK(cudaMemcpyAsync(dord, order.data(), batch * sizeof(int), cudaMemcpyHostToDevice, st));
 
+    if (nrhs > BT_MAXRHS) {
+        ctx->set_error("batched solve takes at most %d right-hand sides (got %d)", BT_MAXRHS, nrhs);
+        return DPLASMA_ERR_NOT_SUPPORTED;
+    }
+    // per-CTA inverses of the diagonal blocks (at most 4 CTAs per SM)
+    T *dscr = (T *)ctx->buffer(BUF_BATCH_SCR, (size_t)ctx->sms * 4 * (BT_NMAX / BT_NB) * 32 * 32 * sizeof(T));
+    if (!dscr) return DPLASMA_ERR_OUT_OF_RESOURCES;
     BatchArgs<T> a;
+    a.dscr = dscr;
     a.batch = batch;
     a.n = d_n;
     a.lda = d_lda;

@@ -35,6 +35,7 @@ enum BufferId : int {
     BUF_BATCH,        // batched: work order and queue counter
     BUF_BATCH_SAVE,   // batched: copy of the inputs while autotuning
     BUF_ADJ,          // adjoint: dense L, W = L^-1 and two products
+    BUF_BATCH_SCR,    // batched: per-CTA inverses of the diagonal blocks
     BUF_COUNT
 };
 

@@ -74,6 +74,15 @@ def test_batched_fp32_backward_errors(gpu_ctx):
     assert (info == 0).sum() >= len(sizes) - 2
 
 
+def test_batched_several_rhs(gpu_ctx):
+    sizes = [33, 64, 200, 511]
+    Ks, ys, mats, rhs, info, logdet = run(gpu_ctx, sizes, torch.float64, nrhs=5)
+    assert (info == 0).all()
+    for K, y, r in zip(Ks, ys, rhs):
+        X = r.cpu().numpy().T            # rhs tensors are (nrhs, n): column-major n x nrhs
+        assert np.abs(K @ X - y.T).max() / (np.abs(K).sum(1).max() * np.abs(X).max()) < 10 * K.shape[0] * 2.0 ** -53
+
+
 def test_batched_info_and_neighbours(gpu_ctx):
     sizes = [50, 80, 120, 33]
     Ks, ys, mats, rhs, info, logdet = run(gpu_ctx, sizes, torch.float64, bad=(1,))
