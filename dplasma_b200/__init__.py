@@ -71,6 +71,7 @@ EXPORTS = (
     "dplasma_b200_fp64_peak_tflops", "dplasma_b200_refine_opts_default", "dplasma_dsposv",
     "dplasma_b200_dsposv_ex", "dplasma_b200_dplgsy_cond", "dplasma_b200_dposv_batched",
     "dplasma_b200_sposv_batched", "dplasma_b200_batched_variant", "dplasma_dpotrf_adjoint",
+    "dplasma_dtrtri", "dplasma_dlauum", "dplasma_dpotri", "dplasma_dpoinv", "dplasma_dpoinv_sync",
 )
 
 
@@ -118,6 +119,9 @@ def lib():
     for f in ("dplasma_b200_dposv_batched", "dplasma_b200_sposv_batched"):
         getattr(L, f).argtypes = [P, I, P, P, P, P, I, P, P]
     L.dplasma_dpotrf_adjoint.argtypes = [P, I, pd, pd]
+    L.dplasma_dtrtri.argtypes = [P, I, I, pd]
+    for f in ("dplasma_dlauum", "dplasma_dpotri", "dplasma_dpoinv", "dplasma_dpoinv_sync"):
+        getattr(L, f).argtypes = [P, I, pd]
     L.dplasma_b200_batched_variant.restype = ctypes.c_char_p
     L.dplasma_b200_batched_variant.argtypes = [P]
     L.dplasma_b200_refine_opts_default.argtypes = [ctypes.POINTER(RefineOpts)]
@@ -301,6 +305,18 @@ class Context:
 
     def batched_variant(self) -> str:
         return lib().dplasma_b200_batched_variant(self.h).decode()
+
+    def dtrtri(self, uplo: int, diag: int, A: Desc) -> int:
+        return lib().dplasma_dtrtri(self.h, uplo, diag, ctypes.byref(A))
+
+    def dlauum(self, uplo: int, A: Desc) -> int:
+        return lib().dplasma_dlauum(self.h, uplo, ctypes.byref(A))
+
+    def dpotri(self, uplo: int, A: Desc) -> int:
+        return lib().dplasma_dpotri(self.h, uplo, ctypes.byref(A))
+
+    def dpoinv(self, uplo: int, A: Desc) -> int:
+        return lib().dplasma_dpoinv(self.h, uplo, ctypes.byref(A))
 
     def dpotrf_adjoint(self, uplo: int, L: Desc, Lbar: Desc) -> int:
         return lib().dplasma_dpotrf_adjoint(self.h, uplo, ctypes.byref(L), ctypes.byref(Lbar))

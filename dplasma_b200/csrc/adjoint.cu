@@ -16,12 +16,17 @@
 // Every product runs on one FP64 tensor-core GEMM kernel over 128x128 output
 // tiles whose K range follows the triangular structure.
 //
+// The same products give the inverse of the factor and of A (dplasma's
+// dtrtri / dlauum / dpotri / dpoinv, src/zpotri_wrapper.c: trtri then lauum):
+//     trtri  W = L^-1;  lauum  L^T L;  potri  A^-1 = W^T W  (lower part).
+//
 // The log-determinant and solve adjoints reduce to it or to rank updates:
 // log det A = 2 sum log L(i,i) gives Lbar(i,i) = 2 / L(i,i) and Abar = A^-1;
 // x = A^-1 b gives Abar = -A^-1 xbar x^T (symmetrized) and bbar = A^-1 xbar.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <vector>
 
 #include "dev_common.cuh"
 #include "dev_trtri.cuh"
@@ -268,7 +273,8 @@ __global__ void ag_sym(double *X, int ld, int n)
 
 // inverses of the 128x128 diagonal blocks of a dense lower factor, written
 // into the diagonal blocks of W (ld = ldw); W's other blocks untouched
-__global__ void __launch_bounds__(256) ag_trtri_diag(const double *L, int ld, double *W, int ldw, double *scratch)
+__global__ void __launch_bounds__(256) ag_trtri_diag(const double *L, int ld, double *W, int ldw, double *scratch,
+                                                     int unit_diag)
 {
     extern __shared__ __align__(16) double tsm[];
     const int b = blockIdx.x;
@@ -283,7 +289,7 @@ __global__ void __launch_bounds__(256) ag_trtri_diag(const double *L, int ld, do
 #pragma unroll
         for (int c = 0; c < 32; ++c) Ls[lane * 33 + c] = (c <= lane) ? T[(int64_t)(p0 + c) * ld + p0 + lane] : 0.0;
         __syncwarp();
-        invert32_lower(Ls, lane, 0, [&](int i, int c, double v) { Wk[(int64_t)(p0 + c) * AG_T + p0 + i] = v; });
+        invert32_lower(Ls, lane, unit_diag, [&](int i, int c, double v) { Wk[(int64_t)(p0 + c) * AG_T + p0 + i] = v; });
         __syncwarp();
     }
     __syncthreads();
@@ -318,7 +324,7 @@ int potrf_adjoint_tiles(Context *ctx, const double *Lt, double *Lbt, const Geom 
     CK(cudaMemsetAsync(W, 0, nn * sizeof(double), st));
     const size_t tsmem = (8 * 32 * 33 + 8 * 32 * 36) * sizeof(double);
     CK(cudaFuncSetAttribute(ag_trtri_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsmem));
-    ag_trtri_diag<<<P, 256, tsmem, st>>>(L, ld, W, ld, scr);
+    ag_trtri_diag<<<P, 256, tsmem, st>>>(L, ld, W, ld, scr, 0);
     CK(cudaGetLastError());
     ctx->launches++;
     for (int i = 1; i < P; ++i) {
@@ -340,6 +346,94 @@ int potrf_adjoint_tiles(Context *ctx, const double *Lt, double *Lbt, const Geom 
     ag_dense_to_tiles<<<tg, 256, 0, st>>>(Y, ld, g.mt, g.nbi, Lbt);
     CK(cudaGetLastError());
     ctx->launches += 2;
+    CK(cudaStreamSynchronize(st));
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
+// inverses: trtri, lauum, potri on the device tiles (lower, padded), in place
+// ---------------------------------------------------------------------------
+// first zero pivot of the diagonal (1-based, 0 if none): LAPACK dtrtri INFO
+__global__ void ag_zero_pivot(const double *L, int ld, int n_valid_rows, const int *rowmap, int *info)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_valid_rows; i += gridDim.x * blockDim.x) {
+        const int ip = rowmap ? rowmap[i] : i;
+        if (L[(int64_t)ip * ld + ip] == 0.0) atomicMin(info, i + 1);
+    }
+}
+
+// W = L^-1 into W (dense, ld), from the dense L; unit: diagonal taken as 1
+static int ag_inverse(Context *ctx, const double *L, double *W, double *Y, double *scr, int P, int ld, int unit)
+{
+    cudaStream_t st = ctx->stream;
+    int rc;
+    CK(cudaMemsetAsync(W, 0, (size_t)ld * ld * sizeof(double), st));
+    const size_t tsmem = (8 * 32 * 33 + 8 * 32 * 36) * sizeof(double);
+    CK(cudaFuncSetAttribute(ag_trtri_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsmem));
+    ag_trtri_diag<<<P, 256, tsmem, st>>>(L, ld, W, ld, scr, unit);
+    CK(cudaGetLastError());
+    ctx->launches++;
+    for (int i = 1; i < P; ++i) {
+        if ((rc = ag_gemm(ctx, AG_ROW, P, i, L, ld, 0, W, ld, Y, ld, 1.0, 0.0))) return rc;
+        if ((rc = ag_gemm(ctx, AG_DIAGMUL, P, i, W, ld, 0, Y, ld, W, ld, -1.0, 0.0))) return rc;
+    }
+    return 0;
+}
+
+// op: 0 trtri (L -> L^-1), 1 lauum (L -> L^T L), 2 potri (L -> (L L^T)^-1);
+// nb/nbi/n describe which padded rows are real (for the INFO of trtri).
+int inverse_tiles(Context *ctx, double *Lt, const Geom &g, int op, int unit, int *info)
+{
+    const int Np = g.mt * g.nbi, P = Np / AG_T, ld = Np;
+    const size_t nn = (size_t)Np * Np;
+    double *D = (double *)ctx->buffer(BUF_ADJ, 4 * nn * sizeof(double) + (size_t)P * AG_T * AG_T * sizeof(double));
+    if (!D) return DPLASMA_ERR_OUT_OF_RESOURCES;
+    double *L = D, *W = D + nn, *Y = D + 2 * nn, *scr = D + 4 * nn;
+    cudaStream_t st = ctx->stream;
+    int rc;
+    const dim3 tg(g.mt, g.mt);
+    ag_tiles_to_dense<<<tg, 256, 0, st>>>(Lt, g.mt, g.nbi, L, ld);
+    CK(cudaGetLastError());
+    ctx->launches++;
+    *info = 0;
+    if (op != 1 && !unit) {
+        // zero pivots (real rows only: row i of the caller is padded row (i/nb)*nbi + i%nb)
+        int *dinfo = (int *)(scr);
+        const int big = 0x7fffffff;
+        CK(cudaMemcpyAsync(dinfo, &big, sizeof(int), cudaMemcpyHostToDevice, st));
+        // a row map is only needed when nb < nbi; build it on the host
+        int *dmap = nullptr;
+        if (g.nb != g.nbi) {
+            std::vector<int> map(g.n);
+            for (int i = 0; i < g.n; ++i) map[i] = (i / g.nb) * g.nbi + i % g.nb;
+            dmap = dinfo + 32;
+            CK(cudaMemcpyAsync(dmap, map.data(), g.n * sizeof(int), cudaMemcpyHostToDevice, st));
+        }
+        ag_zero_pivot<<<ctx->sms, 256, 0, st>>>(L, ld, g.n, dmap, dinfo);
+        CK(cudaGetLastError());
+        int h = big;
+        CK(cudaMemcpyAsync(&h, dinfo, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        ctx->launches++;
+        if (h != big) {
+            *info = h;
+            return 0;
+        }
+    }
+    const double *src = L;
+    if (op != 1) {
+        if ((rc = ag_inverse(ctx, L, W, Y, scr, P, ld, unit))) return rc;
+        src = W;
+    }
+    double *out = W;
+    if (op != 0) {
+        // src^T src, all tiles (k >= max(i, j)); the lower part is the result
+        if ((rc = ag_gemm(ctx, AG_FULL_KGE_MAX, P, 0, src, ld, 1, src, ld, Y, ld, 1.0, 0.0))) return rc;
+        out = Y;
+    }
+    ag_dense_to_tiles<<<tg, 256, 0, st>>>(out, ld, g.mt, g.nbi, Lt);
+    CK(cudaGetLastError());
+    ctx->launches++;
     CK(cudaStreamSynchronize(st));
     return 0;
 }

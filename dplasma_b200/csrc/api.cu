@@ -673,3 +673,88 @@ extern "C" int dplasma_dpotrf_adjoint(parsec_context_t *parsec, dplasma_enum_t u
     ctx->last_factor_ms = ms;
     return 0;
 }
+
+// ---------------------------------------------------------------------------
+// inverses: src/ztrtri_wrapper.c, src/zlauum_wrapper.c, src/zpotri_wrapper.c,
+// src/zpoinv_wrapper.c (dplasma_z.h:78-80,85-86)
+// ---------------------------------------------------------------------------
+static int inverse_api(parsec_context_t *parsec, const char *name, dplasma_enum_t uplo, parsec_tiled_matrix_t *A,
+                       int op, int unit)
+{
+    if (!parsec) return DPLASMA_ERR_NOT_INITIALIZED;
+    int rc;
+    if ((rc = check_square(name, A))) return rc;
+    Context *ctx = &parsec->impl;
+    cudaSetDevice(ctx->device);
+    ctx->launches = 0;
+    ctx->errmsg[0] = 0;
+    if (A->m == 0) return 0;
+    Geom g = make_geom(A->m, A->mb);
+    if (g.mt > 65535 || g.nbi > 512) return DPLASMA_ERR_INTERNAL_LIMIT;
+    double *Lt = (double *)ctx->buffer(BUF_A, g.elems() * sizeof(double));
+    if (!Lt) return DPLASMA_ERR_OUT_OF_RESOURCES;
+    if ((rc = upload_sym(ctx, A, uplo, g, Lt))) return rc;
+    int info = 0;
+    CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    if ((rc = inverse_tiles(ctx, Lt, g, op, unit, &info))) return rc;
+    CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    if (info) return info;   // A untouched, as LAPACK dtrtri on a singular factor
+    if ((rc = download_sym(ctx, A, uplo, g, Lt))) return rc;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    ctx->last_solve_ms = ms;
+    return 0;
+}
+
+// src/ztrtri_wrapper.c: -1 bad uplo, -2 bad diag; INFO > 0 for an exactly zero diagonal entry
+extern "C" int dplasma_dtrtri(parsec_context_t *parsec, dplasma_enum_t uplo, dplasma_enum_t diag,
+                              parsec_tiled_matrix_t *A)
+{
+    if (uplo != dplasmaUpper && uplo != dplasmaLower) {
+        dplasma_error("dplasma_dtrtri", "illegal value of uplo");
+        return -1;
+    }
+    if (diag != dplasmaUnit && diag != dplasmaNonUnit) {
+        dplasma_error("dplasma_dtrtri", "illegal value of diag");
+        return -2;
+    }
+    return inverse_api(parsec, "dplasma_dtrtri", uplo, A, 0, diag == dplasmaUnit);
+}
+
+// src/zlauum_wrapper.c: L^T L (U U^T) of the uplo triangle, in place
+extern "C" int dplasma_dlauum(parsec_context_t *parsec, dplasma_enum_t uplo, parsec_tiled_matrix_t *A)
+{
+    if (uplo != dplasmaUpper && uplo != dplasmaLower) {
+        dplasma_error("dplasma_dlauum", "illegal value of uplo");
+        return -1;
+    }
+    return inverse_api(parsec, "dplasma_dlauum", uplo, A, 1, 0);
+}
+
+// src/zpotri_wrapper.c: trtri then lauum, returns trtri's INFO
+extern "C" int dplasma_dpotri(parsec_context_t *parsec, dplasma_enum_t uplo, parsec_tiled_matrix_t *A)
+{
+    if (uplo != dplasmaUpper && uplo != dplasmaLower) {
+        dplasma_error("dplasma_dpotri", "illegal value of uplo");
+        return -1;
+    }
+    return inverse_api(parsec, "dplasma_dpotri", uplo, A, 2, 0);
+}
+
+// src/zpoinv_wrapper.c: potrf then potri in one call, returns INFO
+extern "C" int dplasma_dpoinv(parsec_context_t *parsec, dplasma_enum_t uplo, parsec_tiled_matrix_t *A)
+{
+    if (uplo != dplasmaUpper && uplo != dplasmaLower) {
+        dplasma_error("dplasma_dpoinv", "illegal value of uplo");
+        return -1;
+    }
+    if (!parsec) return DPLASMA_ERR_NOT_INITIALIZED;
+    const int info = dplasma_dpotrf(parsec, uplo, A);
+    if (info != 0) return info;
+    return dplasma_dpotri(parsec, uplo, A);
+}
+
+extern "C" int dplasma_dpoinv_sync(parsec_context_t *parsec, dplasma_enum_t uplo, parsec_tiled_matrix_t *A)
+{
+    return dplasma_dpoinv(parsec, uplo, A);
+}

@@ -163,6 +163,8 @@ int symm_tiles(Context *ctx, const double *dA, const Geom &g, const double *in, 
 
 // adjoint.cu: Abar from L and Lbar (device tiles, lower); Lbt is overwritten
 int potrf_adjoint_tiles(Context *ctx, const double *Lt, double *Lbt, const Geom &g);
+// op 0 trtri, 1 lauum, 2 potri (device tiles, in place); *info as LAPACK dtrtri
+int inverse_tiles(Context *ctx, double *Lt, const Geom &g, int op, int unit, int *info);
 
 // batched.cu
 template <typename T>

@@ -271,6 +271,24 @@ int dplasma_b200_dsposv_ex(parsec_context_t *parsec, dplasma_enum_t uplo, parsec
                            const parsec_tiled_matrix_t *B, parsec_tiled_matrix_t *X,
                            const dplasma_b200_refine_opts_t *opts, dplasma_b200_refine_stats_t *stats);
 
+/* ---- inverses (the next path after potrf/potrs) --------------------------- */
+/* dplasma_dtrtri: src/ztrtri_wrapper.c (dplasma_z.h:86).  In place inverse of
+ * the uplo triangle; diag dplasmaUnit takes the diagonal as 1.  Returns 0,
+ * -1 / -2 for a bad uplo / diag, or INFO = i when A(i,i) is exactly zero
+ * (A untouched then). */
+int dplasma_dtrtri(parsec_context_t *parsec, dplasma_enum_t uplo, dplasma_enum_t diag, parsec_tiled_matrix_t *A);
+/* dplasma_dlauum: src/zlauum_wrapper.c (dplasma_z.h:78).  L^T L (uplo Lower)
+ * or U U^T (Upper) of the triangle, in place. */
+int dplasma_dlauum(parsec_context_t *parsec, dplasma_enum_t uplo, parsec_tiled_matrix_t *A);
+/* dplasma_dpotri: src/zpotri_wrapper.c (dplasma_z.h:85).  A holds the factor
+ * from dplasma_dpotrf; on return its uplo triangle holds A^-1 (trtri then
+ * lauum).  Returns trtri's INFO. */
+int dplasma_dpotri(parsec_context_t *parsec, dplasma_enum_t uplo, parsec_tiled_matrix_t *A);
+/* dplasma_dpoinv / _sync: src/zpoinv_wrapper.c (dplasma_z.h:79-80).  potrf then
+ * potri: the uplo triangle of SPD A is replaced by that of A^-1; returns INFO. */
+int dplasma_dpoinv(parsec_context_t *parsec, dplasma_enum_t uplo, parsec_tiled_matrix_t *A);
+int dplasma_dpoinv_sync(parsec_context_t *parsec, dplasma_enum_t uplo, parsec_tiled_matrix_t *A);
+
 /* ---- adjoint ------------------------------------------------------------ */
 /* dplasma_dpotrf_adjoint: no dplasma counterpart; the reverse-mode derivative
  * of dplasma_dpotrf.  L holds the factor of A = L L^T (uplo Lower) or
