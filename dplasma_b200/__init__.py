@@ -72,6 +72,7 @@ EXPORTS = (
     "dplasma_b200_dsposv_ex", "dplasma_b200_dplgsy_cond", "dplasma_b200_dposv_batched",
     "dplasma_b200_sposv_batched", "dplasma_b200_batched_variant", "dplasma_dpotrf_adjoint",
     "dplasma_dtrtri", "dplasma_dlauum", "dplasma_dpotri", "dplasma_dpoinv", "dplasma_dpoinv_sync",
+    "dplasma_b200_dpotri_batched",
 )
 
 
@@ -122,6 +123,7 @@ def lib():
     L.dplasma_dtrtri.argtypes = [P, I, I, pd]
     for f in ("dplasma_dlauum", "dplasma_dpotri", "dplasma_dpoinv", "dplasma_dpoinv_sync"):
         getattr(L, f).argtypes = [P, I, pd]
+    L.dplasma_b200_dpotri_batched.argtypes = [P, I, P, P, P, P]
     L.dplasma_b200_batched_variant.restype = ctypes.c_char_p
     L.dplasma_b200_batched_variant.argtypes = [P]
     L.dplasma_b200_refine_opts_default.argtypes = [ctypes.POINTER(RefineOpts)]
@@ -302,6 +304,23 @@ class Context:
         f = lib().dplasma_b200_dposv_batched if dtype == torch.float64 else lib().dplasma_b200_sposv_batched
         return f(self.h, batch, n.data_ptr(), lda.data_ptr(), A.data_ptr(), B.data_ptr() if B is not None else None,
                  nrhs, logdet.data_ptr(), info.data_ptr())
+
+    def potri_batched(self, mats):
+        """dplasma_b200_dpotri_batched on float64 CUDA tensors holding factors
+        (column-major lower = row-major upper, as posv_batched leaves them):
+        each becomes the inverse (column-major lower).  Returns info (CPU)."""
+        import torch
+        batch = len(mats)
+        dev = mats[0].device if batch else torch.device("cuda")
+        n = torch.tensor([m.shape[0] for m in mats], dtype=torch.int32, device=dev)
+        A = torch.tensor([m.data_ptr() for m in mats], dtype=torch.int64, device=dev)
+        info = torch.empty(batch, dtype=torch.int32, device=dev)
+        torch_ready(*mats, n, A)
+        rc = lib().dplasma_b200_dpotri_batched(self.h, batch, n.data_ptr(), n.data_ptr(), A.data_ptr(),
+                                               info.data_ptr())
+        if rc != 0:
+            raise RuntimeError(f"potri_batched rc={rc}: {self.last_error()}")
+        return info.cpu()
 
     def batched_variant(self) -> str:
         return lib().dplasma_b200_batched_variant(self.h).decode()

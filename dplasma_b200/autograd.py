@@ -4,6 +4,10 @@
   float64 CUDA matrix; forward is ``dplasma_dpotrf``, backward
   ``dplasma_dpotrf_adjoint`` (the reverse Cholesky sweep; the gradient returned
   for A is symmetric).
+* ``gp_log_marginal_likelihood_batched(Ks, ys)``: the same for a list of
+  independent problems; forward is one batched launch
+  (``dplasma_b200_dposv_batched``: factor, solve, log-det), backward one
+  batched inverse (``dplasma_b200_dpotri_batched``) for the K_i^-1.
 * ``gp_log_marginal_likelihood(K, y)``: ``-1/2 y^T K^-1 y - 1/2 log det K
   - n/2 log 2 pi`` for a Gaussian-process kernel matrix K and targets y
   (vector or n x m); forward is one factorization and one solve
@@ -135,6 +139,50 @@ class _GPLogML(torch.autograd.Function):
 
 def gp_log_marginal_likelihood(K: torch.Tensor, y: torch.Tensor) -> torch.Tensor:
     return _GPLogML.apply(K, y)
+
+
+class _GPLogMLBatched(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx_, nb, *args):
+        Ks, ys = args[:nb], args[nb:]
+        ctx = context(Ks[0].device)
+        mats = [K.detach().contiguous().clone() for K in Ks]
+        rhs = [y.detach().reshape(1, -1).contiguous().clone() for y in ys]
+        info, logdet = ctx.posv_batched(mats, rhs)
+        if (info != 0).any():
+            raise RuntimeError(f"batched factorization: INFO {info[info != 0][:4].tolist()} (not positive definite)")
+        vals = []
+        for K, y, a, ld in zip(Ks, ys, rhs, logdet.tolist()):
+            n = K.shape[0]
+            vals.append(-0.5 * (y.reshape(-1) * a.reshape(-1)).sum() - 0.5 * ld - 0.5 * n * math.log(2 * math.pi))
+        ctx_.nb = nb
+        ctx_.save_for_backward(*mats, *rhs)
+        ctx_.shapes = [y.shape for y in ys]
+        return torch.stack(vals)
+
+    @staticmethod
+    def backward(ctx_, g):
+        nb = ctx_.nb
+        saved = ctx_.saved_tensors
+        mats, rhs = list(saved[:nb]), saved[nb:]
+        ctx = context(mats[0].device)
+        inv = [m.clone() for m in mats]
+        info = ctx.potri_batched(inv)            # K_i^-1, column-major lower = row-major upper
+        if (info != 0).any():
+            raise RuntimeError("batched inverse failed")
+        dKs, dys = [], []
+        for i, (M, a) in enumerate(zip(inv, rhs)):
+            Kinv = torch.triu(M) + torch.triu(M, 1).t()
+            al = a.reshape(-1, 1)
+            dKs.append(g[i] * (0.5 * al @ al.t() - 0.5 * Kinv))
+            dys.append((-g[i] * al).reshape(ctx_.shapes[i]))
+        return (None, *dKs, *dys)
+
+
+def gp_log_marginal_likelihood_batched(Ks, ys) -> torch.Tensor:
+    """Values (batch,) of the GP log-marginal likelihoods of independent
+    problems K_i (n_i x n_i, float64 CUDA) and y_i (n_i,)."""
+    return _GPLogMLBatched.apply(len(Ks), *Ks, *ys)
 
 
 def se_kernel(x: torch.Tensor, lengthscale: torch.Tensor, nugget: float = 1e-4) -> torch.Tensor:

@@ -758,3 +758,16 @@ extern "C" int dplasma_dpoinv_sync(parsec_context_t *parsec, dplasma_enum_t uplo
 {
     return dplasma_dpoinv(parsec, uplo, A);
 }
+
+extern "C" int dplasma_b200_dpotri_batched(parsec_context_t *parsec, int batch, const int *n, const int *lda,
+                                           double *const *A, int *info)
+{
+    if (batch < 0) return -2;
+    if (!n || !lda || !A || !info) return DPLASMA_ERR_ILLEGAL_VALUE;
+    if (!parsec) return DPLASMA_ERR_NOT_INITIALIZED;
+    Context *ctx = &parsec->impl;
+    cudaSetDevice(ctx->device);
+    ctx->launches = 0;
+    ctx->errmsg[0] = 0;
+    return batched_potri(ctx, batch, n, lda, A, info);
+}

@@ -616,6 +616,264 @@ const char *batched_variant_name(int fp64, int v)
     return (v >= 0 && v < nv) ? vs[v].name : "";
 }
 
+// ---------------------------------------------------------------------------
+// batched inverse from the factors: A_i = L_i (lower) -> A_i^-1 (lower)
+// (dplasma's potri = trtri + lauum, src/zpotri_wrapper.c, per problem), the
+// backward step of a batch of GP likelihoods.  One CTA per problem from the
+// same work queue; 32x32 tiles, one warp per tile, FP64 tensor cores, the
+// factor and W = L^-1 in per-CTA scratch (padded to a multiple of 32 with the
+// identity).
+//   W_jj = L_jj^-1 (warp 0);  W_ij = -(sum_{k=j+1}^{i} W_ik L_kj) W_jj,  j from the last
+//   A^-1 = W^T W:  (i >= j)  sum_{k >= i} W_ki^T W_kj
+// ---------------------------------------------------------------------------
+constexpr int BI_PP = 36;
+
+// acc(32x32) += op(X) op(Y) over one 32-deep K block; X, Y in global memory
+// (column-major, L2 reads), op = transpose when tx / ty
+__device__ __forceinline__ void bi_mma(double (&acc)[2][4][4], const double *X, int ldx, bool tx, const double *Y,
+                                       int ldy, bool ty, int lane)
+{
+    const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int kk = 0; kk < 32; kk += 4) {
+        double af[2][2], bf[4];
+#pragma unroll
+        for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int r = mi * 16 + g + 8 * h, k = kk + t;
+                af[mi][h] = tx ? __ldcg(X + (int64_t)r * ldx + k) : __ldcg(X + (int64_t)k * ldx + r);
+            }
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni) {
+            const int k = kk + t, c = ni * 8 + g;
+            bf[ni] = ty ? __ldcg(Y + (int64_t)k * ldy + c) : __ldcg(Y + (int64_t)c * ldy + k);
+        }
+#pragma unroll
+        for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni) dmma_16x8x4(acc[mi][ni], af[mi][0], af[mi][1], bf[ni]);
+    }
+}
+
+struct BatchInvArgs {
+    int batch;
+    const int *n;
+    const int *lda;
+    double *const *A;
+    int *info;
+    const int *order;
+    int *ticket;
+    double *scr;      // per CTA: padded factor and W, each nmax32^2
+    int nmax32;
+};
+
+__global__ void __launch_bounds__(256) batched_potri_kernel(BatchInvArgs a)
+{
+    extern __shared__ __align__(16) double bism[];
+    double *Wd = bism;                       // W_jj, 32 x BI_PP
+    double *Ls = Wd + 32 * BI_PP;            // staging of L_jj
+    double *Tw = Ls + 32 * BI_PP;            // per warp 32 x BI_PP
+    __shared__ int slot_s, bad_s;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int g = lane >> 2, t = lane & 3;
+    const int64_t ss = (int64_t)a.nmax32 * a.nmax32;
+    double *Lp = a.scr + (int64_t)blockIdx.x * 2 * ss;
+    double *W = Lp + ss;
+    while (true) {
+        __syncthreads();
+        if (tid == 0) slot_s = atomicAdd(a.ticket, 1);
+        __syncthreads();
+        if (slot_s >= a.batch) break;
+        const int pi = a.order[slot_s];
+        const int n = a.n[pi], lda = a.lda[pi];
+        double *A = a.A[pi];
+        if (n <= 0) {
+            if (tid == 0) a.info[pi] = 0;
+            continue;
+        }
+        const int nb = (n + 31) / 32, ld = nb * 32;
+        // padded factor: lower part of L, identity beyond n, zero above
+        for (int64_t e = tid; e < (int64_t)ld * ld; e += 256) {
+            const int r = (int)(e % ld), c = (int)(e / ld);
+            double v = 0.0;
+            if (r >= c) v = (r < n && c < n) ? A[(int64_t)c * lda + r] : (r == c ? 1.0 : 0.0);
+            Lp[e] = v;
+        }
+        __syncthreads();
+        int info = 0;
+        for (int j = nb - 1; j >= 0 && info == 0; --j) {
+            // W_jj = L_jj^-1 by warp 0 (lane c forms column c)
+            if (warp == 0) {
+                const double *Lj = Lp + (int64_t)(32 * j) * ld + 32 * j;
+#pragma unroll
+                for (int c = 0; c < 32; ++c) Ls[lane * BI_PP + c] = (c <= lane) ? __ldcg(Lj + (int64_t)c * ld + lane) : 0.0;
+                __syncwarp();
+                const double dl = Ls[lane * BI_PP + lane];
+                const double rd = 1.0 / dl;
+                const int bad = __ballot_sync(0xffffffffu, dl == 0.0);
+                if (lane == 0) bad_s = bad ? 32 * j + __ffs(bad) : 0;   // INFO of a zero pivot
+                double x[32];
+#pragma unroll
+                for (int i = 0; i < 32; ++i) {
+                    double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+                    for (int l = 0; l + 1 < i; l += 2) {
+                        s0 = fma(Ls[i * BI_PP + l], x[l], s0);
+                        s1 = fma(Ls[i * BI_PP + l + 1], x[l + 1], s1);
+                    }
+                    if (i & 1) s0 = fma(Ls[i * BI_PP + i - 1], x[i - 1], s0);
+                    const double ri = __shfl_sync(0xffffffffu, rd, i);
+                    x[i] = (i < lane) ? 0.0 : ((i == lane) ? ri : -(s0 + s1) * ri);
+                }
+                double *Wj = W + (int64_t)(32 * j) * ld + 32 * j;
+#pragma unroll
+                for (int i = 0; i < 32; ++i) {
+                    Wd[i * BI_PP + lane] = x[i];
+                    Wj[(int64_t)lane * ld + i] = x[i];
+                }
+            }
+            __syncthreads();
+            if (bad_s != 0) {
+                info = bad_s;
+                break;
+            }
+            // block rows below: W_ij = -(sum_{k=j+1}^{i} W_ik L_kj) W_jj
+            double *T = Tw + warp * 32 * BI_PP;
+            for (int i = j + 1 + warp; i < nb; i += 8) {
+                double acc[2][4][4];
+#pragma unroll
+                for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                    for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) acc[mi][ni][q] = 0.0;
+                for (int k = j + 1; k <= i; ++k)
+                    bi_mma(acc, W + (int64_t)(32 * k) * ld + 32 * i, ld, false, Lp + (int64_t)(32 * j) * ld + 32 * k, ld,
+                           false, lane);
+#pragma unroll
+                for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                    for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            const int r = mi * 16 + g + ((q & 2) ? 8 : 0), c = ni * 8 + 2 * t + (q & 1);
+                            T[r * BI_PP + c] = acc[mi][ni][q];
+                            acc[mi][ni][q] = 0.0;
+                        }
+                __syncwarp();
+#pragma unroll
+                for (int kk = 0; kk < 32; kk += 4) {
+                    double af[2][2], bf[4];
+#pragma unroll
+                    for (int mi = 0; mi < 2; ++mi) {
+                        af[mi][0] = T[(mi * 16 + g) * BI_PP + kk + t];
+                        af[mi][1] = T[(mi * 16 + g + 8) * BI_PP + kk + t];
+                    }
+#pragma unroll
+                    for (int ni = 0; ni < 4; ++ni) bf[ni] = Wd[(kk + t) * BI_PP + ni * 8 + g];
+#pragma unroll
+                    for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                        for (int ni = 0; ni < 4; ++ni) dmma_16x8x4(acc[mi][ni], af[mi][0], af[mi][1], bf[ni]);
+                }
+                double *Wij = W + (int64_t)(32 * j) * ld + 32 * i;
+#pragma unroll
+                for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                    for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            const int r = mi * 16 + g + ((q & 2) ? 8 : 0), c = ni * 8 + 2 * t + (q & 1);
+                            Wij[(int64_t)c * ld + r] = -acc[mi][ni][q];
+                        }
+                __syncwarp();
+            }
+            __syncthreads();
+        }
+        if (info == 0) {
+            // A^-1 = W^T W, lower tiles (i >= j), into A
+            const int ntile = nb * (nb + 1) / 2;
+            for (int it = warp; it < ntile; it += 8) {
+                int bi = (int)((sqrtf(8.0f * it + 1.0f) - 1.0f) * 0.5f);
+                while ((bi + 1) * (bi + 2) / 2 <= it) ++bi;
+                while (bi * (bi + 1) / 2 > it) --bi;
+                const int bj = it - bi * (bi + 1) / 2;
+                double acc[2][4][4];
+#pragma unroll
+                for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                    for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) acc[mi][ni][q] = 0.0;
+                for (int k = bi; k < nb; ++k)
+                    bi_mma(acc, W + (int64_t)(32 * bi) * ld + 32 * k, ld, true, W + (int64_t)(32 * bj) * ld + 32 * k, ld,
+                           false, lane);
+#pragma unroll
+                for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                    for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            const int r = 32 * bi + mi * 16 + g + ((q & 2) ? 8 : 0);
+                            const int c = 32 * bj + ni * 8 + 2 * t + (q & 1);
+                            if (r < n && c < n && r >= c) A[(int64_t)c * lda + r] = acc[mi][ni][q];
+                        }
+            }
+        }
+        __syncthreads();
+        if (tid == 0) a.info[pi] = info;
+    }
+}
+
+int batched_potri(Context *ctx, int batch, const int *d_n, const int *d_lda, double *const *d_A, int *d_info)
+{
+    if (batch <= 0) return 0;
+    cudaStream_t st = ctx->stream;
+    std::vector<int> hn(batch);
+    CK(cudaMemcpyAsync(hn.data(), d_n, batch * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    int nmax = 0;
+    for (int v : hn) nmax = std::max(nmax, v);
+    if (nmax > BT_NMAX) return DPLASMA_ERR_INTERNAL_LIMIT;
+    std::vector<int> order(batch);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return hn[x] > hn[y]; });
+    int *dord = (int *)ctx->buffer(BUF_BATCH, ((size_t)batch + 64) * sizeof(int));
+    if (!dord) return DPLASMA_ERR_OUT_OF_RESOURCES;
+    int *ticket = dord + batch + 32;
+    CK(cudaMemcpyAsync(dord, order.data(), batch * sizeof(int), cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(ticket, 0, sizeof(int), st));
+    const int nmax32 = std::max(32, (nmax + 31) & ~31);
+    const size_t smem = (size_t)(2 * 32 * BI_PP + 8 * 32 * BI_PP) * sizeof(double);
+    CK(cudaFuncSetAttribute(batched_potri_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int occ = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batched_potri_kernel, 256, smem));
+    const int grid = ctx->sms * std::max(1, std::min(occ, 2));
+    double *scr = (double *)ctx->buffer(BUF_BATCH_W, (size_t)grid * 2 * nmax32 * nmax32 * sizeof(double));
+    if (!scr) return DPLASMA_ERR_OUT_OF_RESOURCES;
+    BatchInvArgs a;
+    a.batch = batch;
+    a.n = d_n;
+    a.lda = d_lda;
+    a.A = d_A;
+    a.info = d_info;
+    a.order = dord;
+    a.ticket = ticket;
+    a.scr = scr;
+    a.nmax32 = nmax32;
+    CK(cudaEventRecord(ctx->ev0, st));
+    batched_potri_kernel<<<grid, 256, smem, st>>>(a);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(ctx->ev1, st));
+    ctx->launches++;
+    CK(cudaStreamSynchronize(st));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    ctx->last_solve_ms = ms;
+    return 0;
+}
+
 template int batched_posv<double>(Context *, int, const int *, const int *, double *const *, double *const *, int,
                                   double *, int *, int);
 template int batched_posv<float>(Context *, int, const int *, const int *, float *const *, float *const *, int,

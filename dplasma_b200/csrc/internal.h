@@ -36,6 +36,7 @@ enum BufferId : int {
     BUF_BATCH_SAVE,   // batched: copy of the inputs while autotuning
     BUF_ADJ,          // adjoint: dense L, W = L^-1 and two products
     BUF_BATCH_SCR,    // batched: per-CTA inverses of the diagonal blocks
+    BUF_BATCH_W,      // batched inverse: per-CTA padded factor and L^-1
     BUF_COUNT
 };
 
@@ -171,6 +172,7 @@ template <typename T>
 int batched_posv(Context *ctx, int batch, const int *d_n, const int *d_lda, T *const *d_A, T *const *d_B, int nrhs,
                  double *d_logdet, int *d_info, int tune);
 const char *batched_variant_name(int fp64, int v);
+int batched_potri(Context *ctx, int batch, const int *d_n, const int *d_lda, double *const *d_A, int *d_info);
 
 // norms.cu
 int lansy_inf_device(Context *ctx, const double *dA, const Geom &g, double *out);

@@ -321,6 +321,12 @@ int dplasma_b200_dposv_batched(parsec_context_t *parsec, int batch, const int *n
                                double *const *A, double *const *B, int nrhs, double *logdet, int *info);
 int dplasma_b200_sposv_batched(parsec_context_t *parsec, int batch, const int *n, const int *lda,
                                float *const *A, float *const *B, int nrhs, double *logdet, int *info);
+/* dplasma_b200_dpotri_batched: no dplasma counterpart; dplasma_dpotri for a
+ * batch.  A[i] holds the lower factor L_i (as dplasma_b200_dposv_batched
+ * leaves it); on return its lower triangle holds A_i^-1.  info[i] as
+ * dplasma_dpotri.  All arrays in device memory; one persistent launch. */
+int dplasma_b200_dpotri_batched(parsec_context_t *parsec, int batch, const int *n, const int *lda,
+                                double *const *A, int *info);
 /* Name of the kernel variant the last batched call used (autotuner choice). */
 const char *dplasma_b200_batched_variant(const parsec_context_t *parsec);
 

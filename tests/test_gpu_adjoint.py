@@ -118,3 +118,38 @@ def test_gp_log_marginal_likelihood_gradients(gpu_ctx):
     f = lambda l: dag.gp_log_marginal_likelihood(dag.se_kernel(xc, torch.tensor(l, dtype=torch.float64, device="cuda")), yc).item()
     fd = (f(0.2 + h) - f(0.2 - h)) / (2 * h)
     assert abs(fd - lsc.grad.item()) <= 1e-5 * abs(lsc.grad.item())
+
+
+def test_batched_potri_and_gp_gradients(gpu_ctx):
+    # the batch part of the GP configuration: n in [64, 256]
+    rng = np.random.default_rng(13)
+    sizes = [int(v) for v in rng.integers(64, 257, 12)] + [1, 31, 33]
+    gen = torch.Generator().manual_seed(13)
+    xs = [torch.rand(n, 3, generator=gen, dtype=torch.float64) for n in sizes]
+    ys = [torch.randn(n, generator=gen, dtype=torch.float64) for n in sizes]
+    # batched inverse against numpy
+    Ks = [dag.se_kernel(x, torch.tensor(0.2, dtype=torch.float64), nugget=1e-2) for x in xs]
+    mats = [K.cuda().contiguous() for K in Ks]
+    info, _ = gpu_ctx.posv_batched(mats, None)
+    assert (info.numpy() == 0).all()
+    info = gpu_ctx.potri_batched(mats)
+    assert (info.numpy() == 0).all()
+    for K, M in zip(Ks, mats):
+        Mh = M.cpu()
+        Kinv = torch.triu(Mh) + torch.triu(Mh, 1).T
+        ref = torch.linalg.inv(K)
+        assert (Kinv - ref).norm() / ref.norm() < 1e-11
+    # gradients of the summed likelihoods in K and a shared lengthscale
+    ls_ref = torch.tensor(0.2, dtype=torch.float64, requires_grad=True)
+    tot = 0
+    for x, y in zip(xs, ys):
+        K = dag.se_kernel(x, ls_ref)
+        L = torch.linalg.cholesky(K)
+        a = torch.cholesky_solve(y[:, None], L)[:, 0]
+        tot = tot + (-0.5 * y @ a - torch.log(torch.diagonal(L)).sum() - 0.5 * x.shape[0] * np.log(2 * np.pi))
+    tot.backward()
+    ls = torch.tensor(0.2, dtype=torch.float64, device="cuda", requires_grad=True)
+    vals = dag.gp_log_marginal_likelihood_batched([dag.se_kernel(x.cuda(), ls) for x in xs], [y.cuda() for y in ys])
+    assert abs(vals.sum().item() - tot.item()) <= 1e-9 * abs(tot.item())
+    vals.sum().backward()
+    assert abs(ls.grad.item() - ls_ref.grad.item()) <= 1e-8 * abs(ls_ref.grad.item())
