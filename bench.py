@@ -258,7 +258,34 @@ def bench_adjoint(torch):
     torch.cuda.synchronize()
     t_fb = e0.elapsed_time(e1)
     flops_f = n ** 3 / 3.0 + 2.0 * n * n
+    # the batch: 1024 problems, n uniform in [64, 256], shared lengthscale
+    rng = np.random.default_rng(13)
+    sizes = [int(v) for v in rng.integers(64, 257, 1024)]
+    xs = [torch.rand(m, 3, dtype=torch.float64, device="cuda", generator=g) for m in sizes]
+    yb = [torch.randn(m, dtype=torch.float64, device="cuda", generator=g) for m in sizes]
+
+    def fwd_b(l):
+        return dag.gp_log_marginal_likelihood_batched([dag.se_kernel(xx, l) for xx in xs], yb).sum()
+
+    lsb = torch.tensor(0.2, dtype=torch.float64, device="cuda", requires_grad=True)
+    fwd_b(lsb).backward()                       # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    with torch.no_grad():
+        fwd_b(lsb.detach())
+    torch.cuda.synchronize()
+    tb_f = (time.perf_counter() - t0) * 1e3
+    lsb.grad = None
+    t0 = time.perf_counter()
+    fwd_b(lsb).backward()
+    torch.cuda.synchronize()
+    tb_fb = (time.perf_counter() - t0) * 1e3
+    batch = {"problems": 1024, "n": "uniform integer in [64, 256], seed 13", "forward_ms": tb_f,
+             "forward_backward_ms": tb_fb, "dlengthscale": float(lsb.grad),
+             "note": "wall clock including the torch kernel construction and per-problem gradient assembly; "
+                     "library part: one dplasma_b200_dposv_batched and one dplasma_b200_dpotri_batched launch"}
     return {"n": n, "forward_ms": t_f, "forward_backward_ms": t_fb, "backward_over_forward": t_fb / t_f - 1.0,
+            "batch": batch,
             "forward_tflops": flops_f / (t_f * 1e-3) / 1e12, "value": float(v), "dlengthscale": float(ls.grad),
             "note": "backward = dplasma_dpotrf_adjoint for K^-1 (about 1.3 N^3 FP64 tensor-core flops) "
                     "and rank-1 terms; forward = dplasma_dpotrf + dplasma_dpotrs"}
