@@ -122,6 +122,12 @@ __device__ __forceinline__ void red_release_add(int *p, int v)
 {
     asm volatile("red.release.gpu.global.add.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
+// Fire-and-forget FP64 add performed at L2 (no value returned, so the issuing
+// thread never waits for the line).
+__device__ __forceinline__ void red_add_f64(double *p, double v)
+{
+    asm volatile("red.relaxed.gpu.global.add.f64 [%0], %1;" ::"l"(p), "d"(v) : "memory");
+}
 __device__ __forceinline__ int ld_volatile(const int *p)
 {
     return *reinterpret_cast<const volatile int *>(p);

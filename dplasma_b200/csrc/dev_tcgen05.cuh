@@ -102,6 +102,32 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32])
     for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// Two such loads (columns taddr.. and taddr+32..) under one wait.
+__device__ __forceinline__ void tmem_ld32x2(uint32_t taddr, float (&v0)[32], float (&v1)[32])
+{
+    uint32_t r[64];
+#define DB2_TMEM_LD32(OUT, ADDR)                                                                                      \
+    asm volatile(                                                                                                     \
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"              \
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"                                    \
+        : "=r"(OUT[0]), "=r"(OUT[1]), "=r"(OUT[2]), "=r"(OUT[3]), "=r"(OUT[4]), "=r"(OUT[5]), "=r"(OUT[6]),          \
+          "=r"(OUT[7]), "=r"(OUT[8]), "=r"(OUT[9]), "=r"(OUT[10]), "=r"(OUT[11]), "=r"(OUT[12]), "=r"(OUT[13]),      \
+          "=r"(OUT[14]), "=r"(OUT[15]), "=r"(OUT[16]), "=r"(OUT[17]), "=r"(OUT[18]), "=r"(OUT[19]), "=r"(OUT[20]),   \
+          "=r"(OUT[21]), "=r"(OUT[22]), "=r"(OUT[23]), "=r"(OUT[24]), "=r"(OUT[25]), "=r"(OUT[26]), "=r"(OUT[27]),   \
+          "=r"(OUT[28]), "=r"(OUT[29]), "=r"(OUT[30]), "=r"(OUT[31])                                                 \
+        : "r"(ADDR)                                                                                                   \
+        : "memory")
+    DB2_TMEM_LD32(r, taddr);
+    DB2_TMEM_LD32((r + 32), taddr + 32);
+#undef DB2_TMEM_LD32
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) {
+        v0[i] = __uint_as_float(r[i]);
+        v1[i] = __uint_as_float(r[32 + i]);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // TMA tensor (tiled) loads, no multicast
 // ---------------------------------------------------------------------------

@@ -722,29 +722,23 @@ __device__ bool mixed_update(const PotrfArgs &a, SmemCtl *ctl, unsigned char *ri
         const int row = half * BLK + lb + lane;                    // within the tile
         double *C = tile_ptr(a, m, n) + row;                       // column stride nbi
         const double sr = (double)a.scl[m * a.nbs + half];
-        // 64 columns per round: both halves' loads are issued before either
-        // is used, so twice as many C reads are in flight
+        // the update goes to L2 as FP64 reductions: no read of C, so no
+        // round trip to memory on the epilogue's path.  Chunks of one tile are
+        // still ordered by their dependencies (each waits for the previous
+        // chunk's release), so the sum is taken in a fixed order per element.
         for (int c0 = 0; c0 < a.nbi; c0 += 64) {
             if (m == n && c0 > row - lane + 31) break;             // above the diagonal
-            double cv[2][32];
-#pragma unroll
-            for (int h = 0; h < 2; ++h)
-#pragma unroll
-                for (int j = 0; j < 32; ++j) {
-                    const int col = c0 + 32 * h + j;
-                    cv[h][j] = (m != n || row >= col) ? __ldcg(C + (int64_t)col * a.nbi) : 0.0;
-                }
+            float v[2][32];
+            tmem_ld32x2(tmem + ((uint32_t)lb << 16) + (uint32_t)(256 * half + c0), v[0], v[1]);
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 const int cb = c0 + 32 * h;
-                float v[32];
-                tmem_ld32(tmem + ((uint32_t)lb << 16) + (uint32_t)(256 * half + cb), v);
                 // row and column scales are the same for every panel
-                const double inv = 1.0 / (sr * (double)a.scl[n * a.nbs + cb / BLK]);
+                const double inv = -1.0 / (sr * (double)a.scl[n * a.nbs + cb / BLK]);
 #pragma unroll
                 for (int j = 0; j < 32; ++j) {
                     const int col = cb + j;
-                    if (m != n || row >= col) __stcg(C + (int64_t)col * a.nbi, cv[h][j] - (double)v[j] * inv);
+                    if (m != n || row >= col) red_add_f64(C + (int64_t)col * a.nbi, (double)v[h][j] * inv);
                 }
             }
         }
