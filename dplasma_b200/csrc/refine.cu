@@ -15,7 +15,7 @@
 // for condition numbers where plain refinement stagnates.
 //
 // Device kernels here: the symmetric tile product out += alpha A x (FP64
-// DMMA, one CTA per lower tile, panels streamed by bulk copies), column norms,
+// DMMA, persistent CTAs streaming the lower tiles by bulk copies), column norms,
 // column dot products and the small vector updates of GMRES.
 #include <cuda_runtime.h>
 #include <math.h>
@@ -31,150 +31,256 @@ namespace db2 {
 
 // ---------------------------------------------------------------------------
 // out[:, 0:nc] += alpha * A * in[:, 0:nc]   (A symmetric, lower tiles, nbi = 256)
+//
+// Persistent: CTA b streams the lower tiles [b*T/G, (b+1)*T/G) in storage
+// order (one tile column after the other, a contiguous stretch of memory).
+// Each tile (m,n) is read once, in panels of 16 columns, and used twice:
+//   y_m += A(m,n) x_n     warps 4-7, 64 rows each, in registers for the tile,
+//                         added to out at the tile's end (L2 reductions);
+//   y_n += A(m,n)^T x_m   warps 0-3, partial sums over 64 rows each, combined
+//                         through shared memory per panel into per-thread
+//                         registers that live for the whole tile column:
+//                         thread i owns (column 16p + c(i), rhs j(i)) of every
+//                         panel p, added to out when the column ends.
+// A diagonal tile has its upper triangle zeroed and its diagonal halved in
+// shared memory, so the two uses add up to the symmetric product.  Warp 8
+// streams the panels by bulk copies, with the x slices on a tile's first
+// panel: x_m (two buffers, by tile parity) and, when the column changes, x_n
+// (once the consumers have released the previous column's).
 // ---------------------------------------------------------------------------
 constexpr int SY_NBI = 256;
 constexpr int SY_PC = 16;                 // columns per panel
+constexpr int SY_NP = SY_NBI / SY_PC;     // panels per tile
 constexpr int SY_NST = 3;                 // panel stages
-constexpr int SY_PP = SY_NBI + 4;         // panel pitch (doubles), == 4 mod 16: conflict-free fragments
+constexpr int SY_PP = SY_NBI + 4;         // pitch (doubles), == 4 mod 16: conflict-free fragments
 constexpr int SY_NC = 16;                 // right-hand-side columns per launch
-constexpr int SY_THREADS = 256;
-constexpr size_t SY_SMEM = (size_t)(SY_NST * SY_PC * SY_PP + 2 * SY_NC * SY_PP + 2 * 8 * 256) * sizeof(double) + 64;
+constexpr int SY_THREADS = 288;           // 8 consumer warps + the producer warp
+constexpr int SY_SLICE = SY_NC * SY_PP;   // one x slice, [rhs][row]
+struct SyCtl {
+    uint64_t full[SY_NST];
+    uint64_t empty[SY_NST];
+    uint64_t xn_free;
+};
+constexpr size_t SY_SMEM =
+    (size_t)(SY_NST * SY_PC * SY_PP + 3 * SY_SLICE + 2 * 4 * 256) * sizeof(double) + sizeof(SyCtl);
+
+// tile column n and row m of the lower tile with storage index t
+__device__ __forceinline__ void sy_tile_of(int64_t t, int mt, int &m, int &n)
+{
+    int c = 0;
+    while (c + 1 < mt && lower_tile_index(c + 1, c + 1, mt) <= t) ++c;
+    n = c;
+    m = c + (int)(t - lower_tile_index(c, c, mt));
+}
 
 __global__ void __launch_bounds__(SY_THREADS, 1)
-    symm_tiles_kernel(const double *__restrict__ A, int mt, const double *__restrict__ in, int ldin,
-                      double *__restrict__ out, int ldout, int nc, double alpha, int *status, uint64_t limit_ns)
+    symm_stream_kernel(const double *__restrict__ A, int mt, const double *__restrict__ in, int ldin,
+                       double *__restrict__ out, int ldout, int nc, double alpha, int *status, uint64_t limit_ns)
 {
-    const int m = blockIdx.x, n = blockIdx.y;
-    if (m < n) return;
     extern __shared__ __align__(16) double sy[];
-    double *P = sy;                                     // [stage][c][r]
-    double *Xn = P + SY_NST * SY_PC * SY_PP;            // [j][c]: in rows of tile column n
-    double *Xm = Xn + SY_NC * SY_PP;                    // [j][r]: in rows of tile row m
-    double *red = Xm + SY_NC * SY_PP;                   // [2][warp][lane*8]
-    uint64_t *full = reinterpret_cast<uint64_t *>(red + 2 * 8 * 256);
+    double *P = sy;                                 // [stage][c][PP]
+    double *Xm = P + SY_NST * SY_PC * SY_PP;        // [2][rhs][PP]: x rows of tile row m
+    double *Xn = Xm + 2 * SY_SLICE;                 // [rhs][PP]: x rows of tile column n
+    double *red = Xn + SY_SLICE;                    // [2][4 warps][256]
+    SyCtl *ctl = reinterpret_cast<SyCtl *>(red + 2 * 4 * 256);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int g = lane >> 2, t = lane & 3;
-    const double *T = A + lower_tile_index(m, n, mt) * (int64_t)SY_NBI * SY_NBI;
-    constexpr int NP = SY_NBI / SY_PC;
+    const int g = lane >> 2, t4 = lane & 3;
+    const int64_t T = (int64_t)mt * (mt + 1) / 2;
+    const int64_t t0 = T * blockIdx.x / gridDim.x, t1 = T * (blockIdx.x + 1) / gridDim.x;
 
     if (tid == 0) {
-        for (int s = 0; s < SY_NST; ++s) mbar_init(&full[s], 1);
+        for (int s = 0; s < SY_NST; ++s) {
+            mbar_init(&ctl->full[s], 1);
+            mbar_init(&ctl->empty[s], 8);
+        }
+        mbar_init(&ctl->xn_free, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
+    // right-hand sides beyond nc stay zero in every x slice
+    for (int e = tid; e < 3 * SY_SLICE; e += SY_THREADS)
+        if ((e % SY_SLICE) / SY_PP >= nc) Xm[e] = 0.0;
     __syncthreads();
-    if (warp == 0) {
-        for (int s = 0; s < SY_NST; ++s) {
-            if (lane == 0) mbar_arrive_expect_tx(&full[s], SY_PC * SY_NBI * sizeof(double));
-            __syncwarp();
-            if (lane < SY_PC)
-                bulk_g2s(P + (s * SY_PC + lane) * SY_PP, T + (int64_t)(s * SY_PC + lane) * SY_NBI,
-                         SY_NBI * sizeof(double), &full[s]);
-        }
-    }
-    for (int e = tid; e < SY_NC * SY_NBI; e += SY_THREADS) {
-        const int j = e / SY_NBI, r = e % SY_NBI;
-        Xn[j * SY_PP + r] = j < nc ? in[(int64_t)j * ldin + (int64_t)n * SY_NBI + r] : 0.0;
-        Xm[j * SY_PP + r] = j < nc ? in[(int64_t)j * ldin + (int64_t)m * SY_NBI + r] : 0.0;
-    }
-    __syncthreads();
+    if (t0 >= t1) return;
 
-    double ym[2][2][4];
-#pragma unroll
-    for (int a = 0; a < 2; ++a)
-#pragma unroll
-        for (int b = 0; b < 2; ++b)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) ym[a][b][q] = 0.0;
-
-    for (int p = 0; p < NP; ++p) {
-        const int s = p % SY_NST;
-        const bool ok = mbar_wait(&full[s], (p / SY_NST) & 1, limit_ns);
-        if (__syncthreads_or(!ok)) {
-            if (tid == 0) {
-                atomicCAS(status, 0, 2);
-                // copies already issued must land before the CTA exits
-                for (int q = p; q < NP && q < p + SY_NST; ++q) mbar_wait(&full[q % SY_NST], (q / SY_NST) & 1, limit_ns);
+    if (warp == 8) {
+        // producer
+        int m, n;
+        sy_tile_of(t0, mt, m, n);
+        uint32_t it = 0, cols = 0;
+        int cur_n = -1;
+        bool ok = true;
+        for (int64_t t = t0; t < t1 && ok; ++t) {
+            const double *Tt = A + t * (int64_t)SY_NBI * SY_NBI;
+            const int xb = (int)((t - t0) & 1);
+            const bool new_col = (n != cur_n);
+            if (new_col && cur_n >= 0 && !warp_mbar_wait(&ctl->xn_free, (cols - 1) & 1, limit_ns)) {
+                if (lane == 0) atomicCAS(status, ST_OK, ST_MBAR_TIMEOUT);
+                ok = false;
+                break;
             }
+            for (int p = 0; p < SY_NP; ++p) {
+                const uint32_t s = it % SY_NST, r = it / SY_NST;
+                if (r > 0 && !warp_mbar_wait(&ctl->empty[s], (r - 1) & 1, limit_ns)) {
+                    if (lane == 0) atomicCAS(status, ST_OK, ST_MBAR_TIMEOUT);
+                    ok = false;
+                    break;
+                }
+                uint32_t bytes = SY_PC * SY_NBI * sizeof(double);
+                if (p == 0) bytes += (uint32_t)nc * SY_NBI * sizeof(double) * (new_col ? 2 : 1);
+                if (lane == 0) mbar_arrive_expect_tx(&ctl->full[s], bytes);
+                __syncwarp();
+                if (lane < SY_PC) {
+                    bulk_g2s(P + (s * SY_PC + lane) * SY_PP, Tt + (int64_t)(p * SY_PC + lane) * SY_NBI,
+                             SY_NBI * sizeof(double), &ctl->full[s]);
+                } else if (p == 0 && lane - SY_PC < nc) {
+                    const int j = lane - SY_PC;
+                    bulk_g2s(Xm + xb * SY_SLICE + j * SY_PP, in + (int64_t)j * ldin + (int64_t)m * SY_NBI,
+                             SY_NBI * sizeof(double), &ctl->full[s]);
+                    if (new_col)
+                        bulk_g2s(Xn + j * SY_PP, in + (int64_t)j * ldin + (int64_t)n * SY_NBI, SY_NBI * sizeof(double),
+                                 &ctl->full[s]);
+                }
+                ++it;
+            }
+            if (new_col) {
+                cur_n = n;
+                ++cols;
+            }
+            if (++m == mt) {
+                ++n;
+                m = n;
+            }
+        }
+        // copies already issued land before the CTA may exit
+        const uint32_t first = it > SY_NST ? it - SY_NST : 0;
+        for (uint32_t k = first; k < it; ++k) warp_mbar_wait(&ctl->full[k % SY_NST], (k / SY_NST) & 1, limit_ns);
+        return;
+    }
+
+    // consumers
+    int m, n;
+    sy_tile_of(t0, mt, m, n);
+    double yacc[SY_NP];                   // y_n outputs of this thread, one per panel
+#pragma unroll
+    for (int p = 0; p < SY_NP; ++p) yacc[p] = 0.0;
+    const int rl = tid & 31, rni = (tid >> 5) & 1, rq = (tid >> 6) & 3;
+    const int rc = (rl >> 2) + ((rq & 2) ? 8 : 0), rj = rni * 8 + 2 * (rl & 3) + (rq & 1);
+    uint32_t it = 0;
+    for (int64_t t = t0; t < t1; ++t) {
+        const double *xm = Xm + (int)((t - t0) & 1) * SY_SLICE;
+        double ym[4][2][4];
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) ym[mi][ni][q] = 0.0;
+        bool ok = true;
+#pragma unroll
+        for (int p = 0; p < SY_NP; ++p) {
+            const uint32_t s = it % SY_NST;
+            const bool got = warp_mbar_wait(&ctl->full[s], (it / SY_NST) & 1, limit_ns);
+            double *Ps = P + s * SY_PC * SY_PP;
+            if (m == n) {
+                // every warp reads the whole panel: fix it up between two barriers
+                if (named_bar_or(1, 256, !got)) {
+                    ok = false;
+                    break;
+                }
+                for (int e = tid; e < SY_PC * SY_NBI; e += 256) {
+                    const int c = e / SY_NBI, r = e % SY_NBI;
+                    double &v = Ps[c * SY_PP + r];
+                    if (r < p * SY_PC + c) v = 0.0;
+                    else if (r == p * SY_PC + c) v *= 0.5;
+                }
+                fence_proxy_async();   // the stage is refilled by the async proxy
+                named_bar_sync(1, 256);
+            }
+            if (got) {
+                if (warp < 4) {
+                    // y_n(16 panel columns, rhs) partial over rows 64w..64w+63: P^T x_m
+                    const int R0 = warp * 64;
+                    double yn[2][2][4];
+#pragma unroll
+                    for (int h = 0; h < 2; ++h)
+#pragma unroll
+                        for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+                            for (int q = 0; q < 4; ++q) yn[h][ni][q] = 0.0;
+#pragma unroll
+                    for (int kk = 0; kk < 64; kk += 4) {
+                        const int r = R0 + kk + t4;
+                        const double a0 = Ps[g * SY_PP + r], a1 = Ps[(g + 8) * SY_PP + r];
+#pragma unroll
+                        for (int ni = 0; ni < 2; ++ni)
+                            dmma_16x8x4(yn[(kk >> 2) & 1][ni], a0, a1, xm[(ni * 8 + g) * SY_PP + r]);
+                    }
+                    double *rb = red + (p & 1) * 1024 + warp * 256 + lane * 8;
+#pragma unroll
+                    for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) rb[ni * 4 + q] = yn[0][ni][q] + yn[1][ni][q];
+                } else {
+                    // y_m(rows 64(w-4).., rhs) += P(rows, 16 columns) x_n(16 columns, rhs)
+                    const int R0 = (warp - 4) * 64, c0 = p * SY_PC;
+#pragma unroll
+                    for (int kk = 0; kk < SY_PC; kk += 4) {
+                        double bf[2];
+#pragma unroll
+                        for (int ni = 0; ni < 2; ++ni) bf[ni] = Xn[(ni * 8 + g) * SY_PP + c0 + kk + t4];
+#pragma unroll
+                        for (int mi = 0; mi < 4; ++mi) {
+                            const double a0 = Ps[(kk + t4) * SY_PP + R0 + mi * 16 + g];
+                            const double a1 = Ps[(kk + t4) * SY_PP + R0 + mi * 16 + g + 8];
+#pragma unroll
+                            for (int ni = 0; ni < 2; ++ni) dmma_16x8x4(ym[mi][ni], a0, a1, bf[ni]);
+                        }
+                    }
+                }
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&ctl->empty[s]);
+            }
+            ++it;
+            if (named_bar_or(1, 256, !got)) {
+                ok = false;
+                break;
+            }
+            // the four partial sums of this panel's y_n
+            const double *rr = red + (p & 1) * 1024 + rl * 8 + rni * 4 + rq;
+            yacc[p] += (rr[0] + rr[256]) + (rr[512] + rr[768]);
+        }
+        if (!ok) {
+            if (tid == 0) atomicCAS(status, ST_OK, ST_MBAR_TIMEOUT);
             return;
         }
-        double *Ps = P + s * SY_PC * SY_PP;
-        const int c0 = p * SY_PC;
-        if (m == n) {
-            // symmetric use of the lower triangle: keep r > c, halve the diagonal
-            for (int e = tid; e < SY_PC * SY_NBI; e += SY_THREADS) {
-                const int c = e / SY_NBI, r = e % SY_NBI;
-                double &v = Ps[c * SY_PP + r];
-                if (r < c0 + c) v = 0.0;
-                else if (r == c0 + c) v *= 0.5;
+        if (warp >= 4) {
+            const int R0 = (warp - 4) * 64;
+#pragma unroll
+            for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int r = R0 + mi * 16 + g + ((q & 2) ? 8 : 0);
+                        const int j = ni * 8 + 2 * t4 + (q & 1);
+                        if (j < nc) red_add_f64(out + (int64_t)j * ldout + (int64_t)m * SY_NBI + r, alpha * ym[mi][ni][q]);
+                    }
+        }
+        const bool col_end = (m + 1 == mt);
+        if (col_end || t + 1 == t1) {
+#pragma unroll
+            for (int p = 0; p < SY_NP; ++p) {
+                if (rj < nc) red_add_f64(out + (int64_t)rj * ldout + (int64_t)n * SY_NBI + p * SY_PC + rc, alpha * yacc[p]);
+                yacc[p] = 0.0;
             }
-            __syncthreads();
+            // every consumer warp passed the last panel's barrier: x_n is free
+            if (col_end && tid == 0) mbar_arrive(&ctl->xn_free);
         }
-        // y_m(rows 32w..32w+31) += P(rows, 16 cols) * Xn(16 cols, j)
-#pragma unroll
-        for (int kk = 0; kk < SY_PC; kk += 4) {
-            double af[2][2], bf[2];
-#pragma unroll
-            for (int mi = 0; mi < 2; ++mi) {
-                af[mi][0] = Ps[(kk + t) * SY_PP + warp * 32 + mi * 16 + g];
-                af[mi][1] = Ps[(kk + t) * SY_PP + warp * 32 + mi * 16 + g + 8];
-            }
-#pragma unroll
-            for (int ni = 0; ni < 2; ++ni) bf[ni] = Xn[(ni * 8 + g) * SY_PP + c0 + kk + t];
-#pragma unroll
-            for (int mi = 0; mi < 2; ++mi)
-#pragma unroll
-                for (int ni = 0; ni < 2; ++ni) dmma_16x8x4(ym[mi][ni], af[mi][0], af[mi][1], bf[ni]);
-        }
-        // y_n(16 cols, j) partial over rows 32w..32w+31: P^T * Xm
-        double yn[2][4];
-#pragma unroll
-        for (int ni = 0; ni < 2; ++ni)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) yn[ni][q] = 0.0;
-#pragma unroll
-        for (int kk = 0; kk < 32; kk += 4) {
-            const int r = warp * 32 + kk + t;
-            const double a0 = Ps[g * SY_PP + r], a1 = Ps[(g + 8) * SY_PP + r];
-#pragma unroll
-            for (int ni = 0; ni < 2; ++ni) dmma_16x8x4(yn[ni], a0, a1, Xm[(ni * 8 + g) * SY_PP + r]);
-        }
-        double *rb = red + (p & 1) * (8 * 256) + warp * 256 + lane * 8;
-#pragma unroll
-        for (int ni = 0; ni < 2; ++ni)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) rb[ni * 4 + q] = yn[ni][q];
-        fence_proxy_async();   // the diagonal fix-up wrote stage s through the generic proxy
-        __syncthreads();       // stage s and this panel's partials are complete
-        if (warp == 0 && p + SY_NST < NP) {
-            const int pn = p + SY_NST;
-            if (lane == 0) mbar_arrive_expect_tx(&full[s], SY_PC * SY_NBI * sizeof(double));
-            __syncwarp();
-            if (lane < SY_PC)
-                bulk_g2s(Ps + lane * SY_PP, T + (int64_t)(pn * SY_PC + lane) * SY_NBI, SY_NBI * sizeof(double),
-                         &full[s]);
-        }
-        {
-            // thread -> (lane l, register q): output column c, rhs j
-            const int l = tid & 31, ni = (tid >> 5) & 1, q = (tid >> 6) & 3;
-            const double *rr = red + (p & 1) * (8 * 256) + l * 8 + ni * 4 + q;
-            double v = 0.0;
-#pragma unroll
-            for (int w = 0; w < 8; ++w) v += rr[w * 256];
-            const int gg = l >> 2, tt = l & 3;
-            const int c = gg + ((q & 2) ? 8 : 0), j = ni * 8 + 2 * tt + (q & 1);
-            if (j < nc) atomicAdd(out + (int64_t)j * ldout + (int64_t)n * SY_NBI + c0 + c, alpha * v);
+        if (++m == mt) {
+            ++n;
+            m = n;
         }
     }
-#pragma unroll
-    for (int mi = 0; mi < 2; ++mi)
-#pragma unroll
-        for (int ni = 0; ni < 2; ++ni)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int r = warp * 32 + mi * 16 + g + ((q & 2) ? 8 : 0);
-                const int j = ni * 8 + 2 * t + (q & 1);
-                if (j < nc) atomicAdd(out + (int64_t)j * ldout + (int64_t)m * SY_NBI + r, alpha * ym[mi][ni][q]);
-            }
 }
 
 int symm_tiles(Context *ctx, const double *dA, const Geom &g, const double *in, int ldin, double *out, int ldout,
@@ -184,12 +290,18 @@ int symm_tiles(Context *ctx, const double *dA, const Geom &g, const double *in, 
         ctx->set_error("symmetric tile product supports 256-wide internal tiles only");
         return DPLASMA_ERR_NOT_SUPPORTED;
     }
-    CK(cudaFuncSetAttribute(symm_tiles_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SY_SMEM));
+    if (((uintptr_t)in % 16) != 0 || (ldin % 2) != 0) {
+        ctx->set_error("symmetric tile product: x columns must be 16-byte aligned");
+        return DPLASMA_ERR_ILLEGAL_VALUE;
+    }
+    CK(cudaFuncSetAttribute(symm_stream_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SY_SMEM));
+    const int64_t T = (int64_t)g.mt * (g.mt + 1) / 2;
+    const int grid = (int)std::min<int64_t>(T, ctx->sms);
     for (int c0 = 0; c0 < ncols; c0 += SY_NC) {
         const int nc = std::min(SY_NC, ncols - c0);
-        symm_tiles_kernel<<<dim3(g.mt, g.mt), SY_THREADS, SY_SMEM, ctx->stream>>>(
-            dA, g.mt, in + (size_t)c0 * ldin, ldin, out + (size_t)c0 * ldout, ldout, nc, alpha, status,
-            ctx->pipe_limit_ns);
+        symm_stream_kernel<<<grid, SY_THREADS, SY_SMEM, ctx->stream>>>(dA, g.mt, in + (size_t)c0 * ldin, ldin,
+                                                                      out + (size_t)c0 * ldout, ldout, nc, alpha,
+                                                                      status, ctx->pipe_limit_ns);
         CK(cudaGetLastError());
         ctx->launches++;
     }
