@@ -72,7 +72,7 @@ EXPORTS = (
     "dplasma_b200_dsposv_ex", "dplasma_b200_dplgsy_cond", "dplasma_b200_dposv_batched",
     "dplasma_b200_sposv_batched", "dplasma_b200_batched_variant", "dplasma_dpotrf_adjoint",
     "dplasma_dtrtri", "dplasma_dlauum", "dplasma_dpotri", "dplasma_dpoinv", "dplasma_dpoinv_sync",
-    "dplasma_b200_dpotri_batched",
+    "dplasma_b200_dpotri_batched", "pdpotrf_",
 )
 
 
@@ -124,6 +124,9 @@ def lib():
     for f in ("dplasma_dlauum", "dplasma_dpotri", "dplasma_dpoinv", "dplasma_dpoinv_sync"):
         getattr(L, f).argtypes = [P, I, pd]
     L.dplasma_b200_dpotri_batched.argtypes = [P, I, P, P, P, P]
+    pi = ctypes.POINTER(I)
+    L.pdpotrf_.restype = None
+    L.pdpotrf_.argtypes = [ctypes.c_char_p, pi, P, pi, pi, pi, pi]
     L.dplasma_b200_batched_variant.restype = ctypes.c_char_p
     L.dplasma_b200_batched_variant.argtypes = [P]
     L.dplasma_b200_refine_opts_default.argtypes = [ctypes.POINTER(RefineOpts)]
@@ -383,3 +386,18 @@ def attach(d: Desc, buf) -> Desc:
         d.mat = buf.data_ptr()
         d.location = DEVICE
     return d
+
+
+def pdpotrf(uplo: str, n: int, a, ia: int, ja: int, desca) -> int:
+    """ScaLAPACK's PDPOTRF through the library's pdpotrf_ entry: `a` is the
+    local (here: whole) column-major array as a Fortran-ordered float64 numpy
+    array, `desca` the 9 descriptor integers; returns INFO."""
+    if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.f_contiguous):
+        raise ValueError("a must be a Fortran-ordered float64 array")
+    L = lib()
+    c = ctypes.c_int
+    d = (c * 9)(*[int(v) for v in desca])
+    info = c(0)
+    L.pdpotrf_(uplo.encode()[:1], ctypes.byref(c(n)), a.ctypes.data_as(ctypes.c_void_p), ctypes.byref(c(ia)),
+               ctypes.byref(c(ja)), d, ctypes.byref(info))
+    return info.value

@@ -330,6 +330,21 @@ int dplasma_b200_dpotri_batched(parsec_context_t *parsec, int batch, const int *
 /* Name of the kernel variant the last batched call used (autotuner choice). */
 const char *dplasma_b200_batched_variant(const parsec_context_t *parsec);
 
+/* ---- ScaLAPACK-compatible entry ------------------------------------------ */
+/* pdpotrf_: src/scalapack_wrappers/dplasma_wrapper_pdpotrf.c:139-305 (the
+ * Fortran binding pdpotrf_ of GENERATE_F77_BINDINGS, :297-303); ScaLAPACK's
+ * PDPOTRF(UPLO, N, A, IA, JA, DESCA, INFO).  DESCA is the 9-integer
+ * ScaLAPACK descriptor {DTYPE=1, CTXT, M, N, MB, NB, RSRC, CSRC, LLD}; one
+ * process owns the whole matrix (a 1 x 1 grid: RSRC = CSRC = 0, LLD >= M).
+ * The column-major submatrix A(IA:IA+N-1, JA:JA+N-1) (1-based, starting on
+ * a block boundary, MB = NB) is factored in place on the GPU.  INFO = 0,
+ * -(100*i+j) / -i for an illegal entry j of array argument i / scalar
+ * argument i, k > 0 when the leading minor of order k is not positive
+ * definite, DPLASMA_ERR_NOT_INITIALIZED without a usable GPU.  Device:
+ * DPLASMA_B200_DEVICE (default 0), context kept until process exit. */
+void pdpotrf_(const char *uplo, const int *n, double *a, const int *ia, const int *ja, const int *desca,
+              int *info);
+
 /* ---- instrumentation ---------------------------------------------------- */
 /* Device time in milliseconds of the last factorization (CUDA events around
  * the scheduler launch only) and of the last triangular-solve pair. */

@@ -147,6 +147,41 @@ def test_argument_checks_without_a_device():
     assert L.dplasma_b200_taskpool_run(None, None) == db.ERR_NOT_INITIALIZED
 
 
+def test_pdpotrf_argument_checks_without_a_device():
+    """ScaLAPACK PDPOTRF's INFO codes for illegal arguments (-i for scalar
+    argument i, -(100 i + j) for entry j of array argument i), returned before
+    any device work; N = 0 is a no-op."""
+    N, NB = 64, 16
+    a = np.asfortranarray(np.eye(N))
+    good = [1, 0, N, N, NB, NB, 0, 0, N]
+
+    def info(uplo="L", n=N, ia=1, ja=1, desc=None):
+        return db.pdpotrf(uplo, n, a, ia, ja, good if desc is None else desc)
+
+    def with_(j, v):
+        d = list(good)
+        d[j] = v
+        return d
+
+    assert info(desc=with_(0, 2)) == -601          # DTYPE
+    assert info(uplo="X") == -1
+    assert info(n=-1) == -2
+    assert info(ia=0) == -4
+    assert info(ja=0) == -5
+    assert info(desc=with_(4, 0)) == -605          # MB
+    assert info(desc=with_(5, 0)) == -606          # NB
+    assert info(desc=with_(6, 1)) == -607          # RSRC: one process owns the matrix
+    assert info(desc=with_(7, 1)) == -608          # CSRC
+    assert info(desc=with_(8, N - 1)) == -609      # LLD < M
+    assert info(ia=2, n=N - 1) == -4               # not on a block boundary
+    assert info(ja=2, n=N - 1) == -5
+    assert info(ia=NB + 1) == -603                 # IA + N - 1 > M
+    assert info(ja=NB + 1) == -604
+    assert info(desc=with_(4, 8)) == -606          # MB != NB
+    assert np.array_equal(a, np.eye(N))
+    assert info(n=0) == 0
+
+
 def test_python_side_refuses_without_gpu_library_context():
     import torch
     if torch.cuda.is_available():
