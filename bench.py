@@ -491,9 +491,12 @@ def run_gpu(args):
                      "frac": achieved / peak16 if peak16 else None, "traffic": traffic,
                      "kernel": "potrf_persistent_kernel<true> (mixed factorization)",
                      "tensor_flops_per_launch": tensor_flops,
-                     "note": "achieved counts N^3/3 (FP64-equivalent) per launch; peak = dense bf16 burst of "
-                             "measured (MEASURED_PEAKS.json); the kernel is bound by the FP64 tile traffic of "
-                             "its in-place epilogue and the FP64 critical path, not by the tensor pipe"},
+                     "tensor_achieved": tensor_flops / (fac_ms * 1e-3) / 1e12 if fac_ms else None,
+                     "tensor_frac": tensor_flops / (fac_ms * 1e-3) / 1e12 / peak16 if (fac_ms and peak16) else None,
+                     "note": "achieved counts N^3/3 (FP64-equivalent) per launch, tensor_achieved the 16-bit "
+                             "tensor work actually issued (x3 in the split form); peak = dense bf16 burst of "
+                             "measured (MEASURED_PEAKS.json); the update tasks run the tensor pipe near its "
+                             "peak, the rest of the launch is the FP64 POTRF/TRSM work and its chain"},
         "roofline_fp64": {"bound": "tensor", "achieved": ach64, "peak": peak64, "unit": "TFLOP/s",
                           "frac": ach64 / peak64 if peak64 > 0 else None,
                           "kernel": "potrf_persistent_kernel<false> (FP64 DMMA)",
