@@ -341,33 +341,74 @@ __device__ __forceinline__ bool consume_job(const PotrfArgs &a, SmemCtl *ctl, co
     return true;
 }
 
-// One step j of the unblocked right-looking Cholesky of a 32x32 block held
-// by one warp, lane i holding row i in d[]: the recursion over j is resolved
-// at compile time, so every d[] index is a constant and the row stays in
-// registers (a runtime loop of this size may be left rolled, which moves d[]
-// to local memory).  LAPACK dpotf2 order; sqrt and 1/sqrt are independent,
-// so a step costs one of them rather than a square root and a division.  A
-// non-positive pivot (or NaN) marks the column and the remaining steps run
-// on harmless values.
-template <int J>
-__device__ __forceinline__ void chol32_step(double (&d)[32], int lane, int &failcol, double &rdiag)
+// Unblocked right-looking Cholesky of a 32x32 block by one warp, lane i
+// owning row i, LAPACK dpotf2 order.  The row lives in registers in a frame
+// that rotates by one column per step (d[c] = A(i, J + c) at step J), so the
+// loop body is the same for every step: a rolled loop of a few hundred
+// instructions with compile-time register indices.  (POTRF runs once per step
+// on one SM between update tasks; the fully unrolled form is several thousand
+// instructions executed once each, paced by instruction fetch.)  The columns
+// beyond the block are skipped in groups of 8 by uniform branches.  sqrt and
+// 1/sqrt are independent, so a step costs one of them rather than a square
+// root and a division.  A non-positive pivot (or NaN) marks the column and
+// the remaining steps run on harmless values.  Column J of L goes to Ls (row-
+// major, pitch 33); returns the first failing column or -1; rdiag (lane j) =
+// 1 / L(j,j).
+__device__ __forceinline__ int chol32_rot(double (&d)[32], int lane, double &rdiag, double *Ls)
 {
-    double piv = __shfl_sync(0xffffffffu, d[J], J);
-    if (!(piv > 0.0)) {   // LAPACK dpotf2: ajj <= 0 or NaN stops the factorization
-        if (failcol < 0) failcol = J;
-        piv = 1.0;
-    }
-    const double s = sqrt(piv);
-    const double rs = rsqrt(piv);
-    const double lij = (lane == J) ? s : d[J] * rs;
-    if (lane >= J) d[J] = lij;
-    if (lane == J) rdiag = rs;
+    int failcol = -1;
+#pragma unroll 1
+    for (int J = 0; J < 32; ++J) {
+        double piv = __shfl_sync(0xffffffffu, d[0], J);
+        if (!(piv > 0.0)) {   // LAPACK dpotf2: ajj <= 0 or NaN stops the factorization
+            if (failcol < 0) failcol = J;
+            piv = 1.0;
+        }
+        const double sq = sqrt(piv);
+        const double rs = rsqrt(piv);
+        const double lij = (lane == J) ? sq : d[0] * rs;
+        if (lane >= J) Ls[lane * 33 + J] = lij;
+        if (lane == J) rdiag = rs;
 #pragma unroll
-    for (int c = J + 1; c < 32; ++c) {
-        const double lcj = __shfl_sync(0xffffffffu, lij, c);
-        if (lane >= c) d[c] -= lij * lcj;
+        for (int c0 = 1; c0 < 32; c0 += 8) {
+            if (J + c0 < 32) {
+#pragma unroll
+                for (int c = c0; c < c0 + 8 && c < 32; ++c) {
+                    const double lcj = __shfl_sync(0xffffffffu, lij, (J + c) & 31);
+                    if (lane >= J + c) d[c] -= lij * lcj;
+                }
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < 31; ++c) d[c] = d[c + 1];
     }
-    if constexpr (J + 1 < 32) chol32_step<J + 1>(d, lane, failcol, rdiag);
+    return failcol;
+}
+
+// Inverse of the lower 32x32 block L (Ls, from chol32_rot) by one warp, lane
+// c forming column c by a forward sweep in the same rotating frame
+// (b[q] = row j + q of the right-hand side at step j): x_j = b_j / L(j,j),
+// then b_i -= L(i,j) x_j below.  out(j, c, x) receives Dinv(j, c).
+template <class Out>
+__device__ __forceinline__ void inv32_rot(const double *Ls, int lane, double rdiag, Out out)
+{
+    double b[32];
+#pragma unroll
+    for (int q = 0; q < 32; ++q) b[q] = (q == lane) ? 1.0 : 0.0;
+#pragma unroll 1
+    for (int j = 0; j < 32; ++j) {
+        const double x = b[0] * __shfl_sync(0xffffffffu, rdiag, j);
+        out(j, lane, x);
+#pragma unroll
+        for (int c0 = 1; c0 < 32; c0 += 8) {
+            if (j + c0 < 32) {
+#pragma unroll
+                for (int c = c0; c < c0 + 8 && c < 32; ++c) b[c] -= Ls[min(j + c, 31) * 33 + j] * x;
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 31; ++q) b[q] = b[q + 1];
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -375,8 +416,8 @@ __device__ __forceinline__ void chol32_step(double (&d)[32], int lane, int &fail
 // blocks (src/zpotrf_L.jdf:194-206 computes the factor with
 // LAPACKE_dpotrf_work; the inverses feed the TRSM jobs).
 // Blocked right-looking with 32-column panels: one warp factors the 32x32
-// diagonal block with shuffles, all warps form the panel, the trailing
-// update runs on the FP64 tensor cores.
+// diagonal block in shared memory and inverts it, the panel solve and the
+// trailing update run on the FP64 tensor cores.
 // ---------------------------------------------------------------------------
 __device__ void potrf_task(const PotrfArgs &a, SmemCtl *ctl, double *ring, int k)
 {
@@ -418,11 +459,13 @@ __device__ void potrf_task(const PotrfArgs &a, SmemCtl *ctl, double *ring, int k
             double d[32];
 #pragma unroll
             for (int c = 0; c < 32; ++c) d[c] = (c <= lane) ? __ldcg(T + (int64_t)(p0 + c) * nbi + p0 + lane) : 0.0;
+#pragma unroll
+            for (int c = 0; c < 32; ++c) Ls[lane * 33 + c] = 0.0;    // upper part stays zero
             if (a.ptrace) { double z = 0; for (int c = 0; c < 32; ++c) z += d[c]; if (z == 12345.0) colb[0] = z; }
             sub(0);
-            int failcol = -1;
             double rdiag = 0.0;      // lane j: 1 / L(j,j)
-            chol32_step<0>(d, lane, failcol, rdiag);
+            const int failcol = chol32_rot(d, lane, rdiag, Ls);
+            __syncwarp();
             sub(1);
             if (failcol >= 0) {
                 if (lane == 0) {
@@ -432,40 +475,18 @@ __device__ void potrf_task(const PotrfArgs &a, SmemCtl *ctl, double *ring, int k
                     atomicExch(a.abort_flag, 1);
                 }
             } else {
-#pragma unroll
-                for (int c = 0; c < 32; ++c) {
-                    if (c <= lane) T[(int64_t)(p0 + c) * nbi + p0 + lane] = d[c];
-                    Ls[lane * 33 + c] = (c <= lane) ? d[c] : 0.0;
-                }
-                __syncwarp();
+#pragma unroll 8
+                for (int c = 0; c < 32; ++c)
+                    if (c <= lane) T[(int64_t)(p0 + c) * nbi + p0 + lane] = Ls[lane * 33 + c];
                 sub(2);
-                // inverse of the 32x32 lower block: lane c forms column c by
-                // forward substitution, multiplying by the reciprocal pivots
-                // of the factorization, four partial sums per row
+                // inverse of the 32x32 lower block (Dv row-major: Dv[i*33 + c] =
+                // Dinv(i, c)) and its place in the 128-block inverse W
                 const int b = p0 / BLK, q0 = p0 % BLK;
                 double *Wb = Wk + (int64_t)b * BLK * BLK;
-                double x[32];
-#pragma unroll
-                for (int i = 0; i < 32; ++i) {
-                    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-#pragma unroll
-                    for (int l = 0; l + 3 < i; l += 4) {
-                        s0 = fma(Ls[i * 33 + l], x[l], s0);
-                        s1 = fma(Ls[i * 33 + l + 1], x[l + 1], s1);
-                        s2 = fma(Ls[i * 33 + l + 2], x[l + 2], s2);
-                        s3 = fma(Ls[i * 33 + l + 3], x[l + 3], s3);
-                    }
-#pragma unroll
-                    for (int l = i & ~3; l < i; ++l) s0 = fma(Ls[i * 33 + l], x[l], s0);
-                    const double ri = __shfl_sync(0xffffffffu, rdiag, i);
-                    const double sum = (s0 + s1) + (s2 + s3);
-                    x[i] = (i < lane) ? 0.0 : ((i == lane) ? ri : -sum * ri);
-                }
-#pragma unroll
-                for (int i = 0; i < 32; ++i) {
-                    Dv[i * 33 + lane] = x[i];
-                    Wb[(int64_t)(q0 + lane) * BLK + q0 + i] = x[i];
-                }
+                inv32_rot(Ls, lane, rdiag, [&](int i, int c, double x) {
+                    Dv[i * 33 + c] = x;
+                    Wb[(int64_t)(q0 + c) * BLK + q0 + i] = x;
+                });
                 if (a.ptrace) { __syncwarp(); if (Dv[lane * 33] == 12345.0) colb[1] = 0; }
                 sub(3);
             }
@@ -474,21 +495,46 @@ __device__ void potrf_task(const PotrfArgs &a, SmemCtl *ctl, double *ring, int k
         phase(0);
         if (ctl->fail) return;
 
-        // (b) panel below the block: X = P * Dinv^T  (P = T[p0+32:, p0:p0+32])
+        // (b) panel below the block: X = P * Dinv^T (P = T[p0+32:, p0:p0+32])
+        // on the FP64 tensor cores, one 32-row block of X per warp and turn
         const int R = nbi - p0 - 32;
-        for (int rr = tid; rr < R; rr += NCONS) {
-            const int r = p0 + 32 + rr;
-            double av[32];
+        for (int rb = warp; rb < R / 32; rb += NCONS / 32) {
+            const int rr0 = rb * 32, r0 = p0 + 32 + rr0;
+            double af[8][2][2];
 #pragma unroll
-            for (int l = 0; l < 32; ++l) av[l] = __ldcg(T + (int64_t)(p0 + l) * nbi + r);
+            for (int ks = 0; ks < 8; ++ks)
 #pragma unroll
-            for (int c = 0; c < 32; ++c) {
-                double x = 0.0;
+                for (int mi = 0; mi < 2; ++mi) {
+                    const double *col = T + (int64_t)(p0 + ks * 4 + t) * nbi + r0 + mi * 16 + g;
+                    af[ks][mi][0] = __ldcg(col);
+                    af[ks][mi][1] = __ldcg(col + 8);
+                }
+            double acc[2][4][4];
 #pragma unroll
-                for (int l = 0; l <= c; ++l) x += av[l] * Dv[c * 33 + l];
-                T[(int64_t)(p0 + c) * nbi + r] = x;
-                Xs[c * XP + rr] = x;
-            }
+            for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) acc[mi][ni][q] = 0.0;
+#pragma unroll
+            for (int ks = 0; ks < 8; ++ks)
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni) {
+                    const double bf = Dv[(ni * 8 + g) * 33 + ks * 4 + t];   // Dinv^T(l, c) = Dinv(c, l)
+#pragma unroll
+                    for (int mi = 0; mi < 2; ++mi) dmma_16x8x4(acc[mi][ni], af[ks][mi][0], af[ks][mi][1], bf);
+                }
+#pragma unroll
+            for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const int rr = rr0 + mi * 16 + g + ((q & 2) ? 8 : 0);
+                        const int c = ni * 8 + 2 * t + (q & 1);
+                        T[(int64_t)(p0 + c) * nbi + p0 + 32 + rr] = acc[mi][ni][q];
+                        Xs[c * XP + rr] = acc[mi][ni][q];
+                    }
         }
         named_bar_sync(1, NCONS);
         phase(1);
