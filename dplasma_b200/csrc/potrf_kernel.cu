@@ -244,15 +244,6 @@ __device__ void producer_warp(const PotrfArgs &a, SmemCtl *ctl, double *ring, co
             prev_signal = jb.signal;
         }
         if (!pipe_ok) break;
-        if (MIXED && ty == T_TRSM) {
-            // the consumers re-lay the strip out through the ring after its
-            // jobs: no new FP64 stage may land before they are done
-            if (!warp_mbar_wait(&ctl->tempty[slot], round & 1, a.pipe_limit_ns)) {
-                if (lane == 0) report(a, ST_MBAR_TIMEOUT, 2, task_it, tk);
-                pipe_ok = false;
-                break;
-            }
-        }
     }
     if (!pipe_ok) {
         // Error path: tell the consumers to stop, then let the copies already
@@ -337,6 +328,40 @@ __device__ __forceinline__ bool consume_job(const PotrfArgs &a, SmemCtl *ctl, co
                     atomicAdd(p, -acc[mi][ni][q]);
                 }
             }
+    if (MIXED && jb.p16) {
+        // 16-bit copy of the solved block for the tensor-core updates: the
+        // value times its row scale (a power of two, exact) rounded to bf16 or
+        // fp16, in the split form hi = fp16(x) and lo = fp16(x - hi); two
+        // adjacent columns per 32-bit store
+        const int pitch = a.nbi;
+        unsigned short *Plo = jb.p16 + (int64_t)a.p16_rows * pitch;
+#pragma unroll
+        for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const int r = wm * 64 + mi * 16 + g + 8 * h;
+                    const int c = wn * 32 + ni * 8 + 2 * t;
+                    uint32_t hw = 0, lw = 0;
+#pragma unroll
+                    for (int e = 0; e < 2; ++e) {
+                        const double xs = acc[mi][ni][2 * h + e] * (double)jb.p16_scale;
+                        unsigned short hv, lv = 0;
+                        if (a.p16_fmt) {
+                            hv = __bfloat16_as_ushort(__float2bfloat16_rn((float)xs));
+                        } else {
+                            const __half hh = __float2half_rn((float)xs);
+                            hv = __half_as_ushort(hh);
+                            if (a.mx_split) lv = __half_as_ushort(__float2half_rn((float)(xs - (double)__half2float(hh))));
+                        }
+                        hw |= (uint32_t)hv << (16 * e);
+                        lw |= (uint32_t)lv << (16 * e);
+                    }
+                    *reinterpret_cast<uint32_t *>(jb.p16 + (int64_t)r * pitch + c) = hw;
+                    if (a.mx_split) *reinterpret_cast<uint32_t *>(Plo + (int64_t)r * pitch + c) = lw;
+                }
+    }
     __threadfence();   // this thread's reductions are performed before any later release
     return true;
 }
@@ -643,51 +668,6 @@ __global__ void p16_scale_kernel(const double *A, int mt, int nbi, float target,
 }
 
 // ---------------------------------------------------------------------------
-// mixed precision: 16-bit copy of a finished TRSM strip.  The strip (128 rows
-// of tile (m,k), FP64, column-major) is multiplied by its row scale, rounded
-// to bf16/fp16 (split form: hi + lo fp16) and stored K-major (row r holds
-// the nbi values of row r), the operand layout of the tcgen05 update.  All
-// 256 consumer threads; the FP64 ring is scratch.
-// ---------------------------------------------------------------------------
-__device__ void emit_p16_strip(const PotrfArgs &a, double *ring, int m, int k, int bi)
-{
-    const int tid = threadIdx.x;
-    const int nbi = a.nbi;
-    const double *X = tile_ptr(a, m, k) + bi * BLK;     // column stride nbi
-    const float scale = a.scl[m * a.nbs + bi];
-    const int64_t tile = lower_tile_index(m, k, a.mt);
-    // transpose through shared memory, 32 columns at a time
-    double *buf = ring;                                    // 128 x 33
-    unsigned short *P = reinterpret_cast<unsigned short *>(a.P16) + (tile * nbi + bi * BLK) * (int64_t)nbi;
-    unsigned short *Plo = P + (int64_t)a.p16_rows * nbi;  // split form: lo part
-    for (int c0 = 0; c0 < nbi; c0 += 32) {
-        named_bar_sync(1, NCONS);
-        for (int e = tid; e < BLK * 32; e += NCONS) {
-            const int r = e % BLK, c = e / BLK;
-            buf[r * 33 + c] = __ldcg(X + (int64_t)(c0 + c) * nbi + r);
-        }
-        named_bar_sync(1, NCONS);
-        for (int e = tid; e < BLK * 32; e += NCONS) {
-            const int c = e % 32, r = e / 32;
-            const double xs = buf[r * 33 + c] * (double)scale;    // exact: power of two
-            unsigned short h;
-            if (a.p16_fmt) {
-                h = __bfloat16_as_ushort(__float2bfloat16_rn((float)xs));
-            } else {
-                const __half hh = __float2half_rn((float)xs);
-                h = __half_as_ushort(hh);
-                if (a.mx_split) {
-                    // split FP16 (hi + lo): lo carries the next 11 bits of xs
-                    const double rem = xs - (double)__half2float(hh);
-                    Plo[(int64_t)r * nbi + c0 + c] = __half_as_ushort(__float2half_rn((float)rem));
-                }
-            }
-            P[(int64_t)r * nbi + c0 + c] = h;
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------
 // mixed precision: one update task,
 //     C(m,n) -= sum_{j in chunk} P16(m,j) P16(n,j)^T   (scaled back)
 // Warp 4 lane 0 issues tcgen05.mma (M=128, N=256, K=16) for the two 128-row
@@ -853,7 +833,6 @@ __device__ void consumer_warps(const PotrfArgs &a, SmemCtl *ctl, double *ring)
                     if (tid == 0) mbar_arrive(&ctl->epi);
                 }
             }
-            if (MIXED && ty == T_TRSM && !named_bar_or(1, NCONS, !ok)) emit_p16_strip(a, ring, m, k, task_bi(t));
             release = (ty == T_TRSM) ? a.trsm_done + (int64_t)m * a.mt + k : a.upd_done + (int64_t)m * a.mt + n;
         }
         fence_proxy_async();

@@ -131,6 +131,10 @@ struct Job {
     int K;
     int mode;
     bool signal;   // the next job of the same task reads this job's output
+    // mixed precision, TRSM store jobs: the 16-bit copy of the block is
+    // written by the same epilogue (K-major rows of pitch nbi; null otherwise)
+    unsigned short *p16;
+    float p16_scale;
 };
 
 // The job sequence of a task (identical on producer and consumer sides).
@@ -155,6 +159,8 @@ __device__ __forceinline__ Job task_job(const PotrfArgs &a, uint64_t t, int j)
         jb.K = nbi;
         jb.mode = (m == n && bi == bj) ? J_SUB_LOWER : J_SUB;
         jb.signal = false;
+        jb.p16 = nullptr;
+        jb.p16_scale = 1.f;
     } else {
         // TRSM strip bi of tile (m,k): X = A L^{-T} (src/zpotrf_L.jdf:330-333),
         // block-left-looking: jobs  [STORE p=0] [SUB p=1] [STORE p=1] ...
@@ -176,6 +182,14 @@ __device__ __forceinline__ Job task_job(const PotrfArgs &a, uint64_t t, int j)
             jb.signal = true;
         }
         jb.C = Cp; jb.ldc = nbi;
+        jb.p16 = nullptr;
+        jb.p16_scale = 1.f;
+        if (store && a.P16) {
+            // rows bi*128.. of tile (m,k), columns p*128..: P16 row (tile*nbi + row), K-major
+            const int64_t row0 = lower_tile_index(m, k, a.mt) * nbi + bi * BLK;
+            jb.p16 = reinterpret_cast<unsigned short *>(a.P16) + row0 * nbi + p * BLK;
+            jb.p16_scale = a.scl[m * a.nbs + bi];
+        }
     }
     return jb;
 }
