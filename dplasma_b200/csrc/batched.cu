@@ -30,6 +30,7 @@
 
 #include "dev_common.cuh"
 #include "internal.h"
+#include "dev_chol32.cuh"
 
 namespace db2 {
 
@@ -60,29 +61,6 @@ __device__ __forceinline__ double bt_rsqrt<double>(double x) { return rsqrt(x); 
 template <>
 __device__ __forceinline__ float bt_rsqrt<float>(float x) { return rsqrtf(x); }
 
-// 32x32 block factorization (lane i = row i), compile-time steps; rows >= jb
-// hold the identity.  Sets failcol to the first non-positive pivot.
-template <typename T, int J>
-__device__ __forceinline__ void bt_chol_step(T (&d)[32], int lane, int &failcol, T &rdiag)
-{
-    T piv = __shfl_sync(0xffffffffu, d[J], J);
-    if (!(piv > T(0))) {
-        if (failcol < 0) failcol = J;
-        piv = T(1);
-    }
-    const T s = sqrt(piv);
-    const T rs = bt_rsqrt<T>(piv);
-    const T lij = (lane == J) ? s : d[J] * rs;
-    if (lane >= J) d[J] = lij;
-    if (lane == J) rdiag = rs;
-#pragma unroll
-    for (int c = J + 1; c < 32; ++c) {
-        const T lcj = __shfl_sync(0xffffffffu, lij, c);
-        if (lane >= c) d[c] -= lij * lcj;
-    }
-    if constexpr (J + 1 < 32) bt_chol_step<T, J + 1>(d, lane, failcol, rdiag);
-}
-
 // Diagonal block j0 (jb <= 32 columns) of one problem by warp 0: factor in
 // registers, write L back, accumulate log det, form the inverse into Dinv.
 // Returns the failing column within the block or -1.
@@ -94,35 +72,19 @@ __device__ int bt_diag(T *A, int lda, int j0, int jb, T *Dinv, T *Ls, double &ld
     for (int c = 0; c < 32; ++c)
         d[c] = (lane < jb && c < jb) ? ((c <= lane) ? A[(int64_t)(j0 + c) * lda + j0 + lane] : T(0))
                                      : (c == lane ? T(1) : T(0));
-    int failcol = -1;
     T rdiag = T(0);
-    bt_chol_step<T, 0>(d, lane, failcol, rdiag);
+    int failcol = chol32_blk<T>(d, lane, rdiag, Ls);     // Ls: blocked copy of L ([8][32][4])
     if (failcol >= jb) failcol = -1;      // padding rows are the identity
     if (failcol >= 0) return failcol;
-    if (lane < jb) {
-#pragma unroll
-        for (int c = 0; c < 32; ++c)
-            if (c <= lane && c < jb) A[(int64_t)(j0 + c) * lda + j0 + lane] = d[c];
-        ld_acc -= 2.0 * log((double)rdiag);   // rdiag = 1 / L(i,i); no d[lane]: keeps d in registers
-    }
-#pragma unroll
-    for (int c = 0; c < 32; ++c) Ls[lane * BT_PP + c] = (c <= lane) ? d[c] : T(0);
     __syncwarp();
-    T x[32];
-#pragma unroll
-    for (int i = 0; i < 32; ++i) {
-        T s0 = T(0), s1 = T(0);
-#pragma unroll
-        for (int l = 0; l + 1 < i; l += 2) {
-            s0 = fma(Ls[i * BT_PP + l], x[l], s0);
-            s1 = fma(Ls[i * BT_PP + l + 1], x[l + 1], s1);
-        }
-        if (i & 1) s0 = fma(Ls[i * BT_PP + i - 1], x[i - 1], s0);
-        const T ri = __shfl_sync(0xffffffffu, rdiag, i);
-        x[i] = (i < lane) ? T(0) : ((i == lane) ? ri : -(s0 + s1) * ri);
+    if (lane < jb) {
+#pragma unroll 8
+        for (int c = 0; c < 32; ++c)
+            if (c <= lane && c < jb) A[(int64_t)(j0 + c) * lda + j0 + lane] = Ls[(c >> 2) * 128 + lane * 4 + (c & 3)];
+        ld_acc -= 2.0 * log((double)rdiag);   // rdiag = 1 / L(i,i)
     }
-#pragma unroll
-    for (int i = 0; i < 32; ++i) Dinv[i * BT_PP + lane] = x[i];   // Dinv[i][c], lower
+    inv32_blk<T>(Ls, lane, rdiag, [&](int i, int c, T x) { Dinv[i * BT_PP + c] = x; });   // Dinv[i][c], lower
+    __syncwarp();
     return -1;
 }
 

@@ -8,6 +8,7 @@
 
 #include "internal.h"
 #include "potrf_kernel.cuh"
+#include "dev_chol32.cuh"
 #include "dev_trtri.cuh"
 #include "dev_tcgen05.cuh"
 #include <cuda_bf16.h>
@@ -366,149 +367,6 @@ __device__ __forceinline__ bool consume_job(const PotrfArgs &a, SmemCtl *ctl, co
     return true;
 }
 
-// Cholesky of a 32x32 block by one warp, lane i owning row i, in steps of
-// four columns.  The row lives in registers in a frame that rotates by four
-// columns per step (d[c] = A(i, J + c) at step J), so the rolled loop body
-// uses compile-time register indices (POTRF runs once per step on one SM
-// between update tasks; a fully unrolled form is thousands of instructions
-// executed once each, paced by instruction fetch).  Per step: every lane
-// gathers the 4x4 diagonal block by shuffles and factors it redundantly, forms
-// its row of the 4-column panel, publishes it in the blocked copy Lb
-// ([8][32][4]: Lb[J/4][i][k] = L(i, J+k)), and applies the rank-4 update to
-// its remaining columns, reading the panel rows back from Lb with 16-byte
-// broadcasts.  Every element receives the operations of LAPACK dpotf2's
-// right-looking order (the same subtractions in the same order).  sqrt and
-// 1/sqrt are independent, so a pivot costs one of them rather than a square
-// root and a division.  A non-positive pivot (or NaN) marks the column and
-// the remaining steps run on harmless values.  Returns the first failing
-// column or -1; rdiag (lane j) = 1 / L(j,j).
-__device__ __forceinline__ int chol32_blk(double (&d)[32], int lane, double &rdiag, double *Lb)
-{
-    int failcol = -1;
-#pragma unroll 1
-    for (int J = 0; J < 32; J += 4) {
-        double a[4][4], l[4][4], rr[4];
-#pragma unroll
-        for (int r = 0; r < 4; ++r)
-#pragma unroll
-            for (int c = 0; c <= r; ++c) a[r][c] = __shfl_sync(0xffffffffu, d[c], J + r);
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            double piv = a[j][j];
-            if (!(piv > 0.0)) {   // LAPACK dpotf2: ajj <= 0 or NaN stops the factorization
-                if (failcol < 0) failcol = J + j;
-                piv = 1.0;
-            }
-            l[j][j] = sqrt(piv);
-            rr[j] = rsqrt(piv);
-#pragma unroll
-            for (int r = j + 1; r < 4; ++r) l[r][j] = a[r][j] * rr[j];
-#pragma unroll
-            for (int c = j + 1; c < 4; ++c)
-#pragma unroll
-                for (int r = c; r < 4; ++r) a[r][c] -= l[r][j] * l[c][j];
-        }
-        // this lane's row of the 4-column panel
-        const int rb = lane - J;
-        double x[4];
-        {
-            double y1 = d[1], y2 = d[2], y3 = d[3];
-            x[0] = d[0] * rr[0];
-            y1 -= x[0] * l[1][0];
-            y2 -= x[0] * l[2][0];
-            y3 -= x[0] * l[3][0];
-            x[1] = y1 * rr[1];
-            y2 -= x[1] * l[2][1];
-            y3 -= x[1] * l[3][1];
-            x[2] = y2 * rr[2];
-            y3 -= x[2] * l[3][2];
-            x[3] = y3 * rr[3];
-        }
-        if (rb < 0) {
-#pragma unroll
-            for (int c = 0; c < 4; ++c) x[c] = 0.0;            // above the block: upper part of L
-        }
-#pragma unroll
-        for (int r = 0; r < 4; ++r)
-            if (rb == r) {
-#pragma unroll
-                for (int c = 0; c < 4; ++c) x[c] = (c <= r) ? l[r][c] : 0.0;
-                rdiag = rr[r];
-            }
-        double2 *dst = reinterpret_cast<double2 *>(Lb + ((J >> 2) * 32 + lane) * 4);
-        dst[0] = make_double2(x[0], x[1]);
-        dst[1] = make_double2(x[2], x[3]);
-        __syncwarp();
-        // rank-4 update of the columns J+4.. (the values of lanes above the
-        // diagonal are never read)
-        const double2 *Lr = reinterpret_cast<const double2 *>(Lb + (J >> 2) * 128);
-#pragma unroll
-        for (int c0 = 4; c0 < 32; c0 += 4) {
-            if (J + c0 < 32) {
-#pragma unroll
-                for (int c = c0; c < c0 + 4; ++c) {
-                    const double2 p = Lr[(J + c) * 2], q = Lr[(J + c) * 2 + 1];
-                    d[c] -= x[0] * p.x;
-                    d[c] -= x[1] * p.y;
-                    d[c] -= x[2] * q.x;
-                    d[c] -= x[3] * q.y;
-                }
-            }
-        }
-#pragma unroll
-        for (int c = 0; c < 28; ++c) d[c] = d[c + 4];
-    }
-    return failcol;
-}
-
-// Inverse of the lower 32x32 block L (Lb, from chol32_blk) by one warp, lane
-// c forming column c by a forward sweep in steps of four rows, in the same
-// rotating frame (b[q] = row j + q of the right-hand side at step j):
-// x_j = b_j / L(j,j), then b_i -= L(i,j) x_j below, in the order of the
-// row-by-row sweep.  out(j, c, x) receives Dinv(j, c).
-template <class Out>
-__device__ __forceinline__ void inv32_blk(const double *Lb, int lane, double rdiag, Out out)
-{
-    double b[32];
-#pragma unroll
-    for (int q = 0; q < 32; ++q) b[q] = (q == lane) ? 1.0 : 0.0;
-#pragma unroll 1
-    for (int j = 0; j < 32; j += 4) {
-        const double *Lk = Lb + (j >> 2) * 128;
-        const double l10 = Lk[(j + 1) * 4], l20 = Lk[(j + 2) * 4], l21 = Lk[(j + 2) * 4 + 1];
-        const double l30 = Lk[(j + 3) * 4], l31 = Lk[(j + 3) * 4 + 1], l32 = Lk[(j + 3) * 4 + 2];
-        double x[4];
-        x[0] = b[0] * __shfl_sync(0xffffffffu, rdiag, j);
-        b[1] -= l10 * x[0];
-        b[2] -= l20 * x[0];
-        b[3] -= l30 * x[0];
-        x[1] = b[1] * __shfl_sync(0xffffffffu, rdiag, j + 1);
-        b[2] -= l21 * x[1];
-        b[3] -= l31 * x[1];
-        x[2] = b[2] * __shfl_sync(0xffffffffu, rdiag, j + 2);
-        b[3] -= l32 * x[2];
-        x[3] = b[3] * __shfl_sync(0xffffffffu, rdiag, j + 3);
-#pragma unroll
-        for (int r = 0; r < 4; ++r) out(j + r, lane, x[r]);
-        const double2 *Lr = reinterpret_cast<const double2 *>(Lk);
-#pragma unroll
-        for (int c0 = 4; c0 < 32; c0 += 4) {
-            if (j + c0 < 32) {
-#pragma unroll
-                for (int c = c0; c < c0 + 4; ++c) {
-                    const double2 p = Lr[(j + c) * 2], q = Lr[(j + c) * 2 + 1];
-                    b[c] -= p.x * x[0];
-                    b[c] -= p.y * x[1];
-                    b[c] -= q.x * x[2];
-                    b[c] -= q.y * x[3];
-                }
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < 28; ++q) b[q] = b[q + 4];
-    }
-}
-
 // ---------------------------------------------------------------------------
 // consumers: POTRF(k) of one diagonal tile + inverses of its 128x128 diagonal
 // blocks (src/zpotrf_L.jdf:194-206 computes the factor with
@@ -561,7 +419,7 @@ __device__ void potrf_task(const PotrfArgs &a, SmemCtl *ctl, double *ring, int k
             if (a.ptrace) { double z = 0; for (int c = 0; c < 32; ++c) z += d[c]; if (z == 12345.0) colb[0] = z; }
             sub(0);
             double rdiag = 0.0;      // lane j: 1 / L(j,j)
-            const int failcol = chol32_blk(d, lane, rdiag, Lb);
+            const int failcol = chol32_blk<double>(d, lane, rdiag, Lb);
             __syncwarp();
             sub(1);
             if (failcol >= 0) {
@@ -580,7 +438,7 @@ __device__ void potrf_task(const PotrfArgs &a, SmemCtl *ctl, double *ring, int k
                 // Dinv(i, c)) and its place in the 128-block inverse W
                 const int b = p0 / BLK, q0 = p0 % BLK;
                 double *Wb = Wk + (int64_t)b * BLK * BLK;
-                inv32_blk(Lb, lane, rdiag, [&](int i, int c, double x) {
+                inv32_blk<double>(Lb, lane, rdiag, [&](int i, int c, double x) {
                     Dv[i * 33 + c] = x;
                     Wb[(int64_t)(q0 + c) * BLK + q0 + i] = x;
                 });
