@@ -212,6 +212,61 @@ __device__ int bt_factor(T *A, int n, int lda, T *Dinv, T *Ls, T *P, int *sflag,
         // panel rows below: L = A D^-T, to global and to the shared panel
         // (rows up to the next multiple of 32 are zero-filled)
         const int m32 = (m + 31) & ~31;
+        if constexpr (sizeof(T) == 8) {
+            // FP64: X = P Dinv^T on the tensor cores, one 32-row block per warp
+            // and turn, then each lane forward-solves its row of B
+            for (int rb = warp; rb < m32 / 32; rb += NW) {
+                const int rr0 = rb * 32;
+                const int g = lane >> 2, t = lane & 3;
+                double af[8][2][2];
+#pragma unroll
+                for (int ks = 0; ks < 8; ++ks)
+#pragma unroll
+                    for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            const int rr = rr0 + mi * 16 + g + 8 * h, c = ks * 4 + t;
+                            af[ks][mi][h] = (rr < m && c < jb) ? (double)A[(int64_t)(j0 + c) * lda + o + rr] : 0.0;
+                        }
+                double acc[2][4][4];
+#pragma unroll
+                for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                    for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) acc[mi][ni][q] = 0.0;
+#pragma unroll
+                for (int ks = 0; ks < 8; ++ks)
+#pragma unroll
+                    for (int ni = 0; ni < 4; ++ni) {
+                        const double bf = (double)Dinv[(ni * 8 + g) * BT_PP + ks * 4 + t];   // Dinv^T(l, c)
+#pragma unroll
+                        for (int mi = 0; mi < 2; ++mi) dmma_16x8x4(acc[mi][ni], af[ks][mi][0], af[ks][mi][1], bf);
+                    }
+#pragma unroll
+                for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                    for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            const int rr = rr0 + mi * 16 + g + ((q & 2) ? 8 : 0);
+                            const int c = ni * 8 + 2 * t + (q & 1);
+                            const bool in = rr < m && c < jb;
+                            if (in) A[(int64_t)(j0 + c) * lda + o + rr] = (T)acc[mi][ni][q];
+                            P[rr * BT_PP + c] = in ? (T)acc[mi][ni][q] : T(0);
+                        }
+                __syncwarp();
+                const int rr = rr0 + lane;
+                if (B && rr < m) {
+                    for (int col = 0; col < nrhs; ++col) {
+                        T acc1 = T(0);
+#pragma unroll 8
+                        for (int c = 0; c < 32; ++c) acc1 = fma(P[rr * BT_PP + c], ybuf[col * 32 + c], acc1);
+                        B[(int64_t)col * n + o + rr] -= acc1;
+                    }
+                }
+            }
+        } else
         for (int rr = tid; rr < m32; rr += NT) {
             if (rr >= m) {
 #pragma unroll
