@@ -39,12 +39,16 @@ constexpr int AG_K = 16;      // K chunk
 constexpr int AG_P = 132;     // shared pitch
 
 // Tile sets and K ranges (block indices):
-//   ROW       tiles (rowblk, j), j < rowblk     k in [j, rowblk-1]
-//   DIAGMUL   tiles (rowblk, j), j < rowblk     k = rowblk
 //   LOWER_KGE_I   tiles i >= j                 k in [i, P-1]
 //   LOWER_JKI     tiles i >= j                 k in [j, i]
 //   FULL_KGE_MAX  all tiles                    k in [max(i,j), P-1]
-enum : int { AG_ROW = 0, AG_LOWER_KGE_I = 1, AG_LOWER_JKI = 2, AG_FULL_KGE_MAX = 3, AG_DIAGMUL = 4 };
+//   LVL_T, LVL_W  one level of the recursive triangular inverse: for every
+//                 diagonal block [o, o+2h) of 2h tiles, with W11 = the inverse
+//                 of its first half and W22 of its second (previous level),
+//                   LVL_T: Y21 = L21 W11     tiles (o+h+i, o+j), k in [o+j, o+h)
+//                   LVL_W: W21 = -W22 Y21    tiles (o+h+i, o+j), k in [o+h, o+h+i]
+//                 (h = rowblk; the last block's second half may be short)
+enum : int { AG_LOWER_KGE_I = 1, AG_LOWER_JKI = 2, AG_FULL_KGE_MAX = 3, AG_LVL_T = 5, AG_LVL_W = 6 };
 
 struct AgArgs {
     int mode, P, rowblk;
@@ -68,14 +72,26 @@ __global__ void __launch_bounds__(256) ag_gemm_kernel(AgArgs a)
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int g = lane >> 2, t = lane & 3;
     const int wm = warp & 1, wn = warp >> 1;
-    // tile and K range
-    int i, j, k0, k1;
+    // tile and K range; A(i, ako + k), B(bko + k, j)
+    int i, j, k0, k1, ako = 0, bko = 0;
     const int tix = blockIdx.x;
-    if (a.mode == AG_ROW || a.mode == AG_DIAGMUL) {
-        i = a.rowblk;
-        j = tix;
-        k0 = a.mode == AG_ROW ? j : i;
-        k1 = a.mode == AG_ROW ? i - 1 : i;
+    if (a.mode == AG_LVL_T || a.mode == AG_LVL_W) {
+        const int h = a.rowblk;
+        const int b = tix / (h * h), rem = tix % (h * h);
+        const int jj = rem / h, ii = rem % h;
+        const int o = b * 2 * h;
+        if (ii >= min(h, a.P - o - h)) return;   // beyond a short last block
+        i = o + h + ii;
+        j = o + jj;
+        if (a.mode == AG_LVL_T) {
+            ako = bko = o;
+            k0 = jj;
+            k1 = h - 1;
+        } else {
+            ako = bko = o + h;
+            k0 = 0;
+            k1 = ii;
+        }
     } else if (a.mode == AG_FULL_KGE_MAX) {
         i = tix % a.P;
         j = tix / a.P;
@@ -111,13 +127,13 @@ __global__ void __launch_bounds__(256) ag_gemm_kernel(AgArgs a)
             const int e = tid + 256 * q;
             if (!a.transA) {
                 const int r = e & 127, kk = e >> 7;
-                ra[q] = a.A[(int64_t)(kc + kk) * a.lda + i * AG_T + r];
+                ra[q] = a.A[(int64_t)(ako * AG_T + kc + kk) * a.lda + i * AG_T + r];
             } else {
                 const int kk = e & 15, r = e >> 4;
-                ra[q] = a.A[(int64_t)(i * AG_T + r) * a.lda + kc + kk];
+                ra[q] = a.A[(int64_t)(i * AG_T + r) * a.lda + ako * AG_T + kc + kk];
             }
             const int kk = e & 15, c = e >> 4;
-            rb[q] = a.B[(int64_t)(j * AG_T + c) * a.ldb + kc + kk];
+            rb[q] = a.B[(int64_t)(j * AG_T + c) * a.ldb + bko * AG_T + kc + kk];
         }
     };
     auto store = [&](int buf) {
@@ -208,7 +224,7 @@ static int ag_gemm(Context *ctx, int mode, int P, int rowblk, const double *A, i
     a.alpha = alpha;
     a.beta = beta;
     int ntile;
-    if (mode == AG_ROW || mode == AG_DIAGMUL) ntile = rowblk;
+    if (mode == AG_LVL_T || mode == AG_LVL_W) ntile = ((P + 2 * rowblk - 1) / (2 * rowblk)) * rowblk * rowblk;
     else if (mode == AG_FULL_KGE_MAX) ntile = P * P;
     else ntile = P * (P + 1) / 2;
     if (ntile <= 0) return 0;
@@ -302,6 +318,27 @@ __global__ void __launch_bounds__(256) ag_trtri_diag(const double *L, int ld, do
     }
 }
 
+// W = L^-1 into W (dense, ld), from the dense L; unit: diagonal taken as 1.
+// Recursive by levels: the 128x128 diagonal inverses, then for blocks of 2,
+// 4, 8, ... tiles W21 = -W22 (L21 W11) from the two half-blocks' inverses,
+// every block of a level in one launch (log2(P) levels of two launches).
+static int ag_inverse(Context *ctx, const double *L, double *W, double *Y, double *scr, int P, int ld, int unit)
+{
+    cudaStream_t st = ctx->stream;
+    int rc;
+    CK(cudaMemsetAsync(W, 0, (size_t)ld * ld * sizeof(double), st));
+    const size_t tsmem = (8 * 32 * 33 + 8 * 32 * 36) * sizeof(double);
+    CK(cudaFuncSetAttribute(ag_trtri_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsmem));
+    ag_trtri_diag<<<P, 256, tsmem, st>>>(L, ld, W, ld, scr, unit);
+    CK(cudaGetLastError());
+    ctx->launches++;
+    for (int h = 1; h < P; h *= 2) {
+        if ((rc = ag_gemm(ctx, AG_LVL_T, P, h, L, ld, 0, W, ld, Y, ld, 1.0, 0.0))) return rc;
+        if ((rc = ag_gemm(ctx, AG_LVL_W, P, h, W, ld, 0, Y, ld, W, ld, -1.0, 0.0))) return rc;
+    }
+    return 0;
+}
+
 // ---------------------------------------------------------------------------
 // driver: L and Lbar as device tiles (lower, padded), Abar (lower tiles) out
 // ---------------------------------------------------------------------------
@@ -321,17 +358,7 @@ int potrf_adjoint_tiles(Context *ctx, const double *Lt, double *Lbt, const Geom 
     CK(cudaGetLastError());
     ctx->launches += 2;
     // W = L^-1
-    CK(cudaMemsetAsync(W, 0, nn * sizeof(double), st));
-    const size_t tsmem = (8 * 32 * 33 + 8 * 32 * 36) * sizeof(double);
-    CK(cudaFuncSetAttribute(ag_trtri_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsmem));
-    ag_trtri_diag<<<P, 256, tsmem, st>>>(L, ld, W, ld, scr, 0);
-    CK(cudaGetLastError());
-    ctx->launches++;
-    for (int i = 1; i < P; ++i) {
-        // T_ij = sum_{k=j}^{i-1} L_ik W_kj into Y(i, j), then W_ij = -W_ii T_ij
-        if ((rc = ag_gemm(ctx, AG_ROW, P, i, L, ld, 0, W, ld, Y, ld, 1.0, 0.0))) return rc;
-        if ((rc = ag_gemm(ctx, AG_DIAGMUL, P, i, W, ld, 0, Y, ld, W, ld, -1.0, 0.0))) return rc;
-    }
+    if ((rc = ag_inverse(ctx, L, W, Y, scr, P, ld, 0))) return rc;
     // Y = Phi(L^T Lbar), lower tiles, k >= i
     if ((rc = ag_gemm(ctx, AG_LOWER_KGE_I, P, 0, L, ld, 1, Z, ld, Y, ld, 1.0, 0.0))) return rc;
     ag_phi<<<P, 256, 0, st>>>(Y, ld, P);
@@ -360,24 +387,6 @@ __global__ void ag_zero_pivot(const double *L, int ld, int n_valid_rows, const i
         const int ip = rowmap ? rowmap[i] : i;
         if (L[(int64_t)ip * ld + ip] == 0.0) atomicMin(info, i + 1);
     }
-}
-
-// W = L^-1 into W (dense, ld), from the dense L; unit: diagonal taken as 1
-static int ag_inverse(Context *ctx, const double *L, double *W, double *Y, double *scr, int P, int ld, int unit)
-{
-    cudaStream_t st = ctx->stream;
-    int rc;
-    CK(cudaMemsetAsync(W, 0, (size_t)ld * ld * sizeof(double), st));
-    const size_t tsmem = (8 * 32 * 33 + 8 * 32 * 36) * sizeof(double);
-    CK(cudaFuncSetAttribute(ag_trtri_diag, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsmem));
-    ag_trtri_diag<<<P, 256, tsmem, st>>>(L, ld, W, ld, scr, unit);
-    CK(cudaGetLastError());
-    ctx->launches++;
-    for (int i = 1; i < P; ++i) {
-        if ((rc = ag_gemm(ctx, AG_ROW, P, i, L, ld, 0, W, ld, Y, ld, 1.0, 0.0))) return rc;
-        if ((rc = ag_gemm(ctx, AG_DIAGMUL, P, i, W, ld, 0, Y, ld, W, ld, -1.0, 0.0))) return rc;
-    }
-    return 0;
 }
 
 // op: 0 trtri (L -> L^-1), 1 lauum (L -> L^T L), 2 potri (L -> (L L^T)^-1);
