@@ -258,6 +258,21 @@ def bench_adjoint(torch):
     torch.cuda.synchronize()
     t_fb = e0.elapsed_time(e1)
     flops_f = n ** 3 / 3.0 + 2.0 * n * n
+    # the general Cholesky adjoint (dplasma_dpotrf_adjoint) for a dense lower Lbar
+    Kc = dag.se_kernel(x, torch.tensor(0.2, dtype=torch.float64, device="cuda")).requires_grad_(True)
+    Gbar = torch.randn(n, n, dtype=torch.float64, device="cuda", generator=g).tril_()
+    Lc = dag.cholesky(Kc)
+    Lc.backward(Gbar)                           # warm-up
+    torch.cuda.synchronize()
+    Kc.grad = None
+    Lc = dag.cholesky(Kc)
+    torch.cuda.synchronize()
+    e0.record()
+    Lc.backward(Gbar)
+    e1.record()
+    torch.cuda.synchronize()
+    t_adj = e0.elapsed_time(e1)
+    del Kc, Gbar, Lc
     # the batch: 1024 problems, n uniform in [64, 256], shared lengthscale
     rng = np.random.default_rng(13)
     sizes = [int(v) for v in rng.integers(64, 257, 1024)]
@@ -287,8 +302,10 @@ def bench_adjoint(torch):
     return {"n": n, "forward_ms": t_f, "forward_backward_ms": t_fb, "backward_over_forward": t_fb / t_f - 1.0,
             "batch": batch,
             "forward_tflops": flops_f / (t_f * 1e-3) / 1e12, "value": float(v), "dlengthscale": float(ls.grad),
-            "note": "backward = dplasma_dpotrf_adjoint for K^-1 (about 1.3 N^3 FP64 tensor-core flops) "
-                    "and rank-1 terms; forward = dplasma_dpotrf + dplasma_dpotrs"}
+            "cholesky_adjoint_ms": t_adj,
+            "note": "GP backward = dplasma_dpotri for K^-1 (the log-det adjoint; 2/3 N^3 FP64 tensor-core flops) "
+                    "and rank-1 terms; forward = dplasma_dpotrf + dplasma_dpotrs; cholesky_adjoint_ms = "
+                    "dplasma_dpotrf_adjoint for a dense lower Lbar (autograd.cholesky backward, about 1.3 N^3 flops)"}
 
 
 def run_gpu(args):

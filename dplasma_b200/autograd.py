@@ -12,9 +12,9 @@
   - n/2 log 2 pi`` for a Gaussian-process kernel matrix K and targets y
   (vector or n x m); forward is one factorization and one solve
   (``dplasma_dpotrf`` + ``dplasma_dpotrs``), backward
-  ``dK = 1/2 alpha alpha^T - 1/2 K^-1`` with ``K^-1`` from
-  ``dplasma_dpotrf_adjoint`` applied to the log-determinant adjoint
-  ``Lbar = diag(2 / L(i,i))``, and ``dy = -alpha``.  Gradients with respect to
+  ``dK = 1/2 alpha alpha^T - 1/2 K^-1`` with ``K^-1`` -- the Cholesky adjoint
+  of the log-determinant (``Lbar = diag(2 / L(i,i))``) -- formed from the
+  factor by ``dplasma_dpotri``, and ``dy = -alpha``.  Gradients with respect to
   parameters of K (a lengthscale, ...) follow by torch's own chain rule.
 
 Matrices cross the C ABI as LAPACK-storage device descriptors: a row-major
@@ -80,6 +80,19 @@ def _adjoint(Lrow: torch.Tensor, Lbar: torch.Tensor) -> torch.Tensor:
     return up + torch.triu(Bc, 1).t()
 
 
+def _inverse_from_factor(Lrow: torch.Tensor) -> torch.Tensor:
+    """K^-1 (symmetric, row-major) from the lower factor L of K."""
+    n = Lrow.shape[0]
+    ctx = context(Lrow.device)
+    buf = Lrow.t().contiguous()              # column-major L
+    torch_ready(buf)
+    rc = ctx.dpotri(Lower, _lapack_desc(buf, n))
+    if rc != 0:
+        raise RuntimeError(f"dplasma_dpotri: {rc} {ctx.last_error()}")
+    up = torch.triu(buf)                     # column-major lower part = row-major upper
+    return up + torch.triu(buf, 1).t()
+
+
 class _Cholesky(torch.autograd.Function):
     @staticmethod
     def forward(ctx_, A):
@@ -128,8 +141,8 @@ class _GPLogML(torch.autograd.Function):
     def backward(ctx_, g):
         L, alpha = ctx_.saved_tensors
         m = alpha.shape[1]
-        # K^-1 from the log-determinant adjoint: Lbar = diag(2 / L(i,i))
-        Kinv = _adjoint(L, torch.diag(2.0 / torch.diagonal(L)))
+        # K^-1, the adjoint of log det K through the factor, by dplasma_dpotri
+        Kinv = _inverse_from_factor(L)
         dK = g * (0.5 * alpha @ alpha.t() - 0.5 * m * Kinv)
         dy = -g * alpha
         if ctx_.ydim == 1:

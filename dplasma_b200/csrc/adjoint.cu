@@ -436,8 +436,8 @@ int inverse_tiles(Context *ctx, double *Lt, const Geom &g, int op, int unit, int
     }
     double *out = W;
     if (op != 0) {
-        // src^T src, all tiles (k >= max(i, j)); the lower part is the result
-        if ((rc = ag_gemm(ctx, AG_FULL_KGE_MAX, P, 0, src, ld, 1, src, ld, Y, ld, 1.0, 0.0))) return rc;
+        // src^T src, lower tiles only (k >= i >= j): the result is symmetric
+        if ((rc = ag_gemm(ctx, AG_LOWER_KGE_I, P, 0, src, ld, 1, src, ld, Y, ld, 1.0, 0.0))) return rc;
         out = Y;
     }
     ag_dense_to_tiles<<<tg, 256, 0, st>>>(out, ld, g.mt, g.nbi, Lt);
