@@ -64,6 +64,92 @@ __global__ void max_kernel(const double *v, int n, double *out)
     if (threadIdx.x == 0) *out = sm[0];
 }
 
+// L = A (the lower tiles) and, in the same pass, the absolute row sums of
+// the symmetric matrix (rows, caller numbering): one CTA per tile, warp w
+// streams columns w, w+8, ... four at a time (32 loads in flight per lane);
+// element (r, c) of tile (m, n) adds to row m*nb + r and, strictly below
+// the diagonal, to row n*nb + c (the mirrored upper part).  Column sums are
+// reduced in the warp, row sums across warps in shared memory.  nbi = 32 KR.
+template <int KR>
+__global__ void __launch_bounds__(256) copy_rowsum_sym_kernel(const double *__restrict__ A, double *__restrict__ L,
+                                                              int mt, int nb, int n, double *rows)
+{
+    constexpr int nbi = KR * 32;
+    const int64_t idx = blockIdx.x;
+    int lo = 0, hi = mt - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) / 2;
+        int64_t start = (int64_t)mid * mt - ((int64_t)mid * (mid - 1)) / 2;
+        if (start <= idx) lo = mid; else hi = mid - 1;
+    }
+    const int tn = lo;
+    const int tm = tn + (int)(idx - ((int64_t)tn * mt - ((int64_t)tn * (tn - 1)) / 2));
+    const double *T = A + idx * (int64_t)nbi * nbi;
+    double *D = L + idx * (int64_t)nbi * nbi;
+    const int rows_m = (tm == mt - 1) ? n - tm * nb : nb;
+    const int rows_n = (tn == mt - 1) ? n - tn * nb : nb;
+    const bool diag = (tm == tn);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __shared__ double red[8][nbi];
+    double rs[KR];
+#pragma unroll
+    for (int k = 0; k < KR; ++k) rs[k] = 0.0;
+    for (int c0 = warp * 4; c0 < nbi; c0 += 32) {
+        double v[4][KR];
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+            for (int k = 0; k < KR; ++k) v[q][k] = __ldcs(T + (int64_t)(c0 + q) * nbi + lane + 32 * k);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int c = c0 + q;
+            double cs = 0.0;
+#pragma unroll
+            for (int k = 0; k < KR; ++k) {
+                const int r = lane + 32 * k;
+                __stcs(D + (int64_t)c * nbi + r, v[q][k]);
+                const double x = fabs(v[q][k]);
+                const bool in = r < rows_m && c < rows_n;
+                if (in && (!diag || c <= r)) rs[k] += x;
+                if (in && (!diag || r > c)) cs += x;
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) cs += __shfl_xor_sync(0xffffffffu, cs, o);
+            if (lane == 0 && c < rows_n && cs != 0.0) atomicAdd(rows + (int64_t)tn * nb + c, cs);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < KR; ++k) red[warp][lane + 32 * k] = rs[k];
+    __syncthreads();
+    for (int r = threadIdx.x; r < nbi; r += blockDim.x) {
+        double sum = 0.0;
+#pragma unroll
+        for (int w = 0; w < 8; ++w) sum += red[w][r];
+        if (r < rows_m) atomicAdd(rows + (int64_t)tm * nb + r, sum);
+    }
+}
+
+// L = A (lower tiles) and the max absolute row sum of A into rows[g.n]
+// (device); rows must hold g.n + 1 doubles.
+int copy_lansy_inf(Context *ctx, const double *dA, double *dL, const Geom &g, double *rows)
+{
+    CK(cudaMemsetAsync(rows, 0, ((size_t)g.n + 1) * sizeof(double), ctx->stream));
+    const unsigned nt = (unsigned)g.ntiles();
+    cudaStream_t st = ctx->stream;
+    switch (g.nbi) {
+    case 128: copy_rowsum_sym_kernel<4><<<nt, 256, 0, st>>>(dA, dL, g.mt, g.nb, g.n, rows); break;
+    case 256: copy_rowsum_sym_kernel<8><<<nt, 256, 0, st>>>(dA, dL, g.mt, g.nb, g.n, rows); break;
+    case 384: copy_rowsum_sym_kernel<12><<<nt, 256, 0, st>>>(dA, dL, g.mt, g.nb, g.n, rows); break;
+    case 512: copy_rowsum_sym_kernel<16><<<nt, 256, 0, st>>>(dA, dL, g.mt, g.nb, g.n, rows); break;
+    default: return DPLASMA_ERR_NOT_SUPPORTED;
+    }
+    CK(cudaGetLastError());
+    max_kernel<<<1, 256, 0, ctx->stream>>>(rows, g.n, rows + g.n);
+    CK(cudaGetLastError());
+    ctx->launches += 2;
+    return 0;
+}
+
 int lansy_inf_device(Context *ctx, const double *dA, const Geom &g, double *out)
 {
     double *rows = (double *)ctx->buffer(BUF_NORM, ((size_t)g.n + 1) * sizeof(double));

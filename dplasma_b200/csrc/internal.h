@@ -176,6 +176,8 @@ int batched_potri(Context *ctx, int batch, const int *d_n, const int *d_lda, dou
 
 // norms.cu
 int lansy_inf_device(Context *ctx, const double *dA, const Geom &g, double *out);
+// L = A (lower tiles) with the max absolute row sum of A into rows[g.n] (device)
+int copy_lansy_inf(Context *ctx, const double *dA, double *dL, const Geom &g, double *rows);
 
 // peak.cu
 double fp64_peak_tflops(Context *ctx);

@@ -732,14 +732,13 @@ int refine_solve(Context *ctx, const double *A0, double *L, const Geom &g, doubl
     st.backward_error = 0.0;
     st.factor_ms = st.refine_ms = 0.0;
 
-    // ||A||_inf of the FP64 matrix (to the host)
-    double anrm = 0.0;
-    if ((rc = lansy_inf_device(ctx, A0, g, &anrm))) return rc;
-    const double cte = anrm * eps * sqrt((double)g.n) * o.bwd_factor;
-
-    // mixed factorization of the working copy
+    // mixed factorization of the working copy; the copy also forms ||A||_inf
+    double *nrm = (double *)ctx->buffer(BUF_NORM, ((size_t)g.n + 1) * sizeof(double));
+    if (!nrm) return DPLASMA_ERR_OUT_OF_RESOURCES;
     CK(cudaEventRecord(e0, ctx->stream));
-    CK(cudaMemcpyAsync(L, A0, g.elems() * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    if ((rc = copy_lansy_inf(ctx, A0, L, g, nrm))) return rc;
+    double anrm = 0.0;
+    CK(cudaMemcpyAsync(&anrm, nrm + g.n, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     int info = 0;
     st.fmt_used = o.fmt;
     if ((rc = potrf_run(ctx, L, g.mt, g.nbi, g.nb, g.n, &info, o.fmt))) return rc;
@@ -751,6 +750,8 @@ int refine_solve(Context *ctx, const double *A0, double *L, const Geom &g, doubl
         if ((rc = potrf_run(ctx, L, g.mt, g.nbi, g.nb, g.n, &info, 2))) return rc;
     }
     CK(cudaEventRecord(e1, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));     // anrm has landed
+    const double cte = anrm * eps * sqrt((double)g.n) * o.bwd_factor;
     R.W = (const double *)ctx->buffer(BUF_W, 0);
 
     std::vector<double> xmax, xss, rmax, rss, bmax, bss;
