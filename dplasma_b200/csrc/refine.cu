@@ -176,7 +176,11 @@ __global__ void __launch_bounds__(SY_THREADS, 1)
 #pragma unroll
                 for (int q = 0; q < 4; ++q) ym[mi][ni][q] = 0.0;
         bool ok = true;
-#pragma unroll
+        // a rolled panel loop (an unrolled one outgrows the instruction
+        // cache); yacc rotates by one per panel, so the current panel's
+        // accumulator is always yacc[0] and the order is restored after
+        // SY_NP panels
+#pragma unroll 1
         for (int p = 0; p < SY_NP; ++p) {
             const uint32_t s = it % SY_NST;
             const bool got = warp_mbar_wait(&ctl->full[s], (it / SY_NST) & 1, limit_ns);
@@ -247,7 +251,10 @@ __global__ void __launch_bounds__(SY_THREADS, 1)
             }
             // the four partial sums of this panel's y_n
             const double *rr = red + (p & 1) * 1024 + rl * 8 + rni * 4 + rq;
-            yacc[p] += (rr[0] + rr[256]) + (rr[512] + rr[768]);
+            const double y0 = yacc[0] + ((rr[0] + rr[256]) + (rr[512] + rr[768]));
+#pragma unroll
+            for (int q = 0; q < SY_NP - 1; ++q) yacc[q] = yacc[q + 1];
+            yacc[SY_NP - 1] = y0;
         }
         if (!ok) {
             if (tid == 0) atomicCAS(status, ST_OK, ST_MBAR_TIMEOUT);
