@@ -54,7 +54,7 @@ class RefineStats(ctypes.Structure):
 
     _fields_ = [("iter", ctypes.c_int), ("inner_iters", ctypes.c_int), ("fallback", ctypes.c_int),
                 ("solver_used", ctypes.c_int), ("fmt_used", ctypes.c_int), ("backward_error", ctypes.c_double), ("factor_ms", ctypes.c_double),
-                ("refine_ms", ctypes.c_double)]
+                ("refine_ms", ctypes.c_double), ("anorm", ctypes.c_double)]
 
 
 FP16, BF16, FP16_SPLIT = 0, 1, 2

@@ -544,6 +544,7 @@ extern "C" int dplasma_b200_dsposv_ex(parsec_context_t *parsec, dplasma_enum_t u
         stats->backward_error = st.backward_error;
         stats->factor_ms = st.factor_ms;
         stats->refine_ms = st.refine_ms;
+        stats->anorm = st.anorm;
     }
     if (rc) return rc;   // error, or INFO > 0 of the FP64 fallback
     ctx->last_factor_ms = st.factor_ms;

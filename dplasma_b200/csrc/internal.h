@@ -154,7 +154,7 @@ struct RefineOpts {
 };
 struct RefineStats {
     int iter = 0, inner_iters = 0, fallback = 0, solver_used = 0, fmt_used = 0;
-    double backward_error = 0.0, factor_ms = 0.0, refine_ms = 0.0;
+    double backward_error = 0.0, factor_ms = 0.0, refine_ms = 0.0, anorm = 0.0;
 };
 int refine_solve(Context *ctx, const double *A0, double *L, const Geom &g, double *b, double *x, int npad, int nc,
                  const RefineOpts &o, RefineStats &st);

@@ -759,6 +759,7 @@ int refine_solve(Context *ctx, const double *A0, double *L, const Geom &g, doubl
     CK(cudaEventRecord(e1, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));     // anrm has landed
     const double cte = anrm * eps * sqrt((double)g.n) * o.bwd_factor;
+    st.anorm = anrm;
     R.W = (const double *)ctx->buffer(BUF_W, 0);
 
     std::vector<double> xmax, xss, rmax, rss, bmax, bss;

@@ -237,6 +237,7 @@ typedef struct dplasma_b200_refine_stats_s {
     double backward_error; /* max_j ||b_j - A x_j||_inf / (||A||_inf ||x_j||_inf + ||b_j||_inf) */
     double factor_ms;      /* device time of the mixed factorization (with its working copy) */
     double refine_ms;      /* device time of the solves and refinement (and of a fallback) */
+    double anorm;          /* ||A||_inf of the FP64 matrix, the scale of the stopping test */
 } dplasma_b200_refine_stats_t;
 
 /* Defaults: FP16, IR_AUTO, itermax 30, gmres_m 30, gmres_tol 1e-4, bwdmax 1, escalate 1. */

@@ -100,6 +100,9 @@ def test_dsposv_dplgsy(gpu_ctx, N, NB, NRHS, uplo, fmt):
     X64 = run_dposv(gpu_ctx, A, B, NB, uplo)
     assert np.abs(X - X64).max() / np.abs(X64).max() < 1e-12
     assert st["backward_error"] < 10 * N * EPS
+    # the infinity norm formed on the way through the working copy (padding excluded)
+    anorm = np.abs(A).sum(axis=1).max()
+    assert abs(st["anorm"] - anorm) <= 1e-13 * anorm, (st["anorm"], anorm)
 
 
 @pytest.mark.parametrize("kappa", [1e2, 1e4, 1e6])
