@@ -7,10 +7,11 @@
 // CTAs take problems from an atomic work queue in decreasing order of n
 // (longest first), so one launch balances sizes from 1 to 512.  A problem is
 // factored right-looking in 32-column panels:
-//   1. warp 0 factors the 32x32 diagonal block in registers (shuffles) and
-//      forms its inverse;
-//   2. every thread turns one row of the panel below into L (row x D^-T),
-//      storing it to global memory and to a shared panel;
+//   1. warp 0 factors the 32x32 diagonal block in registers, four columns
+//      per step (dev_chol32.cuh), and forms its inverse;
+//   2. the panel below becomes L = P D^-T (FP64: tensor cores, one 32-row
+//      block per warp; FP32: one row per thread), stored to global memory
+//      and to a shared panel;
 //   3. the lower triangle of the trailing matrix is updated from the shared
 //      panel in 32x32 tiles, one warp per tile (FP64 tensor cores; FP32 on
 //      the FMA pipes), the next panel's columns first so that warp 0 factors
@@ -53,13 +54,6 @@ struct BatchArgs {
     int *ticket;
     T *dscr;              // per CTA: inverses of the 32x32 diagonal blocks of its current problem
 };
-
-template <typename T>
-__device__ __forceinline__ T bt_rsqrt(T x);
-template <>
-__device__ __forceinline__ double bt_rsqrt<double>(double x) { return rsqrt(x); }
-template <>
-__device__ __forceinline__ float bt_rsqrt<float>(float x) { return rsqrtf(x); }
 
 // Diagonal block j0 (jb <= 32 columns) of one problem by warp 0: factor in
 // registers, write L back, accumulate log det, form the inverse into Dinv.
