@@ -279,8 +279,10 @@ def bench_adjoint(torch):
     xs = [torch.rand(m, 3, dtype=torch.float64, device="cuda", generator=g) for m in sizes]
     yb = [torch.randn(m, dtype=torch.float64, device="cuda", generator=g) for m in sizes]
 
+    ybf = torch.cat(yb)
+
     def fwd_b(l):
-        return dag.gp_log_marginal_likelihood_batched([dag.se_kernel(xx, l) for xx in xs], yb).sum()
+        return dag.gp_log_marginal_likelihood_flat(dag.se_kernel_batched(xs, l, flat=True), ybf, sizes).sum()
 
     lsb = torch.tensor(0.2, dtype=torch.float64, device="cuda", requires_grad=True)
     fwd_b(lsb).backward()                       # warm-up
@@ -297,8 +299,9 @@ def bench_adjoint(torch):
     tb_fb = (time.perf_counter() - t0) * 1e3
     batch = {"problems": 1024, "n": "uniform integer in [64, 256], seed 13", "forward_ms": tb_f,
              "forward_backward_ms": tb_fb, "dlengthscale": float(lsb.grad),
-             "note": "wall clock including the torch kernel construction and per-problem gradient assembly; "
-                     "library part: one dplasma_b200_dposv_batched and one dplasma_b200_dpotri_batched launch"}
+             "note": "wall clock including the kernel-matrix construction (se_kernel_batched, flat form) and the gradient "
+                     "assembly; library part: one dplasma_b200_dposv_batched and one dplasma_b200_dpotri_batched "
+                     "launch"}
     return {"n": n, "forward_ms": t_f, "forward_backward_ms": t_fb, "backward_over_forward": t_fb / t_f - 1.0,
             "batch": batch,
             "forward_tflops": flops_f / (t_f * 1e-3) / 1e12, "value": float(v), "dlengthscale": float(ls.grad),

@@ -153,3 +153,20 @@ def test_batched_potri_and_gp_gradients(gpu_ctx):
     assert abs(vals.sum().item() - tot.item()) <= 1e-9 * abs(tot.item())
     vals.sum().backward()
     assert abs(ls.grad.item() - ls_ref.grad.item()) <= 1e-8 * abs(ls_ref.grad.item())
+    # the same through the whole-batch kernel construction
+    ls2 = torch.tensor(0.2, dtype=torch.float64, device="cuda", requires_grad=True)
+    Kb = dag.se_kernel_batched([x.cuda() for x in xs], ls2)
+    for Kbi, x in zip(Kb, xs):
+        assert Kbi.shape == (x.shape[0], x.shape[0])
+        assert (Kbi.detach() - dag.se_kernel(x.cuda(), ls2.detach())).abs().max().item() <= 1e-15
+    vals2 = dag.gp_log_marginal_likelihood_batched(Kb, [y.cuda() for y in ys])
+    assert (vals2.detach() - vals.detach()).abs().max().item() <= 1e-9 * vals.detach().abs().max().item()
+    vals2.sum().backward()
+    assert abs(ls2.grad.item() - ls.grad.item()) <= 1e-9 * abs(ls.grad.item())
+    # and in the flat form (one autograd node)
+    ls3 = torch.tensor(0.2, dtype=torch.float64, device="cuda", requires_grad=True)
+    Kf = dag.se_kernel_batched([x.cuda() for x in xs], ls3, flat=True)
+    vals3 = dag.gp_log_marginal_likelihood_flat(Kf, torch.cat([y.cuda() for y in ys]), sizes)
+    assert (vals3.detach() - vals.detach()).abs().max().item() <= 1e-9 * vals.detach().abs().max().item()
+    vals3.sum().backward()
+    assert abs(ls3.grad.item() - ls.grad.item()) <= 1e-9 * abs(ls.grad.item())
