@@ -416,6 +416,7 @@ __device__ void potrf_task(const PotrfArgs &a, SmemCtl *ctl, double *ring, int k
             double d[32];
 #pragma unroll
             for (int c = 0; c < 32; ++c) d[c] = (c <= lane) ? __ldcg(T + (int64_t)(p0 + c) * nbi + p0 + lane) : 0.0;
+            // phase trace only: a use of the loaded values, so they have arrived at the timestamp
             if (a.ptrace) { double z = 0; for (int c = 0; c < 32; ++c) z += d[c]; if (z == 12345.0) colb[0] = z; }
             sub(0);
             double rdiag = 0.0;      // lane j: 1 / L(j,j)
@@ -442,6 +443,7 @@ __device__ void potrf_task(const PotrfArgs &a, SmemCtl *ctl, double *ring, int k
                     Dv[i * 33 + c] = x;
                     Wb[(int64_t)(q0 + c) * BLK + q0 + i] = x;
                 });
+                // phase trace only: the inverse is complete at the timestamp
                 if (a.ptrace) { __syncwarp(); if (Dv[lane * 33] == 12345.0) colb[1] = 0; }
                 sub(3);
             }
