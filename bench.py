@@ -311,6 +311,24 @@ def bench_adjoint(torch):
                     "dplasma_dpotrf_adjoint for a dense lower Lbar (autograd.cholesky backward, about 1.3 N^3 flops)"}
 
 
+def max_over_ranks(ms, dist, device):
+    """The slowest rank's time: every rank contributes its own device-timed
+    ms and all receive the max (the contract's max-over-ranks); one process
+    (dist None) returns ms itself."""
+    if dist is None:
+        return float(ms)
+    import torch
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(world, flops_per_step, ms_step):
+    """Whole-job TFLOP/s of `world` replicas that each ran flops_per_step in
+    the slowest rank's ms_step."""
+    return world * flops_per_step / (ms_step * 1e-3) / 1e12
+
+
 def run_gpu(args):
     import torch
     import dplasma_b200 as db
@@ -400,15 +418,11 @@ def run_gpu(args):
         wall = time.perf_counter() - t0
     if dist:
         dist.barrier()
-    total_ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
     ms_step = total_ms / args.steps
     iters = statistics.median(st["iter"] for st in stats)
     eff_flops = potrf_flops(N) + 2.0 * NRHS * N * N * (max(iters, 0) + 1)
-    value = world * eff_flops / (ms_step * 1e-3) / 1e12
+    value = replica_value(world, eff_flops, ms_step)
     fac_ms = statistics.median(st["factor_ms"] for st in stats)
     mixed_fwd = fwd_err(X, X64)
     clocks = clk.summary()
@@ -433,8 +447,8 @@ def run_gpu(args):
             assert rc == 0, ctx.last_error()
             if i > 0:
                 times.append(dt)
-        e2e_s = sum(times) / len(times)
-        e2e = {"value": world * eff_flops / e2e_s / 1e12, "unit": "TFLOP/s",
+        e2e_s = max_over_ranks(1e3 * sum(times) / len(times), dist, "cuda") * 1e-3
+        e2e = {"value": replica_value(world, eff_flops, e2e_s * 1e3), "unit": "TFLOP/s",
                "h2d_bytes_per_step": int(hA.numel() * 8 + hB.numel() * 8),
                "d2h_bytes_per_step": int(hX.numel() * 8), "s_per_step": e2e_s, "steps": len(times),
                "fp64_dposv_speedup": (fp64_ms * 1e-3) / e2e_s}
