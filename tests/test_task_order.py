@@ -70,7 +70,7 @@ def test_fp64_ticket_order(mt, nbs, delay):
 
 
 @pytest.mark.parametrize("mt,S,delay", [(1, 4, 0), (2, 4, 3), (5, 4, 0), (9, 4, 7), (17, 3, 100), (33, 4, 444),
-                                        (12, 1, 10), (10, 16, 5)])
+                                        (12, 1, 10), (10, 16, 5), (65, 8, 444), (65, 16, 444)])
 def test_mixed_ticket_order(mt, S, delay):
     replay(tasks(S, mt, 2, delay), mt, 2, S)
 
