@@ -55,7 +55,7 @@ def test_batched_fp64_matches_numpy(gpu_ctx):
 
 
 def test_batched_fp32_backward_errors(gpu_ctx):
-    # FP32 on kernels whose condition reaches ~1e6: judged by backward errors
+    # FP32 on kernels whose condition reaches ~1e6: checked by backward errors
     sizes = [1, 31, 32, 33, 100, 257, 512] + list(range(40, 520, 61))
     Ks, ys, mats, rhs, info, logdet = run(gpu_ctx, sizes, torch.float32)
     eps = 2.0 ** -24

@@ -1,7 +1,7 @@
 """GPU tests of the inverse routines next to the Cholesky path:
 dplasma_dtrtri, dplasma_dlauum, dplasma_dpotri, dplasma_dpoinv (the
 reference's src/ztrtri_wrapper.c, src/zlauum_wrapper.c, src/zpotri_wrapper.c,
-src/zpoinv_wrapper.c), judged by the reference's own check_zpoinv ratio
+src/zpoinv_wrapper.c), checked by the reference's own check_zpoinv ratio
 ||I - A^-1 A||_1 / (||A||_1 ||A^-1||_1 N eps) < 10 (src/dplasma_zcheck.c:264-314)
 and against numpy on the triangular pieces."""
 import numpy as np
