@@ -20,13 +20,26 @@
 //     on every GPU that loads the library until the process exits;
 //   * every call uses the same array and finds the previous call's contents:
 //     the counters that must start at zero are cleared on the caller's stream
-//     at the start of each call.  Calls that overlap on the GPU (two streams,
-//     two host threads) race on it and must not be issued;
+//     at the start of each call;
+//   * calls are serialized inside the process: a host mutex is held for the
+//     whole call, and the call returns only after its stream has finished the
+//     factorization, so a second caller (another thread, another stream)
+//     blocks until the first one's factorization is complete.  (Each process
+//     has its own copy of the array, so processes sharing a GPU do not share
+//     it.)  Nothing that goes through this entry point can race on it;
+//   * the current device must be the device that holds A->mat and owns
+//     `stream`; a mismatch is rejected before anything is launched;
+//   * the call cannot be recorded into a CUDA graph: it copies the ticket
+//     order from host memory and waits for its stream, which a stream
+//     capture forbids, so it returns DPLASMA_ERR_NOT_SUPPORTED when `stream`
+//     is capturing;
 //   * the first call on a device looks up the array's device address
-//     (cudaGetSymbolAddress, with that device current) and caches it; make
-//     that first call before any stream capture.
+//     (cudaGetSymbolAddress, with that device current) and caches it;
+//   * dependency and pipeline waits are bounded by DPLASMA_B200_WAIT_LIMIT_MS
+//     (milliseconds, default 4000), the setting of the regular entry points.
 #include <cuda_runtime.h>
 #include <stdio.h>
+#include <stdlib.h>
 
 #include <mutex>
 
@@ -96,6 +109,30 @@ extern "C" int dplasma_b200_dpotrf_noalloc(void *stream, dplasma_enum_t uplo, pa
     cudaStream_t st = (cudaStream_t)stream;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) return DPLASMA_ERR_UNEXPECTED;
+    // the matrix and the stream must belong to the current device
+    cudaPointerAttributes pa;
+    if (cudaPointerGetAttributes(&pa, A->mat) != cudaSuccess || pa.type != cudaMemoryTypeDevice || pa.device != dev) {
+        cudaGetLastError();
+        fprintf(stderr, "[dplasma_b200_dpotrf_noalloc] A->mat is not device memory of the current device %d\n", dev);
+        return DPLASMA_ERR_ILLEGAL_VALUE;
+    }
+    if (st) {
+        int sdev = -1;
+        if (cudaStreamGetDevice(st, &sdev) != cudaSuccess || sdev != dev) {
+            cudaGetLastError();
+            fprintf(stderr, "[dplasma_b200_dpotrf_noalloc] the stream does not belong to the current device %d\n", dev);
+            return DPLASMA_ERR_ILLEGAL_VALUE;
+        }
+    }
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone) {
+        cudaGetLastError();
+        fprintf(stderr, "[dplasma_b200_dpotrf_noalloc] cannot run under stream capture\n");
+        return DPLASMA_ERR_NOT_SUPPORTED;
+    }
+    const char *lim = getenv("DPLASMA_B200_WAIT_LIMIT_MS");
+    const long lim_ms = lim ? atol(lim) : 4000;
+    const uint64_t limit_ns = (uint64_t)(lim_ms > 0 ? lim_ms : 4000) * 1000000ull;
 
     std::lock_guard<std::mutex> guard(g_lock);
     // one-time set-up on this device: the device address of the scratch array
@@ -133,7 +170,7 @@ extern "C" int dplasma_b200_dpotrf_noalloc(void *stream, dplasma_enum_t uplo, pa
     }
     int info = 0, status = 0, diag[4] = {0, 0, 0, 0};
     const int rc = potrf_launch_prealloc(st, (double *)A->mat, mt, nb, nb, n, W, tasks, (int)ntasks, ctr, grid,
-                                         4000000000ull, &info, &status, diag);
+                                         limit_ns, &info, &status, diag);
     if (rc) return rc;
     if (status != 0) {
         fprintf(stderr, "[dplasma_b200_dpotrf_noalloc] scheduler status %d (site %d)\n", status, diag[0]);
