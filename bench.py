@@ -311,6 +311,59 @@ def bench_adjoint(torch):
                     "dplasma_dpotrf_adjoint for a dense lower Lbar (autograd.cholesky backward, about 1.3 N^3 flops)"}
 
 
+def bench_fp64_sweep(ctx, db, torch, peak64, sizes=(16384, 32768, 65536), nbs=(256, 384, 512), nrhs=16):
+    """Plain FP64 dpotrf + dpotrs on device-resident dplgsy matrices (seed
+    3872, diagonal += N) for N x NB x uplo, NRHS = 16 dplrnt right-hand sides
+    (seed 3873): factorization TFLOP/s against the measured DMMA peak, solve
+    GB/s of the two sweeps, and the reference's check_zaxmb ratio of the
+    solution formed on the GPU (dplasma_dsymm / dlansy / dlange)."""
+    out = []
+    for N in sizes:
+        # the residual needs A with 256-wide tiles; dplgsy depends on (i, j)
+        # only, so this is the same matrix whatever NB the factorization used
+        dR = db.desc_sym(N, 256, db.Lower)
+        Ar = torch.empty(db.desc_elems(dR), dtype=torch.float64, device="cuda")
+        db.attach(dR, Ar)
+        assert ctx.dplgsy(float(N), db.Lower, dR, SEED_A) == 0
+        for NB in nbs:
+            dB = db.desc_general(N, nrhs, NB, NB)
+            B0 = torch.empty(db.desc_elems(dB), dtype=torch.float64, device="cuda")
+            db.attach(dB, B0)
+            assert ctx.dplrnt(0, dB, SEED_B) == 0
+            for uplo, name in ((db.Lower, "L"), (db.Upper, "U")):
+                dA = db.desc_sym(N, NB, uplo)
+                A = torch.empty(db.desc_elems(dA), dtype=torch.float64, device="cuda")
+                db.attach(dA, A)
+                assert ctx.dplgsy(float(N), uplo, dA, SEED_A) == 0
+                info = ctx.dpotrf(uplo, dA)
+                if info != 0:
+                    raise RuntimeError(f"fp64 sweep dpotrf N={N} NB={NB} {name}: {info} {ctx.last_error()}")
+                fac_ms = ctx.last_factor_ms()
+                X = B0.clone()
+                db.attach(dB, X)
+                assert ctx.dpotrs(uplo, dA, dB) == 0, ctx.last_error()
+                sol_ms = ctx.last_solve_ms()
+                del A
+                # residual B - A X
+                R = B0.clone()
+                dXr, dRr, dBr = (db.desc_general(N, nrhs, NB, NB) for _ in range(3))
+                db.attach(dXr, X)
+                db.attach(dRr, R)
+                db.attach(dBr, B0)
+                ratio = ctx.check_daxmb(db.Lower, dR, dBr, dXr, dRr)
+                tf = potrf_flops(N) / (fac_ms * 1e-3) / 1e12
+                sweep_bytes = 2.0 * (N * (N + 1) / 2.0 * 8 + 2.0 * N * nrhs * 8)
+                out.append({"n": N, "nb": NB, "uplo": name, "dpotrf_ms": fac_ms, "dpotrf_tflops": tf,
+                            "frac_of_fp64_peak": tf / peak64 if peak64 > 0 else None,
+                            "dpotrs_ms": sol_ms, "dpotrs_gbs": sweep_bytes / (sol_ms * 1e-3) / 1e9,
+                            "check_daxmb": ratio})
+                del X, R
+            del B0
+        del Ar
+        torch.cuda.empty_cache()
+    return out
+
+
 def max_over_ranks(ms, dist, device):
     """The slowest rank's time: every rank contributes its own device-timed
     ms and all receive the max (the contract's max-over-ranks); one process
@@ -427,6 +480,20 @@ def run_gpu(args):
     mixed_fwd = fwd_err(X, X64)
     clocks = clk.summary()
 
+    # the reference's check_zaxmb on the GPU for both solutions (A_pristine is
+    # the untouched matrix, B_pristine the right-hand sides)
+    def daxmb(Xsol):
+        dXc, dRc, dBc, dAc = db.desc_general(N, NRHS, NB, NB), db.desc_general(N, NRHS, NB, NB), \
+            db.desc_general(N, NRHS, NB, NB), db.desc_sym(N, NB, db.Lower)
+        Xc, Rc = Xsol.clone(), B_pristine.clone()
+        db.attach(dXc, Xc)
+        db.attach(dRc, Rc)
+        db.attach(dBc, B_pristine)
+        db.attach(dAc, A_pristine)
+        return ctx.check_daxmb(db.Lower, dAc, dBc, dXc, dRc)
+
+    ratio64, ratio_mixed = daxmb(X64), daxmb(X)
+
     # ---- end to end through the C ABI with pinned host buffers
     e2e = None
     if args.e2e_steps > 0:
@@ -477,6 +544,13 @@ def run_gpu(args):
                               "fmt_used": st["fmt_used"], "backward_error": st["backward_error"],
                               "forward_error_vs_fp64": fwd_err(X, Xk), "factor_ms": st["factor_ms"]})
 
+    a_gb = A.numel() * 8 / 1e9
+    fp64_sweep = None
+    if args.fp64_sweep:
+        del A, B
+        torch.cuda.empty_cache()
+        fp64_sweep = bench_fp64_sweep(ctx, db, torch, peak64)
+
     batched = adjoint = None
     if args.extras:
         batched = bench_batched(ctx, db, torch, peak64)
@@ -512,15 +586,16 @@ def run_gpu(args):
                                f"{args.fmt} trailing updates, FP64 IR/GMRES-IR to the LAPACK dsposv accuracy; "
                                f"A = Q diag(geomspace(1, {args.kappa:g})) Q^T, Q = 64 Householder reflectors "
                                "(seed 7), B = dplrnt(seed 3873)",
-                   "l2": "inputs larger than L2 (A is %.1f GB)" % (A.numel() * 8 / 1e9),
+                   "l2": "inputs larger than L2 (A is %.1f GB)" % a_gb,
                    "parallelism": "replicas" if world > 1 else "single GPU"},
         "time_to_accuracy_s": ms_step * 1e-3, "mixed_iter": iters,
         "mixed_backward_error": max(st["backward_error"] for st in stats),
         "mixed_forward_error_vs_fp64": mixed_fwd, "mixed_fallback": max(st["fallback"] for st in stats),
-        "mixed_factor_ms": fac_ms,
+        "mixed_factor_ms": fac_ms, "mixed_check_daxmb": ratio_mixed,
         "fp64": {"dposv_ms": fp64_ms, "tflops": posv_flops(N, NRHS) / (fp64_ms * 1e-3) / 1e12,
                  "dpotrf_ms": fac64, "dpotrs_ms": statistics.median(r[3] for r in fp64),
-                 "speedup_of_mixed": fp64_ms / ms_step},
+                 "speedup_of_mixed": fp64_ms / ms_step, "check_daxmb": ratio64},
+        "fp64_sweep": fp64_sweep,
         "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak16, "unit": "TFLOP/s",
                      "frac": achieved / peak16 if peak16 else None, "traffic": traffic,
                      "kernel": "potrf_persistent_kernel<true> (mixed factorization)",
@@ -563,6 +638,8 @@ def main():
     p.add_argument("--no-sweep", dest="sweep", action="store_false")
     p.add_argument("--no-extras", dest="extras", action="store_false",
                    help="skip the batched and adjoint measurements")
+    p.add_argument("--no-fp64-sweep", dest="fp64_sweep", action="store_false",
+                   help="skip the FP64 dpotrf/dpotrs sweep over N x NB x uplo")
     args = p.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)

@@ -27,7 +27,7 @@ NoTrans, Trans, ConjTrans = 111, 112, 113
 Upper, Lower, UpperLower = 121, 122, 123
 NonUnit, Unit = 131, 132
 Left, Right = 141, 142
-InfNorm = 175
+OneNorm, FrobeniusNorm, InfNorm, MaxNorm = 171, 174, 175, 177
 MATRIX_DOUBLE = 3
 STORAGE_LAPACK, STORAGE_TILE = 0, 1
 HOST, DEVICE = 0, 1
@@ -72,8 +72,11 @@ EXPORTS = (
     "dplasma_b200_dsposv_ex", "dplasma_b200_dplgsy_cond", "dplasma_b200_dposv_batched",
     "dplasma_b200_sposv_batched", "dplasma_b200_batched_variant", "dplasma_dpotrf_adjoint",
     "dplasma_dtrtri", "dplasma_dlauum", "dplasma_dpotri", "dplasma_dpoinv", "dplasma_dpoinv_sync",
-    "dplasma_b200_dpotri_batched", "pdpotrf_",
+    "dplasma_b200_dpotri_batched", "pdpotrf_", "dplasma_b200_dpotrf_noalloc", "dplasma_b200_inject_fault",
+    "dplasma_b200_set_wait_limits", "dplasma_b200_set_selfcheck", "dplasma_b200_selfcheck", "dplasma_dlange",
+    "dplasma_dsymm",
 )
+INJECT_NONE, INJECT_TASK_FAILED, INJECT_WITHHOLD = 0, 1, 2
 
 
 def lib():
@@ -132,6 +135,14 @@ def lib():
     L.dplasma_b200_refine_opts_default.argtypes = [ctypes.POINTER(RefineOpts)]
     L.dplasma_dsposv.argtypes = [P, I, pd, pd, pd, ctypes.POINTER(I)]
     L.dplasma_b200_dsposv_ex.argtypes = [P, I, pd, pd, pd, ctypes.POINTER(RefineOpts), ctypes.POINTER(RefineStats)]
+    L.dplasma_dlange.restype = D
+    L.dplasma_dlange.argtypes = [P, I, pd]
+    L.dplasma_dsymm.argtypes = [P, I, I, D, pd, pd, D, pd]
+    L.dplasma_b200_inject_fault.argtypes = [P, I, I]
+    L.dplasma_b200_set_wait_limits.argtypes = [P, I, I]
+    L.dplasma_b200_set_selfcheck.argtypes = [P, I]
+    pll = ctypes.POINTER(ctypes.c_longlong)
+    L.dplasma_b200_selfcheck.argtypes = [P, pll, pll, pll]
     _lib = L
     return L
 
@@ -246,6 +257,23 @@ class Context:
     def fp64_peak_tflops(self) -> float:
         return lib().dplasma_b200_fp64_peak_tflops(self.h)
 
+    # -- failure detection
+    def inject_fault(self, kind: int, arg: int) -> int:
+        return lib().dplasma_b200_inject_fault(self.h, kind, arg)
+
+    def set_wait_limits(self, dep_ms: int, pipe_ms: int) -> int:
+        return lib().dplasma_b200_set_wait_limits(self.h, dep_ms, pipe_ms)
+
+    def set_selfcheck(self, on: bool) -> int:
+        return lib().dplasma_b200_set_selfcheck(self.h, 1 if on else 0)
+
+    def selfcheck(self):
+        """(tickets, task runs, tickets not run exactly once) of the last
+        factorization, or None when the self check is off."""
+        t, r, b = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
+        rc = lib().dplasma_b200_selfcheck(self.h, ctypes.byref(t), ctypes.byref(r), ctypes.byref(b))
+        return None if rc else (t.value, r.value, b.value)
+
     # -- the dplasma calls (descriptor `mat` must be set by the caller)
     def dpotrf(self, uplo: int, A: Desc) -> int:
         return lib().dplasma_dpotrf(self.h, uplo, ctypes.byref(A))
@@ -267,6 +295,25 @@ class Context:
 
     def dlansy(self, ntype: int, uplo: int, A: Desc) -> float:
         return lib().dplasma_dlansy(self.h, ntype, uplo, ctypes.byref(A))
+
+    def dlange(self, ntype: int, A: Desc) -> float:
+        return lib().dplasma_dlange(self.h, ntype, ctypes.byref(A))
+
+    def dsymm(self, side: int, uplo: int, alpha: float, A: Desc, B: Desc, beta: float, C: Desc) -> int:
+        return lib().dplasma_dsymm(self.h, side, uplo, alpha, ctypes.byref(A), ctypes.byref(B), beta, ctypes.byref(C))
+
+    def check_daxmb(self, uplo: int, A: Desc, B: Desc, X: Desc, R: Desc) -> float:
+        """The reference's check_zaxmb (src/dplasma_zcheck.c:179-224) on the GPU:
+        ||B - A X||_inf / ((||A||_inf ||X||_inf + ||B||_inf) N eps).  R must be a
+        descriptor shaped like B holding a copy of B; it receives B - A X."""
+        an = self.dlansy(InfNorm, uplo, A)
+        bn = self.dlange(InfNorm, B)
+        xn = self.dlange(InfNorm, X)
+        rc = self.dsymm(Left, uplo, -1.0, A, X, 1.0, R)
+        if rc != 0 or min(an, bn, xn) < 0:
+            raise RuntimeError(f"check_daxmb on the GPU failed (rc={rc}): {self.last_error()}")
+        rn = self.dlange(InfNorm, R)
+        return rn / ((an * xn + bn) * A.n * 2.0 ** -53)
 
     def posv_batched(self, mats, rhs=None, keep=None):
         """Batched Cholesky + solve + log-det (dplasma_b200_dposv_batched or

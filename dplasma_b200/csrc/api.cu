@@ -5,7 +5,10 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
 #include <new>
+#include <vector>
+#include <math.h>
 
 #include "internal.h"
 
@@ -176,6 +179,37 @@ extern "C" const char *dplasma_b200_last_error(const parsec_context_t *p) { retu
 extern "C" double dplasma_b200_last_factor_ms(const parsec_context_t *p) { return p ? p->impl.last_factor_ms : 0.0; }
 extern "C" double dplasma_b200_last_solve_ms(const parsec_context_t *p) { return p ? p->impl.last_solve_ms : 0.0; }
 extern "C" int dplasma_b200_last_launches(const parsec_context_t *p) { return p ? p->impl.launches : 0; }
+extern "C" int dplasma_b200_inject_fault(parsec_context_t *p, int kind, int arg)
+{
+    if (!p) return DPLASMA_ERR_NOT_INITIALIZED;
+    if ((kind != INJECT_NONE && kind != INJECT_TASK_FAILED && kind != INJECT_WITHHOLD) || arg < 0)
+        return DPLASMA_ERR_ILLEGAL_VALUE;
+    p->impl.inject_kind = kind;
+    p->impl.inject_arg = arg;
+    return 0;
+}
+extern "C" int dplasma_b200_set_wait_limits(parsec_context_t *p, int dep_ms, int pipe_ms)
+{
+    if (!p) return DPLASMA_ERR_NOT_INITIALIZED;
+    if (dep_ms <= 0 || pipe_ms <= 0) return DPLASMA_ERR_ILLEGAL_VALUE;
+    p->impl.dep_limit_ns = (uint64_t)dep_ms * 1000000ull;
+    p->impl.pipe_limit_ns = (uint64_t)pipe_ms * 1000000ull;
+    return 0;
+}
+extern "C" int dplasma_b200_set_selfcheck(parsec_context_t *p, int on)
+{
+    if (!p) return DPLASMA_ERR_NOT_INITIALIZED;
+    p->impl.self_check = on != 0;
+    return 0;
+}
+extern "C" int dplasma_b200_selfcheck(const parsec_context_t *p, long long *tickets, long long *runs, long long *bad)
+{
+    if (!p) return DPLASMA_ERR_NOT_INITIALIZED;
+    if (tickets) *tickets = p->impl.last_tickets;
+    if (runs) *runs = p->impl.last_tasks_executed;
+    if (bad) *bad = p->impl.last_tickets_bad;
+    return p->impl.self_check ? 0 : DPLASMA_ERR_NOT_INITIALIZED;
+}
 extern "C" double dplasma_b200_fp64_peak_tflops(parsec_context_t *p)
 {
     if (!p) return -1.0;
@@ -462,6 +496,107 @@ extern "C" double dplasma_dlansy(parsec_context_t *parsec, dplasma_enum_t ntype,
     return out;
 }
 
+// dplasma_dlange (src/zlange_wrapper.c, dplasma_z.h:98): norm of a general
+// matrix, computed on the GPU; -1.0 for a bad norm type or descriptor.
+extern "C" double dplasma_dlange(parsec_context_t *parsec, dplasma_enum_t ntype, const parsec_tiled_matrix_t *A)
+{
+    if (!parsec || (ntype != dplasmaInfNorm && ntype != dplasmaOneNorm && ntype != dplasmaMaxNorm &&
+                    ntype != dplasmaFrobeniusNorm))
+        return -1.0;
+    if (check_general("dplasma_dlange", A)) return -1.0;
+    Context *ctx = &parsec->impl;
+    cudaSetDevice(ctx->device);
+    ctx->launches = 0;
+    if (A->m == 0 || A->n == 0) return 0.0;
+    // the padded column-major form of the right-hand-side path (rows of tile mb)
+    const int nbi = ((A->mb + 127) / 128) * 128;
+    const int mt = (A->m + A->mb - 1) / A->mb;
+    const int npad = mt * nbi, ncols = A->n;
+    double *dX = (double *)ctx->buffer(BUF_R, (size_t)npad * ncols * sizeof(double));
+    if (!dX) return -1.0;
+    if (upload_rhs(ctx, A, A->mb, nbi, npad, ncols, dX)) return -1.0;
+    std::vector<double> o(3 + (size_t)ncols);
+    if (lange_device(ctx, dX, npad, npad, ncols, o.data())) return -1.0;
+    if (ntype == dplasmaInfNorm) return o[0];
+    if (ntype == dplasmaMaxNorm) return o[1];
+    if (ntype == dplasmaFrobeniusNorm) return sqrt(o[2]);
+    double one = 0.0;
+    for (int j = 0; j < ncols; ++j) one = std::max(one, o[3 + j]);
+    return one;
+}
+
+// dplasma_dsymm: src/zsymm_wrapper.c (dplasma_z.h:40), the product the
+// reference's check_zaxmb forms (src/dplasma_zcheck.c:196-197).  C = alpha A B
+// + beta C with A symmetric (its uplo triangle); left side only, A with
+// 256-wide internal tiles (tile size 129..256).  Returns 0, -1/-2 for a bad
+// side/uplo, -4..-6 for bad shapes (as the reference), or a negative code.
+extern "C" int dplasma_dsymm(parsec_context_t *parsec, dplasma_enum_t side, dplasma_enum_t uplo, double alpha,
+                             const parsec_tiled_matrix_t *A, const parsec_tiled_matrix_t *B, double beta,
+                             parsec_tiled_matrix_t *C)
+{
+    if (side != dplasmaLeft && side != dplasmaRight) {
+        dplasma_error("dplasma_dsymm", "illegal value of side");
+        return -1;
+    }
+    if (uplo != dplasmaLower && uplo != dplasmaUpper) {
+        dplasma_error("dplasma_dsymm", "illegal value of uplo");
+        return -2;
+    }
+    if (!A || !B || !C) return DPLASMA_ERR_ILLEGAL_VALUE;
+    if (A->m != A->n) {
+        dplasma_error("dplasma_dsymm", "illegal size of matrix A which should be square");
+        return -4;
+    }
+    if (B->m != C->m || B->n != C->n) {
+        dplasma_error("dplasma_dsymm", "illegal sizes of matrices B and C");
+        return -5;
+    }
+    if ((side == dplasmaLeft && A->n != C->m) || (side == dplasmaRight && A->n != C->n)) {
+        dplasma_error("dplasma_dsymm", "illegal size of matrix A");
+        return -6;
+    }
+    if (side == dplasmaRight) {
+        dplasma_error("dplasma_dsymm", "side == dplasmaRight is not provided by this library");
+        return DPLASMA_ERR_NOT_SUPPORTED;
+    }
+    if (!parsec) return DPLASMA_ERR_NOT_INITIALIZED;
+    int rc;
+    if ((rc = check_square("dplasma_dsymm", A)) || (rc = check_general("dplasma_dsymm", B)) ||
+        (rc = check_general("dplasma_dsymm", C)))
+        return rc;
+    Context *ctx = &parsec->impl;
+    cudaSetDevice(ctx->device);
+    ctx->launches = 0;
+    ctx->errmsg[0] = 0;
+    if (C->m == 0 || C->n == 0) return 0;
+    Geom g = make_geom(A->m, A->mb);
+    if (g.nbi != 256) {
+        ctx->set_error("dplasma_dsymm: tile size %d not supported (129..256)", A->mb);
+        return DPLASMA_ERR_NOT_SUPPORTED;
+    }
+    const bool inplace = in_place_ok(A, uplo, g);
+    double *dA = inplace ? (double *)A->mat : (double *)ctx->buffer(BUF_A, g.elems() * sizeof(double));
+    if (!dA) return DPLASMA_ERR_OUT_OF_RESOURCES;
+    if (!inplace && (rc = upload_sym(ctx, A, uplo, g, dA))) return rc;
+    const int ncols = C->n, npad = g.mt * g.nbi, ncp = ((ncols + 7) / 8) * 8;
+    double *dB = (double *)ctx->buffer(BUF_B, (size_t)npad * ncp * sizeof(double));
+    double *dC = (double *)ctx->buffer(BUF_R, (size_t)npad * ncp * sizeof(double));
+    int *status = (int *)ctx->buffer(BUF_SOLVE_CTR, 256);
+    if (!dB || !dC || !status) return DPLASMA_ERR_OUT_OF_RESOURCES;
+    CK(cudaMemsetAsync(status, 0, sizeof(int), ctx->stream));
+    if ((rc = upload_rhs(ctx, B, g.nb, g.nbi, npad, ncols, dB))) return rc;
+    if ((rc = upload_rhs(ctx, C, g.nb, g.nbi, npad, ncols, dC))) return rc;
+    if ((rc = scale_cols(ctx, dC, npad, npad, ncols, beta))) return rc;
+    if (alpha != 0.0 && (rc = symm_tiles(ctx, dA, g, dB, npad, dC, npad, ncols, alpha, status))) return rc;
+    int hs = 0;
+    CK(cudaMemcpyAsync(&hs, status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    if ((rc = download_rhs(ctx, C, g.nb, g.nbi, npad, ncols, dC))) return rc;
+    if (hs != 0) {
+        ctx->set_error("dplasma_dsymm: product kernel status %d (pipeline wait timed out)", hs);
+        return DPLASMA_ERR_UNEXPECTED;
+    }
+    return 0;
+}
 
 // ---------------------------------------------------------------------------
 // mixed precision (no dplasma counterpart; LAPACK dsposv argument meaning)

@@ -166,6 +166,74 @@ int lansy_inf_device(Context *ctx, const double *dA, const Geom &g, double *out)
 }
 
 // ---------------------------------------------------------------------------
+// Norms of a general rows x ncols column-major array (padding rows and columns
+// are zero): out[0] = max row sum |a|, out[1] = max |a|, out[2] = sum a^2,
+// out[3 + j] = column sum |a| of column j.  Non-negative doubles are
+// compared by their bit patterns (monotone in integer order).
+// ---------------------------------------------------------------------------
+__global__ void lange_kernel(const double *__restrict__ X, int ld, int rows, int ncols, double *out)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    double rs = 0.0, mx = 0.0, ss = 0.0;
+    if (r < rows) {
+        for (int j = 0; j < ncols; ++j) {
+            const double v = X[(int64_t)j * ld + r];
+            const double a = fabs(v);
+            rs += a;
+            mx = (a > mx || a != a) ? a : mx;
+            ss = fma(v, v, ss);
+            if (a != 0.0) atomicAdd(out + 3 + j, a);
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        rs = fmax(rs, __shfl_xor_sync(0xffffffffu, rs, o));
+        mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        ss += __shfl_xor_sync(0xffffffffu, ss, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(reinterpret_cast<unsigned long long *>(out + 0), (unsigned long long)__double_as_longlong(rs));
+        atomicMax(reinterpret_cast<unsigned long long *>(out + 1), (unsigned long long)__double_as_longlong(mx));
+        atomicAdd(out + 2, ss);
+    }
+}
+
+int lange_device(Context *ctx, const double *dX, int ld, int rows, int ncols, double *host_out)
+{
+    double *o = (double *)ctx->buffer(BUF_NORM, (size_t)(3 + ncols) * sizeof(double));
+    if (!o) return DPLASMA_ERR_OUT_OF_RESOURCES;
+    CK(cudaMemsetAsync(o, 0, (size_t)(3 + ncols) * sizeof(double), ctx->stream));
+    if (rows > 0 && ncols > 0) {
+        lange_kernel<<<(rows + 255) / 256, 256, 0, ctx->stream>>>(dX, ld, rows, ncols, o);
+        CK(cudaGetLastError());
+        ctx->launches++;
+    }
+    CK(cudaMemcpyAsync(host_out, o, (size_t)(3 + ncols) * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return 0;
+}
+
+// C = beta C on a rows x ncols column-major array (beta == 0 writes zeros).
+__global__ void scale_cols_kernel(double *X, int ld, int rows, int ncols, double beta)
+{
+    const int64_t n = (int64_t)rows * ncols;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        const int j = (int)(e / rows), r = (int)(e % rows);
+        double *p = X + (int64_t)j * ld + r;
+        *p = beta == 0.0 ? 0.0 : beta * *p;
+    }
+}
+
+int scale_cols(Context *ctx, double *dX, int ld, int rows, int ncols, double beta)
+{
+    if (beta == 1.0 || rows == 0 || ncols == 0) return 0;
+    scale_cols_kernel<<<ctx->sms * 4, 256, 0, ctx->stream>>>(dX, ld, rows, ncols, beta);
+    CK(cudaGetLastError());
+    ctx->launches++;
+    return 0;
+}
+
+// ---------------------------------------------------------------------------
 // FP64 tensor-core peak: register-only DMMA chains on every SM.
 // ---------------------------------------------------------------------------
 constexpr int PEAK_ITERS = 4096;

@@ -16,6 +16,7 @@ enum : int {
     ST_DEP_TIMEOUT = 1,     // a dependency wait ran past its time limit
     ST_MBAR_TIMEOUT = 2,    // a pipeline (mbarrier) wait ran past its time limit
     ST_BAD_TASK = 3,        // malformed task descriptor
+    ST_TASK_FAILED = 4,     // a task was marked failed by the host (fault injection)
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p)

@@ -37,6 +37,7 @@ enum BufferId : int {
     BUF_ADJ,          // adjoint: dense L, W = L^-1 and two products
     BUF_BATCH_SCR,    // batched: per-CTA inverses of the diagonal blocks
     BUF_BATCH_W,      // batched inverse: per-CTA padded factor and L^-1
+    BUF_SELFCHECK,    // per-ticket run counters (self check)
     BUF_COUNT
 };
 
@@ -69,6 +70,8 @@ struct Context {
     double last_factor_ms = 0.0, last_solve_ms = 0.0;
     int launches = 0;
     long long last_tasks_executed = 0;
+    long long last_tickets = 0, last_tickets_bad = 0;   // self check of the last factorization
+    int inject_kind = 0, inject_arg = -1;                // one-shot fault injection of the next factorization
     int bt_choice[2][8] = {{-1, -1, -1, -1, -1, -1, -1, -1}, {-1, -1, -1, -1, -1, -1, -1, -1}};   // autotuned variant
     int bt_last_variant = -1;
     BatchGraph bt_graph[2];                  // FP64, FP32
@@ -108,6 +111,9 @@ struct Context {
             return DPLASMA_ERR_UNEXPECTED;                                                              \
         }                                                                                               \
     } while (0)
+
+// Host-side fault injection (dplasma_b200_inject_fault).
+enum : int { INJECT_NONE = 0, INJECT_TASK_FAILED = 1, INJECT_WITHHOLD = 2 };
 
 // Geometry of the device copy of an N x N symmetric matrix with caller tile nb.
 struct Geom {
@@ -178,6 +184,11 @@ int batched_potri(Context *ctx, int batch, const int *d_n, const int *d_lda, dou
 int lansy_inf_device(Context *ctx, const double *dA, const Geom &g, double *out);
 // L = A (lower tiles) with the max absolute row sum of A into rows[g.n] (device)
 int copy_lansy_inf(Context *ctx, const double *dA, double *dL, const Geom &g, double *rows);
+
+// norms of a padded column-major array: out[0] inf, out[1] max, out[2] sum of
+// squares, out[3 + j] one-norm of column j (host array of 3 + ncols)
+int lange_device(Context *ctx, const double *dX, int ld, int rows, int ncols, double *host_out);
+int scale_cols(Context *ctx, double *dX, int ld, int rows, int ncols, double beta);
 
 // peak.cu
 double fp64_peak_tflops(Context *ctx);

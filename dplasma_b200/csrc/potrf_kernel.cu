@@ -110,16 +110,27 @@ __device__ void producer_warp(const PotrfArgs &a, SmemCtl *ctl, double *ring, co
         tk = __shfl_sync(0xffffffffu, tk, 0);
         bool end = (tk < 0 || tk >= a.ntasks);
         uint64_t t = end ? 0 : a.tasks[tk];
+        // fault injection (host-chosen): a ticket taken and dropped withholds
+        // the dependency it would have released
+        if (!end && tk == a.skip_ticket) continue;
         int ok = 1;
         if (!end && lane == 0) {
-            if (a.trace) a.trace[4 * (int64_t)tk + 0] = globaltimer_ns();
-            ok = wait_deps<MIXED>(a, t) ? 1 : 0;
-            if (a.trace) a.trace[4 * (int64_t)tk + 1] = globaltimer_ns();
-            if (!ok && ld_volatile(a.status) == ST_DEP_TIMEOUT && a.diag[0] == 0) {
-                a.diag[0] = 7;
-                a.diag[1] = blockIdx.x;
-                a.diag[2] = tk;
-                a.diag[3] = (int)(t & 0xFFFFFFFF);
+            if (task_type(t) == T_POTRF && task_k(t) == a.fail_potrf) {
+                // fault injection: the task is reported failed instead of run
+                report(a, ST_TASK_FAILED, 12, task_k(t), tk);
+                ok = 0;
+            } else {
+                if (a.trace) a.trace[4 * (int64_t)tk + 0] = globaltimer_ns();
+                ok = wait_deps<MIXED>(a, t) ? 1 : 0;
+                if (a.trace) a.trace[4 * (int64_t)tk + 1] = globaltimer_ns();
+                if (!ok && ld_volatile(a.status) == ST_DEP_TIMEOUT && a.diag[0] == 0) {
+                    a.diag[0] = 7;
+                    a.diag[1] = blockIdx.x;
+                    a.diag[2] = tk;
+                    a.diag[3] = (int)(t & 0xFFFFFFFF);
+                }
+                // a wait that gave up stops every CTA at its next ticket
+                if (!ok) atomicExch(a.abort_flag, 1);
             }
         }
         ok = __shfl_sync(0xffffffffu, ok, 0);
@@ -777,6 +788,7 @@ __device__ void consumer_warps(const PotrfArgs &a, SmemCtl *ctl, double *ring)
                 __threadfence();
                 red_release_add(release, 1);
             }
+            if (a.ran) atomicAdd(a.ran + tk, 1);
             if (a.trace) {
                 a.trace[4 * (int64_t)tk + 3] = globaltimer_ns();
                 a.trace_cta[tk] = blockIdx.x;
@@ -1064,6 +1076,16 @@ int potrf_run(Context *ctx, double *dA, int mt, int nbi, int nb_user, int n_user
     a.diag = ctr + 4;
     a.trace = nullptr;
     a.ptrace = nullptr;
+    a.ran = nullptr;
+    // one-shot fault injection of this call (host side only)
+    a.fail_potrf = ctx->inject_kind == INJECT_TASK_FAILED ? ctx->inject_arg : -1;
+    a.skip_ticket = ctx->inject_kind == INJECT_WITHHOLD ? ctx->inject_arg : -1;
+    ctx->inject_kind = 0;
+    if (ctx->self_check) {
+        a.ran = (int *)ctx->buffer(BUF_SELFCHECK, (size_t)a.ntasks * sizeof(int));
+        if (!a.ran) return DPLASMA_ERR_OUT_OF_RESOURCES;
+        CK(cudaMemsetAsync(a.ran, 0, (size_t)a.ntasks * sizeof(int), st));
+    }
     if (ctx->trace_path[0]) {
         const size_t tbytes = ((size_t)a.ntasks * 4 + 8 * (size_t)grid) * sizeof(unsigned long long) + (size_t)a.ntasks * sizeof(int);
         a.trace = (unsigned long long *)ctx->buffer(BUF_TRACE, tbytes);
@@ -1127,17 +1149,30 @@ int potrf_run(Context *ctx, double *dA, int mt, int nbi, int nb_user, int n_user
     cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
     ctx->last_factor_ms = ms;
     if (hs[3] != ST_OK) {
-        ctx->set_error("potrf scheduler status %d (1: dependency wait timed out, 2: pipeline wait timed out); "
-                       "site %d cta %d values %d %d; tickets taken %d of %d",
-                       hs[3], hs[4], hs[5], hs[6], hs[7], hs[0], ctx->ntasks);
+        static const char *what[] = {"ok", "dependency wait timed out", "pipeline wait timed out", "malformed task",
+                                     "task reported failed"};
+        ctx->set_error("potrf scheduler status %d (%s); site %d cta %d values %d %d; tickets taken %d of %d", hs[3],
+                       (hs[3] >= 0 && hs[3] <= ST_TASK_FAILED) ? what[hs[3]] : "unknown", hs[4], hs[5], hs[6], hs[7],
+                       hs[0], ctx->ntasks);
         return DPLASMA_ERR_UNEXPECTED;
     }
     if (ctx->self_check) {
-        std::vector<int> cnt(grid);
+        // every ticket must have run exactly once (unless INFO > 0 stopped the
+        // scheduler early, when the tickets after the failing POTRF never run)
+        std::vector<int> cnt(grid), ran(a.ntasks);
         CK(cudaMemcpy(cnt.data(), a.task_count, grid * sizeof(int), cudaMemcpyDeviceToHost));
-        long long tot = 0;
+        CK(cudaMemcpy(ran.data(), a.ran, (size_t)a.ntasks * sizeof(int), cudaMemcpyDeviceToHost));
+        long long tot = 0, bad = 0;
         for (int c : cnt) tot += c;
+        for (int r : ran) bad += (r != 1);
         ctx->last_tasks_executed = tot;
+        ctx->last_tickets = a.ntasks;
+        ctx->last_tickets_bad = bad;
+        if (hs[1] == 0 && (bad != 0 || tot != a.ntasks)) {
+            ctx->set_error("potrf self check: %lld of %d tickets did not run exactly once (%lld task runs)", bad,
+                           a.ntasks, tot);
+            return DPLASMA_ERR_UNEXPECTED;
+        }
     }
     if (a.trace) {
         // one line per ticket: type k m n bi bj fetched deps_met started finished cta (ns, relative)
@@ -1273,6 +1308,9 @@ int potrf_launch_prealloc(cudaStream_t st, double *dA, int mt, int nbi, int nb_u
     a.trsm_done = a.potrf_done + mt;
     a.upd_done = a.trsm_done + (size_t)mt * mt;
     a.task_count = nullptr;
+    a.ran = nullptr;
+    a.fail_potrf = -1;
+    a.skip_ticket = -1;
     a.trace = nullptr;
     a.trace_exit = nullptr;
     a.trace_cta = nullptr;

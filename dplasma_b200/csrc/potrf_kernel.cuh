@@ -92,6 +92,9 @@ struct PotrfArgs {
     int *abort_flag;       // set on failure: stop fetching tasks
     int *status;           // ST_* error word
     int *task_count;       // per-CTA executed-task counters (self check), may be null
+    int *ran;              // per-ticket run counters (self check: each must end at 1), may be null
+    int fail_potrf;        // fault injection: POTRF(fail_potrf) is reported failed when fetched (-1: none)
+    int skip_ticket;       // fault injection: this ticket is taken but neither run nor released (-1: none)
     int *diag;             // [4]: where the first failed wait gave up (site, CTA, two values)
     unsigned long long *trace; // opt-in, 4 per ticket: fetched, dependencies met, started, finished (ns); may be null
     unsigned long long *trace_exit; // 2 per CTA: producer and consumer exit times

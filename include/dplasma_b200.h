@@ -188,6 +188,21 @@ int dplasma_dplrnt(parsec_context_t *parsec, int diagdom, parsec_tiled_matrix_t 
 double dplasma_dlansy(parsec_context_t *parsec, dplasma_enum_t ntype, dplasma_enum_t uplo,
                       const parsec_tiled_matrix_t *A);
 
+/* dplasma_dlange: src/zlange_wrapper.c (dplasma_z.h:98).  dplasmaInfNorm,
+ * OneNorm, MaxNorm or FrobeniusNorm of a general matrix, computed on the GPU;
+ * returns a negative value for an unsupported norm or descriptor. */
+double dplasma_dlange(parsec_context_t *parsec, dplasma_enum_t ntype, const parsec_tiled_matrix_t *A);
+
+/* dplasma_dsymm: src/zsymm_wrapper.c (dplasma_z.h:40), the product of the
+ * reference's residual check (src/dplasma_zcheck.c:196-197).  C = alpha A B +
+ * beta C, A symmetric given by its uplo triangle.  Left side only
+ * (dplasmaRight: DPLASMA_ERR_NOT_SUPPORTED); A's tile size in 129..256, B
+ * and C of any tiling.  Returns 0, -1 / -2 for a bad side / uplo,
+ * -4 / -5 / -6 for bad shapes, or a negative code. */
+int dplasma_dsymm(parsec_context_t *parsec, dplasma_enum_t side, dplasma_enum_t uplo, double alpha,
+                  const parsec_tiled_matrix_t *A, const parsec_tiled_matrix_t *B, double beta,
+                  parsec_tiled_matrix_t *C);
+
 /* dplasma_b200_dpotrf_noalloc: no counterpart in the reference.  The lower
  * tile Cholesky of a device-resident matrix (TILE storage of the lower
  * triangle of tiles, nb a multiple of 128 and at most 512, n a multiple of nb,
@@ -196,10 +211,15 @@ double dplasma_dlansy(parsec_context_t *parsec, dplasma_enum_t ntype, dplasma_en
  * grow.  It allocates nothing: its scratch is one fixed array of about
  * 8.4 MiB in the library's device image, held on every GPU that loads the
  * library until exit; larger n is rejected with DPLASMA_ERR_INTERNAL_LIMIT.
- * Runs on `stream` (a cudaStream_t, or NULL for the default stream) of the
- * current device and returns INFO as dplasma_dpotrf does.  All calls share
- * the scratch, so calls that overlap on the GPU race; the first call on a
- * device looks the scratch up and should come before any stream capture. */
+ * Runs on `stream` (a cudaStream_t, or NULL for the default stream); the
+ * current device must hold A->mat and own the stream (else
+ * DPLASMA_ERR_ILLEGAL_VALUE).  Returns INFO as dplasma_dpotrf does.  Calls in
+ * one process are serialized: a host mutex is held and the call returns once
+ * its stream has finished, so they never overlap on the shared scratch.  The
+ * call waits for its stream and copies from host memory, so it cannot run
+ * under stream capture (DPLASMA_ERR_NOT_SUPPORTED).  The first call on a
+ * device looks up the scratch's device address.  Waits are bounded by
+ * DPLASMA_B200_WAIT_LIMIT_MS as in the other entry points. */
 int dplasma_b200_dpotrf_noalloc(void *stream, dplasma_enum_t uplo, parsec_tiled_matrix_t *A);
 
 /* ---- mixed precision ---------------------------------------------------- */
@@ -353,6 +373,38 @@ double dplasma_b200_last_factor_ms(const parsec_context_t *ctx);
 double dplasma_b200_last_solve_ms(const parsec_context_t *ctx);
 /* Number of kernel launches issued by the last public call. */
 int dplasma_b200_last_launches(const parsec_context_t *ctx);
+
+/* ---- failure detection --------------------------------------------------- */
+/* Every wait inside the device scheduler is bounded: a dependency wait gives
+ * up after `dep_ms`, a pipeline wait after `pipe_ms` milliseconds (default
+ * DPLASMA_B200_WAIT_LIMIT_MS, 4000); the kernel then stops every CTA and the
+ * call returns DPLASMA_ERR_UNEXPECTED with the site, CTA and ticket in
+ * dplasma_b200_last_error.  The context stays usable. */
+int dplasma_b200_set_wait_limits(parsec_context_t *ctx, int dep_ms, int pipe_ms);
+/* Host-side fault injection for the next factorization of this context (the
+ * reference's failure paths -- PARSEC_HOOK_RETURN_ERROR from a task body,
+ * src/zpotrf_L.jdf:136,261,390,530 -- made testable without faulting a GPU):
+ *   DPLASMA_B200_INJECT_TASK_FAILED, arg k: POTRF(k) reports failure when it
+ *     is fetched; the scheduler stops and the call returns
+ *     DPLASMA_ERR_UNEXPECTED ("task reported failed");
+ *   DPLASMA_B200_INJECT_WITHHOLD, arg i: ticket i of the ticket order is taken
+ *     but neither run nor released, so the tasks that depend on it wait until
+ *     the dependency-wait limit and the call returns DPLASMA_ERR_UNEXPECTED
+ *     ("dependency wait timed out", site recorded).
+ * The injection is consumed by that one call.  Returns 0 or
+ * DPLASMA_ERR_ILLEGAL_VALUE. */
+#define DPLASMA_B200_INJECT_NONE        0
+#define DPLASMA_B200_INJECT_TASK_FAILED 1
+#define DPLASMA_B200_INJECT_WITHHOLD    2
+int dplasma_b200_inject_fault(parsec_context_t *ctx, int kind, int arg);
+/* Scheduler self check (also DPLASMA_B200_SELFCHECK=1 at dplasma_b200_init):
+ * every factorization counts the runs of each ticket on the device and the
+ * call fails with DPLASMA_ERR_UNEXPECTED unless each ran exactly once.
+ * dplasma_b200_selfcheck reports the last factorization's tickets, task runs
+ * and tickets that did not run exactly once; it returns
+ * DPLASMA_ERR_NOT_INITIALIZED when the check is off. */
+int dplasma_b200_set_selfcheck(parsec_context_t *ctx, int on);
+int dplasma_b200_selfcheck(const parsec_context_t *ctx, long long *tickets, long long *runs, long long *bad);
 
 /* Measured FP64 tensor-core (DMMA) throughput of this GPU in TFLOP/s: a
  * register-only mma.sync.m16n8k4.f64 loop on every SM, timed with CUDA

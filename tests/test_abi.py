@@ -34,7 +34,7 @@ def test_library_exports_every_declared_symbol():
     missing = [n for n in sorted(names) if not hasattr(L, n)]
     assert not missing, missing
     # and the python binding covers them
-    assert not [n for n in names if n not in db.EXPORTS and n != "dplasma_b200_dpotrf_noalloc"]
+    assert not [n for n in names if n not in db.EXPORTS]
 
 
 def test_enum_values_match_reference_constants():
@@ -188,3 +188,11 @@ def test_python_side_refuses_without_gpu_library_context():
         pytest.skip("a GPU is present")
     with pytest.raises(RuntimeError):
         db.Context(0)
+
+
+def test_failure_hooks_check_arguments_without_a_context():
+    L = db.lib()
+    assert L.dplasma_b200_inject_fault(None, db.INJECT_TASK_FAILED, 0) == db.ERR_NOT_INITIALIZED
+    assert L.dplasma_b200_set_wait_limits(None, 10, 10) == db.ERR_NOT_INITIALIZED
+    assert L.dplasma_b200_set_selfcheck(None, 1) == db.ERR_NOT_INITIALIZED
+    assert L.dplasma_b200_selfcheck(None, None, None, None) == db.ERR_NOT_INITIALIZED
