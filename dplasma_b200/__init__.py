@@ -74,8 +74,11 @@ EXPORTS = (
     "dplasma_dtrtri", "dplasma_dlauum", "dplasma_dpotri", "dplasma_dpoinv", "dplasma_dpoinv_sync",
     "dplasma_b200_dpotri_batched", "pdpotrf_", "dplasma_b200_dpotrf_noalloc", "dplasma_b200_inject_fault",
     "dplasma_b200_set_wait_limits", "dplasma_b200_set_selfcheck", "dplasma_b200_selfcheck", "dplasma_dlange",
-    "dplasma_dsymm",
+    "dplasma_dsymm", "dplasma_b200_dtd_new", "dplasma_b200_dtd_insert", "dplasma_b200_dtd_panel_received",
+    "dplasma_b200_dtd_flush", "dplasma_b200_dtd_data_flush_all", "dplasma_b200_dtd_tiles",
+    "dplasma_b200_dtd_tickets", "dplasma_b200_dtd_destruct", "dplasma_dpotrf_dtd",
 )
+TASK_POTRF, TASK_TRSM, TASK_SYRK, TASK_GEMM = 1, 2, 3, 4
 INJECT_NONE, INJECT_TASK_FAILED, INJECT_WITHHOLD = 0, 1, 2
 
 
@@ -138,6 +141,17 @@ def lib():
     L.dplasma_dlange.restype = D
     L.dplasma_dlange.argtypes = [P, I, pd]
     L.dplasma_dsymm.argtypes = [P, I, I, D, pd, pd, D, pd]
+    L.dplasma_b200_dtd_new.restype = P
+    L.dplasma_b200_dtd_new.argtypes = [P, I, pd]
+    L.dplasma_b200_dtd_insert.argtypes = [P, I, I, I, I]
+    L.dplasma_b200_dtd_panel_received.argtypes = [P, I]
+    for f in ("dplasma_b200_dtd_flush", "dplasma_b200_dtd_data_flush_all", "dplasma_b200_dtd_destruct"):
+        getattr(L, f).argtypes = [P]
+    L.dplasma_b200_dtd_tiles.restype = P
+    L.dplasma_b200_dtd_tiles.argtypes = [P]
+    L.dplasma_b200_dtd_tickets.restype = ctypes.c_longlong
+    L.dplasma_b200_dtd_tickets.argtypes = [P]
+    L.dplasma_dpotrf_dtd.argtypes = [P, I, pd]
     L.dplasma_b200_inject_fault.argtypes = [P, I, I]
     L.dplasma_b200_set_wait_limits.argtypes = [P, I, I]
     L.dplasma_b200_set_selfcheck.argtypes = [P, I]
@@ -296,6 +310,12 @@ class Context:
     def dlansy(self, ntype: int, uplo: int, A: Desc) -> float:
         return lib().dplasma_dlansy(self.h, ntype, uplo, ctypes.byref(A))
 
+    def dpotrf_dtd(self, uplo: int, A: Desc) -> int:
+        return lib().dplasma_dpotrf_dtd(self.h, uplo, ctypes.byref(A))
+
+    def dtd(self, uplo: int, A: Desc) -> "TaskPool":
+        return TaskPool(self, uplo, A)
+
     def dlange(self, ntype: int, A: Desc) -> float:
         return lib().dplasma_dlange(self.h, ntype, ctypes.byref(A))
 
@@ -405,6 +425,49 @@ class Context:
         rc = lib().dplasma_b200_dsposv_ex(self.h, uplo, ctypes.byref(A), ctypes.byref(B), ctypes.byref(X),
                                           ctypes.byref(o), ctypes.byref(st))
         return rc, {f: getattr(st, f) for f, _ in RefineStats._fields_}
+
+
+class TaskPool:
+    """Task insertion on the tiles of one matrix (dplasma_b200_dtd_*): insert
+    POTRF / TRSM / SYRK / GEMM tile tasks in a sequential program order, flush
+    to run them on the GPU.  Keeps the descriptor alive."""
+
+    def __init__(self, ctx: Context, uplo: int, A: Desc):
+        self.ctx, self.A = ctx, A
+        self.h = lib().dplasma_b200_dtd_new(ctx.h, uplo, ctypes.byref(A))
+        if not self.h:
+            raise RuntimeError(f"dplasma_b200_dtd_new failed: {ctx.last_error()}")
+
+    def insert(self, op: int, k: int, m: int = 0, n: int = 0) -> int:
+        return lib().dplasma_b200_dtd_insert(self.h, op, k, m, n)
+
+    def panel_received(self, k: int) -> int:
+        return lib().dplasma_b200_dtd_panel_received(self.h, k)
+
+    def flush(self) -> int:
+        return lib().dplasma_b200_dtd_flush(self.h)
+
+    def data_flush_all(self) -> int:
+        return lib().dplasma_b200_dtd_data_flush_all(self.h)
+
+    def tiles(self) -> int:
+        return lib().dplasma_b200_dtd_tiles(self.h) or 0
+
+    def tickets(self) -> int:
+        return lib().dplasma_b200_dtd_tickets(self.h)
+
+    def destruct(self) -> int:
+        r = 0
+        if self.h:
+            r = lib().dplasma_b200_dtd_destruct(self.h)
+            self.h = None
+        return r
+
+    def __del__(self):
+        try:
+            self.destruct()
+        except Exception:
+            pass
 
 
 def torch_ready(*tensors):

@@ -105,7 +105,7 @@ static int check_general(const char *func, const parsec_tiled_matrix_t *B)
 static bool in_place_ok(const parsec_tiled_matrix_t *A, dplasma_enum_t uplo, const Geom &g)
 {
     return A->location == DPLASMA_B200_DEVICE && A->storage == PARSEC_MATRIX_TILE && A->uplo == dplasmaLower &&
-           uplo == dplasmaLower && g.nbi == g.nb && (g.n % g.nb) == 0 && A->lmt == g.mt;
+           uplo == dplasmaLower && g.nbi == g.nb && g.nb == A->mb && (g.n % g.nb) == 0 && A->lmt == g.mt;
 }
 
 // ---------------------------------------------------------------------------
@@ -149,6 +149,7 @@ extern "C" parsec_context_t *dplasma_b200_init(int device)
     int occs = sweep_max_blocks_per_sm();
     ctx->solve_grid = ctx->sms * (occs < 1 ? 1 : occs);
     ctx->self_check = getenv_int("DPLASMA_B200_SELFCHECK", 0) != 0;
+    ctx->trsm_inv = getenv_int("DPLASMA_B200_TRSM_INV", 0) != 0;
     if (const char *tp = getenv("DPLASMA_B200_TRACE")) snprintf(ctx->trace_path, sizeof(ctx->trace_path), "%s", tp);
     const int lim_ms = getenv_int("DPLASMA_B200_WAIT_LIMIT_MS", 4000);
     ctx->dep_limit_ns = (uint64_t)lim_ms * 1000000ull;
@@ -220,9 +221,12 @@ extern "C" double dplasma_b200_fp64_peak_tflops(parsec_context_t *p)
 // ---------------------------------------------------------------------------
 // factorization
 // ---------------------------------------------------------------------------
-static int potrf_impl(Context *ctx, dplasma_enum_t uplo, parsec_tiled_matrix_t *A, double **factor_out, Geom *gout)
+static int potrf_impl(Context *ctx, dplasma_enum_t uplo, parsec_tiled_matrix_t *A, double **factor_out, Geom *gout,
+                      int nb_tasks = 0)
 {
-    Geom g = make_geom(A->m, A->mb);
+    // nb_tasks: tile edge of the task DAG when it differs from the caller's
+    // tiles (the recursive variant's sub-tiles); 0 = the caller's
+    Geom g = make_geom(A->m, nb_tasks > 0 ? nb_tasks : A->mb);
     if (gout) *gout = g;
     if (A->m == 0) return 0;
     if (g.mt > 65535 || g.nbi > 512) {
@@ -288,17 +292,34 @@ extern "C" int dplasma_b200_taskpool_run(parsec_context_t *parsec, parsec_taskpo
 {
     if (!parsec) return DPLASMA_ERR_NOT_INITIALIZED;
     if (!tp || tp->kind != 1) return DPLASMA_ERR_ILLEGAL_VALUE;
-    const int r = dplasma_dpotrf(parsec, tp->uplo, tp->A);
+    const int r = tp->hmb > 0 ? dplasma_dpotrf_rec(parsec, tp->uplo, tp->A, tp->hmb)
+                              : dplasma_dpotrf(parsec, tp->uplo, tp->A);
     if (r < 0) return r;
     *tp->info = r;
     return 0;
 }
 
-// src/zpotrf_wrapper.c:425-451
+// src/zpotrf_wrapper.c:425-451.  The reference splits each task on an NB tile
+// into a sub-DAG on hmb x hmb sub-tiles (src/zpotrf_L.jdf:168-192, the
+// RECURSIVE bodies); the sub-tiles of every task together are the flat tile
+// algorithm with tile edge hmb, which is what runs here: the device
+// scheduler's tasks are built on hmb tiles (copied from and back to the
+// caller's NB tiles).  hmb <= 0 or hmb >= NB factors on the NB tiles.
 extern "C" int dplasma_dpotrf_rec(parsec_context_t *parsec, dplasma_enum_t uplo, parsec_tiled_matrix_t *A, int hmb)
 {
-    (void)hmb;
-    return dplasma_dpotrf(parsec, uplo, A);
+    if (uplo != dplasmaUpper && uplo != dplasmaLower) {
+        dplasma_error("dplasma_dpotrf_rec", "illegal value of uplo");
+        return -1;
+    }
+    if (!parsec) return DPLASMA_ERR_NOT_INITIALIZED;
+    int rc = check_square("dplasma_dpotrf_rec", A);
+    if (rc) return rc;
+    if (hmb <= 0 || hmb >= A->mb) return dplasma_dpotrf(parsec, uplo, A);
+    Context *ctx = &parsec->impl;
+    cudaSetDevice(ctx->device);
+    ctx->launches = 0;
+    ctx->errmsg[0] = 0;
+    return potrf_impl(ctx, uplo, A, nullptr, nullptr, hmb);
 }
 
 // ---------------------------------------------------------------------------

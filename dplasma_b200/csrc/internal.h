@@ -38,6 +38,7 @@ enum BufferId : int {
     BUF_BATCH_SCR,    // batched: per-CTA inverses of the diagonal blocks
     BUF_BATCH_W,      // batched inverse: per-CTA padded factor and L^-1
     BUF_SELFCHECK,    // per-ticket run counters (self check)
+    BUF_WX,           // second block row [Linv10 | W1] of the inverses of 256-wide diagonal tiles
     BUF_COUNT
 };
 
@@ -62,6 +63,7 @@ struct Context {
     uint64_t dep_limit_ns = 4000000000ull;   // 4 s
     uint64_t pipe_limit_ns = 4000000000ull;  // 4 s
     bool self_check = false;
+    bool trsm_inv = false;                   // DPLASMA_B200_TRSM_INV: 256-wide TRSM strips on the tile's whole inverse
     void *bufs[BUF_COUNT] = {};
     size_t bufsz[BUF_COUNT] = {};
     int task_mt = -1, task_nbs = -1, task_delay = -1, ntasks = 0;

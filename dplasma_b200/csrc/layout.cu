@@ -131,6 +131,60 @@ __global__ void from_internal_kernel(DescView dst, int uplo_upper, int n_user, i
     }
 }
 
+// Internal tiles of a different edge than the caller's (the recursive
+// variant's sub-tiles): element by element.  Internal tile (m,n) element
+// (r,c) is matrix element (i,j) = (m nb + r, n nb + c); only i >= j is moved
+// (the stored triangle), the rest of a diagonal tile is zero and the padding
+// the identity.
+__global__ void to_internal_retile_kernel(DescView src, int uplo_upper, int n_user, int nb, int nbi, int mt,
+                                          double *dA)
+{
+    int m, n;
+    tile_of_index(blockIdx.x, mt, m, n);
+    double *T = dA + (int64_t)blockIdx.x * nbi * nbi;
+    const int tm = (m == mt - 1) ? n_user - m * nb : nb;
+    const int tn = (n == mt - 1) ? n_user - n * nb : nb;
+    const int ld = view_ld(src);
+    for (int e = threadIdx.x; e < nbi * nbi; e += blockDim.x) {
+        const int r = e % nbi, c = e / nbi;
+        const int64_t i = (int64_t)m * nb + r, j = (int64_t)n * nb + c;
+        double v;
+        if (r < tm && c < tn) {
+            if (i < j) {
+                v = 0.0;
+            } else {
+                // lower storage holds (i, j); upper storage its mirror (j, i)
+                const int64_t a = uplo_upper ? j : i, b = uplo_upper ? i : j;
+                v = src.mat[view_tile_offset(src, (int)(a / src.mb), (int)(b / src.nb)) + (a % src.mb) +
+                            (b % src.nb) * ld];
+            }
+        } else {
+            v = (m == n && r == c) ? 1.0 : 0.0;
+        }
+        T[e] = v;
+    }
+}
+
+__global__ void from_internal_retile_kernel(DescView dst, int uplo_upper, int n_user, int nb, int nbi, int mt,
+                                            const double *dA)
+{
+    int m, n;
+    tile_of_index(blockIdx.x, mt, m, n);
+    const double *T = dA + (int64_t)blockIdx.x * nbi * nbi;
+    const int tm = (m == mt - 1) ? n_user - m * nb : nb;
+    const int tn = (n == mt - 1) ? n_user - n * nb : nb;
+    const int ld = view_ld(dst);
+    for (int e = threadIdx.x; e < nbi * nbi; e += blockDim.x) {
+        const int r = e % nbi, c = e / nbi;
+        const int64_t i = (int64_t)m * nb + r, j = (int64_t)n * nb + c;
+        if (r < tm && c < tn && i >= j) {
+            const int64_t a = uplo_upper ? j : i, b = uplo_upper ? i : j;
+            dst.mat[view_tile_offset(dst, (int)(a / dst.mb), (int)(b / dst.nb)) + (a % dst.mb) + (b % dst.nb) * ld] =
+                T[e];
+        }
+    }
+}
+
 static bool fast_path(const parsec_tiled_matrix_t *A, dplasma_enum_t uplo, const Geom &g)
 {
     return A->storage == PARSEC_MATRIX_TILE && A->uplo == dplasmaLower && uplo == dplasmaLower &&
@@ -153,7 +207,11 @@ int upload_sym(Context *ctx, const parsec_tiled_matrix_t *A, dplasma_enum_t uplo
         CK(cudaMemcpyAsync(src, A->mat, bytes, cudaMemcpyHostToDevice, st));
     }
     DescView v = view_of(A, src);
-    to_internal_kernel<<<(unsigned)g.ntiles(), 256, 0, st>>>(v, uplo == dplasmaUpper, g.n, g.nb, g.nbi, g.mt, dA);
+    if (g.nb != A->mb)
+        to_internal_retile_kernel<<<(unsigned)g.ntiles(), 256, 0, st>>>(v, uplo == dplasmaUpper, g.n, g.nb, g.nbi,
+                                                                        g.mt, dA);
+    else
+        to_internal_kernel<<<(unsigned)g.ntiles(), 256, 0, st>>>(v, uplo == dplasmaUpper, g.n, g.nb, g.nbi, g.mt, dA);
     CK(cudaGetLastError());
     ctx->launches++;
     return 0;
@@ -172,7 +230,12 @@ int download_sym(Context *ctx, parsec_tiled_matrix_t *A, dplasma_enum_t uplo, co
     double *dst = (double *)A->mat;
     if (A->location != DPLASMA_B200_DEVICE) dst = (double *)ctx->buffer(BUF_STAGE, 0);   // filled by upload_sym
     DescView v = view_of(A, dst);
-    from_internal_kernel<<<(unsigned)g.ntiles(), 256, 0, st>>>(v, uplo == dplasmaUpper, g.n, g.nb, g.nbi, g.mt, dA);
+    if (g.nb != A->mb)
+        from_internal_retile_kernel<<<(unsigned)g.ntiles(), 256, 0, st>>>(v, uplo == dplasmaUpper, g.n, g.nb, g.nbi,
+                                                                          g.mt, dA);
+    else
+        from_internal_kernel<<<(unsigned)g.ntiles(), 256, 0, st>>>(v, uplo == dplasmaUpper, g.n, g.nb, g.nbi, g.mt,
+                                                                   dA);
     CK(cudaGetLastError());
     ctx->launches++;
     if (A->location != DPLASMA_B200_DEVICE) CK(cudaMemcpyAsync(A->mat, dst, bytes, cudaMemcpyDeviceToHost, st));

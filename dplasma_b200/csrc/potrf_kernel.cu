@@ -379,6 +379,62 @@ __device__ __forceinline__ bool consume_job(const PotrfArgs &a, SmemCtl *ctl, co
 }
 
 // ---------------------------------------------------------------------------
+// C(128x128) = alpha A(128x128) B(128x128), column-major operands (A from
+// global memory through L2, B from global or shared memory), by the FP64
+// tensor cores; one warp per 32x32 output block.  A (B) lower triangular by
+// 32-blocks when lowA (lowB): the zero blocks of the K range are skipped.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void gemm128_tri(const double *A, int lda, bool lowA, const double *B, int ldb, bool lowB,
+                                            bool b_shared, double *C, int ldc, double alpha, int warp, int lane,
+                                            int nwarps)
+{
+    const int g = lane >> 2, t = lane & 3;
+    for (int blk = warp; blk < 16; blk += nwarps) {
+        const int bi = blk & 3, bj = blk >> 2;
+        const int l0 = lowB ? bj : 0, l1 = lowA ? bi : 3;
+        double acc[2][4][4];
+#pragma unroll
+        for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) acc[mi][ni][q] = 0.0;
+        for (int l = l0; l <= l1; ++l) {
+#pragma unroll
+            for (int kk = 0; kk < 32; kk += 4) {
+                const int kq = l * 32 + kk + t;
+                double af[2][2], bf[4];
+#pragma unroll
+                for (int mi = 0; mi < 2; ++mi) {
+                    const double *pa = A + (int64_t)kq * lda + bi * 32 + mi * 16 + g;
+                    af[mi][0] = __ldcg(pa);
+                    af[mi][1] = __ldcg(pa + 8);
+                }
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni) {
+                    const double *pb = B + (int64_t)(bj * 32 + ni * 8 + g) * ldb + kq;
+                    bf[ni] = b_shared ? *pb : __ldcg(pb);
+                }
+#pragma unroll
+                for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                    for (int ni = 0; ni < 4; ++ni) dmma_16x8x4(acc[mi][ni], af[mi][0], af[mi][1], bf[ni]);
+            }
+        }
+#pragma unroll
+        for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int r = bi * 32 + mi * 16 + g + ((q & 2) ? 8 : 0);
+                    const int c = bj * 32 + ni * 8 + 2 * t + (q & 1);
+                    C[(int64_t)c * ldc + r] = alpha * acc[mi][ni][q];
+                }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // consumers: POTRF(k) of one diagonal tile + inverses of its 128x128 diagonal
 // blocks (src/zpotrf_L.jdf:194-206 computes the factor with
 // LAPACKE_dpotrf_work; the inverses feed the TRSM jobs).
@@ -570,6 +626,21 @@ __device__ void potrf_task(const PotrfArgs &a, SmemCtl *ctl, double *ring, int k
 
     // Inverses of the 128x128 diagonal blocks from the 32x32 ones.
     assemble_w128(T, nbi, Wk, a.nbs, Sw, warp, lane, NCONS / 32, 1, NCONS);
+    if (a.nbs == 2 && a.Wx) {
+        // the off-diagonal block of the tile's inverse, Linv10 = -W1 (L10 W0),
+        // so the TRSM strips are two independent products; P = L10 W0 is kept
+        // in shared memory (the ring is free during POTRF) with a pitch of
+        // 132 doubles (= 4 mod 16: conflict-free fragment reads)
+        double *P = ring;
+        double *Wxk = a.Wx + (int64_t)k * (2 * BLK * BLK);
+        gemm128_tri(T + BLK, nbi, false, Wk, BLK, true, false, P, SP, 1.0, warp, lane, NCONS / 32);
+        named_bar_sync(1, NCONS);
+        gemm128_tri(Wk + BLK * BLK, BLK, true, P, SP, false, true, Wxk, BLK, -1.0, warp, lane, NCONS / 32);
+        // W1 beside it, so the strip's second product reads one 128 x 256 operand
+        for (int e = tid; e < BLK * BLK; e += NCONS) Wxk[BLK * BLK + e] = __ldcg(Wk + BLK * BLK + e);
+        __threadfence();
+        named_bar_sync(1, NCONS);
+    }
     phase(3);
 }
 
@@ -1050,6 +1121,13 @@ int potrf_run(Context *ctx, double *dA, int mt, int nbi, int nb_user, int n_user
         ctx->ntasks = (int)tasks.size();
     }
     double *W = (double *)ctx->buffer(BUF_W, (size_t)mt * nbs * BLK * BLK * sizeof(double));
+    // opt-in: TRSM strips of 256-wide tiles as two independent products on the
+    // tile's whole inverse (strips 84 -> 70 us, but POTRF +55 us on the
+    // critical path: no net gain at N = 32768 .. 65536)
+    double *Wx = nbs == 2 && ctx->trsm_inv
+                     ? (double *)ctx->buffer(BUF_WX, (size_t)mt * 2 * BLK * BLK * sizeof(double))
+                     : nullptr;
+    if (nbs == 2 && ctx->trsm_inv && !Wx) return DPLASMA_ERR_OUT_OF_RESOURCES;
     const size_t nctr = 8 + (size_t)mt + 2 * (size_t)mt * mt + grid;
     int *ctr = (int *)ctx->buffer(BUF_COUNTERS, nctr * sizeof(int));
     if (!W || !ctr) return DPLASMA_ERR_OUT_OF_RESOURCES;
@@ -1058,6 +1136,7 @@ int potrf_run(Context *ctx, double *dA, int mt, int nbi, int nb_user, int n_user
     PotrfArgs a;
     a.A = dA;
     a.W = W;
+    a.Wx = Wx;
     a.tasks = (const uint64_t *)ctx->buffer(BUF_TASKS, 0);
     a.ntasks = ctx->ntasks;
     a.mt = mt;
@@ -1292,6 +1371,7 @@ int potrf_launch_prealloc(cudaStream_t st, double *dA, int mt, int nbi, int nb_u
     PotrfArgs a;
     a.A = dA;
     a.W = W;
+    a.Wx = nullptr;
     a.tasks = tasks;
     a.ntasks = ntasks;
     a.mt = mt;

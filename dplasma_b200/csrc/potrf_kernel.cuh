@@ -79,6 +79,9 @@ __host__ __device__ __forceinline__ int task_bj(uint64_t t) { return (int)((t >>
 struct PotrfArgs {
     double *A;             // device tiles (lower, packed)
     double *W;             // mt * nbs blocks of 128x128: inverses of diagonal blocks
+    double *Wx;            // nbs == 2 (may be null): per diagonal tile k, the second block row of
+                           // its inverse, [Linv10 | W1] (128 x 256, column-major, ld 128),
+                           // Linv10 = -W1 L10 W0
     const uint64_t *tasks; // ticket order
     int ntasks;
     int mt, nbi, nbs;      // tiles per side, tile edge, 128-blocks per tile edge
@@ -145,7 +148,7 @@ __device__ __forceinline__ int task_njobs(const PotrfArgs &a, uint64_t t)
 {
     int ty = task_type(t);
     if (ty == T_GEMM) return 1;
-    if (ty == T_TRSM) return 2 * a.nbs - 1;
+    if (ty == T_TRSM) return (a.nbs == 2 && a.Wx) ? 2 : 2 * a.nbs - 1;
     return 0;
 }
 __device__ __forceinline__ Job task_job(const PotrfArgs &a, uint64_t t, int j)
@@ -164,6 +167,33 @@ __device__ __forceinline__ Job task_job(const PotrfArgs &a, uint64_t t, int j)
         jb.signal = false;
         jb.p16 = nullptr;
         jb.p16_scale = 1.f;
+    } else if (a.nbs == 2 && a.Wx) {
+        // TRSM strip bi of a 256-wide tile (m,k) with the whole inverse of
+        // L(k,k) = [L00 0; L10 L11]:  L^-1 = [W0 0; Linv10 W1],
+        //   X1 = A0 Linv10^T + A1 W1^T  (job 0, K = 256),   X0 = A0 W0^T  (job 1, K = 128).
+        // The two jobs are independent; X1 goes first since it reads A0,
+        // which X0 then overwrites (X1 writes only the columns X0 never reads).
+        const int p = 1 - j;
+        double *Amk = tile_ptr(a, m, k);
+        jb.A = Amk + bi * BLK; jb.lda = nbi;
+        jb.C = Amk + (int64_t)p * BLK * nbi + bi * BLK; jb.ldc = nbi;
+        jb.ldb = BLK;
+        if (p == 1) {
+            jb.B = a.Wx + (int64_t)k * (2 * BLK * BLK);     // [Linv10 | W1]
+            jb.K = 2 * BLK;
+        } else {
+            jb.B = wblk_ptr(a, k, 0);
+            jb.K = BLK;
+        }
+        jb.mode = J_STORE;
+        jb.signal = false;
+        jb.p16 = nullptr;
+        jb.p16_scale = 1.f;
+        if (a.P16) {
+            const int64_t row0 = lower_tile_index(m, k, a.mt) * nbi + bi * BLK;
+            jb.p16 = reinterpret_cast<unsigned short *>(a.P16) + row0 * nbi + p * BLK;
+            jb.p16_scale = a.scl[m * a.nbs + bi];
+        }
     } else {
         // TRSM strip bi of tile (m,k): X = A L^{-T} (src/zpotrf_L.jdf:330-333),
         // block-left-looking: jobs  [STORE p=0] [SUB p=1] [STORE p=1] ...

@@ -149,8 +149,12 @@ void dplasma_dpotrf_Destruct(parsec_taskpool_t *tp);
 int dplasma_b200_taskpool_run(parsec_context_t *parsec, parsec_taskpool_t *tp);
 
 /* dplasma_dpotrf_rec / _setrecursive: src/zpotrf_wrapper.c:425-451
- * (dplasma_z.h:83, 273).  The hierarchical split of the reference is subsumed
- * by the device scheduler; hmb is validated and otherwise ignored. */
+ * (dplasma_z.h:83, 273).  With 0 < hmb < NB the tasks of the factorization
+ * run on hmb x hmb sub-tiles (the reference's recursive bodies split each NB
+ * tile task into a sub-DAG on hmb tiles, src/zpotrf_L.jdf:168-192; together
+ * they are the tile algorithm with tile edge hmb); the caller's NB tiles are
+ * copied to and from that layout.  Otherwise the same as dplasma_dpotrf.
+ * _setrecursive sets hmb for a taskpool made by dplasma_dpotrf_New. */
 int dplasma_dpotrf_rec(parsec_context_t *parsec, dplasma_enum_t uplo, parsec_tiled_matrix_t *A, int hmb);
 void dplasma_dpotrf_setrecursive(parsec_taskpool_t *tp, int hmb);
 
@@ -187,6 +191,51 @@ int dplasma_dplrnt(parsec_context_t *parsec, int diagdom, parsec_tiled_matrix_t 
  * returns a negative value for an unsupported norm or descriptor. */
 double dplasma_dlansy(parsec_context_t *parsec, dplasma_enum_t ntype, dplasma_enum_t uplo,
                       const parsec_tiled_matrix_t *A);
+
+/* ---- task insertion (the DTD front-end) ---------------------------------- */
+/* The counterpart of dplasma's DTD Cholesky (src/dtd_wrappers/zpotrf.c and
+ * the insertion loop of tests/testing_zpotrf_dtd.c:125-200): the caller
+ * inserts the tile tasks of a lower Cholesky in a sequential program order and
+ * flushes; each flush runs the tasks inserted since the last one as one
+ * launch of the device scheduler, in insertion order, with dependency
+ * counters that persist across flushes.  An insertion whose dependencies have
+ * not all been inserted before it is refused (DPLASMA_ERR_ILLEGAL_VALUE), so
+ * every flush completes.  A: lower descriptor (device-resident lower TILE
+ * storage with nb a multiple of 128 dividing n is used in place; any other
+ * layout is copied to the device by _new and written back by
+ * _data_flush_all).  Tasks (indices of tiles):
+ *   POTRF k       A(k,k) = chol(A(k,k))
+ *   TRSM  k, m    A(m,k) = A(m,k) A(k,k)^-T            m > k
+ *   SYRK  k, m    A(m,m) -= A(m,k) A(m,k)^T             m > k
+ *   GEMM  k, m, n A(m,n) -= A(m,k) A(n,k)^T             m > n > k */
+#define DPLASMA_B200_TASK_POTRF 1
+#define DPLASMA_B200_TASK_TRSM  2
+#define DPLASMA_B200_TASK_SYRK  3
+#define DPLASMA_B200_TASK_GEMM  4
+typedef struct dplasma_b200_dtd_s dplasma_b200_dtd_t;
+dplasma_b200_dtd_t *dplasma_b200_dtd_new(parsec_context_t *parsec, dplasma_enum_t uplo, parsec_tiled_matrix_t *A);
+/* Insert one task (m, n ignored where the task has no such index). */
+int dplasma_b200_dtd_insert(dplasma_b200_dtd_t *tp, int op, int k, int m, int n);
+/* Tile column k was factored elsewhere (POTRF(k) and TRSM(:,k) by another
+ * process) and its tiles copied into this matrix: later tasks may use it. */
+int dplasma_b200_dtd_panel_received(dplasma_b200_dtd_t *tp, int k);
+/* Run the pending tasks and wait: 0, INFO > 0, or a negative code. */
+int dplasma_b200_dtd_flush(dplasma_b200_dtd_t *tp);
+/* Flush, then write the tiles back to A when the pool works on a copy
+ * (parsec_dtd_data_flush_all). */
+int dplasma_b200_dtd_data_flush_all(dplasma_b200_dtd_t *tp);
+/* Device address of the tile storage the pool works on (lower tiles packed
+ * by columns, tile edge nb rounded up to a multiple of 128). */
+void *dplasma_b200_dtd_tiles(dplasma_b200_dtd_t *tp);
+/* Tickets (scheduler tasks) launched so far. */
+long long dplasma_b200_dtd_tickets(const dplasma_b200_dtd_t *tp);
+/* Free the pool; returns its INFO (or its first error). */
+int dplasma_b200_dtd_destruct(dplasma_b200_dtd_t *tp);
+/* dplasma_dpotrf through the task-insertion front-end (the reference's
+ * testing_zpotrf_dtd flow): inserts POTRF, TRSM, SYRK, GEMM of every step in
+ * the reference's order and flushes once.  Lower only (dplasmaUpper:
+ * DPLASMA_ERR_NOT_SUPPORTED).  Returns INFO as dplasma_dpotrf. */
+int dplasma_dpotrf_dtd(parsec_context_t *parsec, dplasma_enum_t uplo, parsec_tiled_matrix_t *A);
 
 /* dplasma_dlange: src/zlange_wrapper.c (dplasma_z.h:98).  dplasmaInfNorm,
  * OneNorm, MaxNorm or FrobeniusNorm of a general matrix, computed on the GPU;
