@@ -364,6 +364,32 @@ def bench_fp64_sweep(ctx, db, torch, peak64, sizes=(16384, 32768, 65536), nbs=(2
     return out
 
 
+def retile_lower(torch, src, n, nb_src, nb_dst, dst):
+    """Copy a matrix held as packed lower tiles of edge nb_src (column-major
+    tiles) into packed lower tiles of edge nb_dst = r * nb_src (data movement
+    on the device; the upper part of the destination's diagonal tiles is left
+    zero).  Used to run the FP64 comparison at its fastest tile size on the
+    same matrix."""
+    r = nb_dst // nb_src
+    mts, mtd = n // nb_src, n // nb_dst
+    S = src.view(-1, nb_src, nb_src)                 # [tile][col][row]
+    D = dst.view(-1, r, nb_src, r, nb_src)           # [tile][col block][col][row block][row]
+    D.zero_()
+    for Nd in range(mtd):
+        for j in range(r):
+            c = Nd * r + j                           # source tile column
+            for i in range(r):
+                # destination tiles (Md, Nd), source tile row Md*r + i; on the
+                # diagonal tile only the sub-tiles with i >= j are stored
+                Md = torch.arange(Nd if i >= j else Nd + 1, mtd, device=src.device)
+                if Md.numel() == 0:
+                    continue
+                ms = Md * r + i
+                sidx = c * mts - (c * (c - 1)) // 2 + (ms - c)
+                didx = Nd * mtd - (Nd * (Nd - 1)) // 2 + (Md - Nd)
+                D[didx, j, :, i, :] = S[sidx]
+
+
 def max_over_ranks(ms, dist, device):
     """The slowest rank's time: every rank contributes its own device-timed
     ms and all receive the max (the contract's max-over-ranks); one process
@@ -414,21 +440,39 @@ def run_gpu(args):
     peak64 = ctx.fp64_peak_tflops()
     peaks = measured_peaks()
 
+    A64_stale = [True]
+
     def generate(kappa):
         db.attach(dA, A_pristine)
         rc = ctx.dplgsy_cond(kappa, 64, db.Lower, dA, 7)
         db.attach(dA, A)
+        A64_stale[0] = True
         if rc != 0:
             raise RuntimeError(f"dplgsy_cond rc={rc}: {ctx.last_error()}")
 
+    # the FP64 comparison runs at its fastest tile size (NB=512 on this GPU)
+    # on the same matrix, re-tiled on the device
+    nb64 = args.fp64_nb if (args.fp64_nb % NB == 0 and N % args.fp64_nb == 0) else NB
+    if nb64 != NB:
+        dA64 = db.desc_sym(N, nb64, db.Lower)
+        A64_pristine, A64 = dev_buf(dA64), dev_buf(dA64)
+        db.attach(dA64, A64)
+    else:
+        dA64, A64 = dA, A
+
     def fp64_solve():
         """plain FP64 dposv on fresh copies; returns (ms, solution)"""
-        A.copy_(A_pristine)
+        if nb64 != NB:
+            retile_lower(torch, A_pristine, N, NB, nb64, A64_pristine) if A64_stale[0] else None
+            A64_stale[0] = False
+            A64.copy_(A64_pristine)
+        else:
+            A.copy_(A_pristine)
         B.copy_(B_pristine)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        info = ctx.dposv(db.Lower, dA, dB)
+        info = ctx.dposv(db.Lower, dA64, dB)
         e1.record()
         torch.cuda.synchronize()
         if info != 0:
@@ -547,6 +591,8 @@ def run_gpu(args):
     a_gb = A.numel() * 8 / 1e9
     fp64_sweep = None
     if args.fp64_sweep:
+        if nb64 != NB:
+            del A64_pristine, A64
         del A, B
         torch.cuda.empty_cache()
         fp64_sweep = bench_fp64_sweep(ctx, db, torch, peak64)
@@ -592,7 +638,7 @@ def run_gpu(args):
         "mixed_backward_error": max(st["backward_error"] for st in stats),
         "mixed_forward_error_vs_fp64": mixed_fwd, "mixed_fallback": max(st["fallback"] for st in stats),
         "mixed_factor_ms": fac_ms, "mixed_check_daxmb": ratio_mixed,
-        "fp64": {"dposv_ms": fp64_ms, "tflops": posv_flops(N, NRHS) / (fp64_ms * 1e-3) / 1e12,
+        "fp64": {"nb": nb64, "dposv_ms": fp64_ms, "tflops": posv_flops(N, NRHS) / (fp64_ms * 1e-3) / 1e12,
                  "dpotrf_ms": fac64, "dpotrs_ms": statistics.median(r[3] for r in fp64),
                  "speedup_of_mixed": fp64_ms / ms_step, "check_daxmb": ratio64},
         "fp64_sweep": fp64_sweep,
@@ -630,6 +676,8 @@ def main():
     p.add_argument("--n", type=int, default=65536)
     p.add_argument("--nb", type=int, default=256)
     p.add_argument("--nrhs", type=int, default=16)
+    p.add_argument("--fp64-nb", type=int, default=512,
+                   help="tile size of the plain FP64 comparison (a multiple of --nb dividing N)")
     p.add_argument("--e2e-steps", type=int, default=2)
     p.add_argument("--cpu-n", type=int, default=16384)
     p.add_argument("--no-cpu", action="store_true")

@@ -69,6 +69,7 @@ struct Context {
     int task_mt = -1, task_nbs = -1, task_delay = -1, ntasks = 0;
     int task_mixed = 0;                      // chunk size of the cached mixed task list (0: FP64 list)
     int mx_chunk = 0;                        // panels per mixed-precision update task (0: by operand form)
+    int mx_block_w = 0, mx_block_h = 0;      // blocked order of the mixed update tasks (tile columns x rows; 0: by columns)
     double last_factor_ms = 0.0, last_solve_ms = 0.0;
     int launches = 0;
     long long last_tasks_executed = 0;

@@ -999,7 +999,44 @@ std::vector<uint64_t> build_potrf_tasks(int mt, int nbs, int delay)
 // always issued by step n-2, before its own critical step).  Step k: the
 // critical column k+1, POTRF(k+1), `delay` tasks of the step's share,
 // TRSM(*,k+1), the rest of the share.
-std::vector<uint64_t> build_potrf_tasks_mixed(int mt, int nbs, int delay, int S)
+// Order of one step's share of update tasks (all independent: one chunk per
+// tile) in blocks of bw tile columns x bh tile rows, so that the 16-bit panel
+// operands of a block (bh row sets and bw column sets of S panels) stay in L2
+// while the block's tasks reuse them; bw = 0 keeps the column order.
+static void block_share(std::vector<uint64_t> &v, int bw, int bh)
+{
+    if (bw <= 0 || bh <= 0 || v.size() < 2) return;
+    std::vector<uint64_t> out;
+    out.reserve(v.size());
+    size_t i = 0;
+    while (i < v.size()) {
+        // columns of this group: the next bw distinct n (tasks come by column)
+        const size_t g0 = i;
+        int ncols = 0, lastn = -1;
+        while (i < v.size()) {
+            const int n = task_n(v[i]);
+            if (n != lastn) {
+                if (ncols == bw) break;
+                ++ncols;
+                lastn = n;
+            }
+            ++i;
+        }
+        int mmin = 1 << 30, mmax = -1;
+        for (size_t j = g0; j < i; ++j) {
+            mmin = std::min(mmin, task_m(v[j]));
+            mmax = std::max(mmax, task_m(v[j]));
+        }
+        for (int mb = mmin; mb <= mmax; mb += bh)
+            for (size_t j = g0; j < i; ++j) {
+                const int m = task_m(v[j]);
+                if (m >= mb && m < mb + bh) out.push_back(v[j]);
+            }
+    }
+    v.swap(out);
+}
+
+std::vector<uint64_t> build_potrf_tasks_mixed(int mt, int nbs, int delay, int S, int bw = 0, int bh = 0)
 {
     std::vector<uint64_t> v;
     auto push_trsm = [&](int k) {
@@ -1020,6 +1057,7 @@ std::vector<uint64_t> build_potrf_tasks_mixed(int mt, int nbs, int delay, int S)
             done += mt - n;
         }
     }
+    for (auto &sh : share) block_share(sh, bw, bh);
     v.push_back(make_task(T_POTRF, 0, 0, 0, 0, 0));
     push_trsm(0);
     for (int k = 0; k + 1 < mt; ++k) {
@@ -1109,7 +1147,8 @@ int potrf_run(Context *ctx, double *dA, int mt, int nbi, int nb_user, int n_user
     // and take 16 (same refinement steps as 8, 15% faster factorization)
     const int chunk = !mixed ? 0 : (ctx->mx_chunk > 0 ? ctx->mx_chunk : (p16_fmt == 2 ? 8 : 16));
     if (ctx->task_mt != mt || ctx->task_nbs != nbs || ctx->task_delay != ctx->potrf_delay || ctx->task_mixed != chunk) {
-        std::vector<uint64_t> tasks = mixed ? build_potrf_tasks_mixed(mt, nbs, ctx->potrf_delay, chunk)
+        std::vector<uint64_t> tasks = mixed ? build_potrf_tasks_mixed(mt, nbs, ctx->potrf_delay, chunk, ctx->mx_block_w,
+                                                                      ctx->mx_block_h)
                                             : build_potrf_tasks(mt, nbs, ctx->potrf_delay);
         uint64_t *dt = (uint64_t *)ctx->buffer(BUF_TASKS, tasks.size() * sizeof(uint64_t));
         if (!dt) return DPLASMA_ERR_OUT_OF_RESOURCES;
@@ -1428,6 +1467,14 @@ int potrf_launch_prealloc(cudaStream_t st, double *dA, int mt, int nbi, int nb_u
 // launch, so host tests can replay the dependency rules on the CPU.  Returns
 // the number of tasks (those beyond `cap` are not written).
 // ---------------------------------------------------------------------------
+extern "C" int dplasma_b200_debug_task_list_blocked(int mixed_chunk, int mt, int nbs, int delay, int bw, int bh,
+                                                    unsigned long long *out, int cap)
+{
+    const std::vector<uint64_t> v = db2::build_potrf_tasks_mixed(mt, nbs, delay, mixed_chunk, bw, bh);
+    for (size_t i = 0; i < v.size() && (int)i < cap; ++i) out[i] = v[i];
+    return (int)v.size();
+}
+
 extern "C" int dplasma_b200_debug_task_list(int mixed_chunk, int mt, int nbs, int delay, unsigned long long *out,
                                             int cap)
 {

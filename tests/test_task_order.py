@@ -83,3 +83,22 @@ def test_mixed_steps_share_update_work():
     for a, b in zip(potrf_pos[S:mt - 3 * S], potrf_pos[S + 1:mt - 3 * S + 1]):
         between = [t for t in tl[a:b] if t[0] == T_GEMM and t[3] != tl[b][1]]
         assert len(between) > 0
+
+
+def tasks_blocked(chunk, mt, nbs, delay, bw, bh):
+    L = db.lib()
+    f = L.dplasma_b200_debug_task_list_blocked
+    f.argtypes = [ctypes.c_int] * 6 + [ctypes.c_void_p, ctypes.c_int]
+    n = f(chunk, mt, nbs, delay, bw, bh, None, 0)
+    out = np.zeros(n, dtype=np.uint64)
+    assert f(chunk, mt, nbs, delay, bw, bh, out.ctypes.data, n) == n
+    return [(int(t) & 0xF, (int(t) >> 4) & 0xFFFF, (int(t) >> 20) & 0xFFFF, (int(t) >> 36) & 0xFFFF,
+             (int(t) >> 52) & 0xF, (int(t) >> 56) & 0xF) for t in out]
+
+
+@pytest.mark.parametrize("mt,S,bw,bh", [(33, 4, 4, 8), (65, 8, 4, 32), (65, 8, 1, 1), (40, 3, 7, 5)])
+def test_mixed_blocked_ticket_order(mt, S, bw, bh):
+    # the blocked order permutes each step's share: same tasks, same dependency guarantees
+    tl = tasks_blocked(S, mt, 2, 444, bw, bh)
+    replay(tl, mt, 2, S)
+    assert sorted(tl) == sorted(tasks(S, mt, 2, 444))
