@@ -128,6 +128,7 @@ extern "C" parsec_context_t *dplasma_b200_init(int device)
     Context *ctx = &p->impl;
     ctx->device = device;
     if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess ||
         cudaEventCreate(&ctx->ev2) != cudaSuccess || cudaEventCreate(&ctx->ev3) != cudaSuccess) {
         dplasma_error("dplasma_b200_init", cudaGetErrorString(cudaGetLastError()));
@@ -149,6 +150,9 @@ extern "C" parsec_context_t *dplasma_b200_init(int device)
     // at N=65536)
     ctx->mx_block_w = getenv_int("DPLASMA_B200_MX_BLOCK_W", 8);
     ctx->mx_block_h = getenv_int("DPLASMA_B200_MX_BLOCK_H", 32);
+    ctx->stream_cb = getenv_int("DPLASMA_B200_STREAM_CB", 16);
+    ctx->no_stream = getenv_int("DPLASMA_B200_NO_STREAM", 0) != 0;
+    ctx->stream_trace = getenv_int("DPLASMA_B200_STREAM_TRACE", 0) != 0;
     ctx->potrf_delay = getenv_int("DPLASMA_B200_DELAY", 3 * ctx->potrf_grid);
     ctx->wave_occ = getenv_int("DPLASMA_B200_NO_WAVE", 0) ? 0 : wave_max_blocks_per_sm();
     int occs = sweep_max_blocks_per_sm();
@@ -176,6 +180,8 @@ extern "C" void dplasma_b200_fini(parsec_context_t **pctx)
     cudaEventDestroy(ctx->ev1);
     cudaEventDestroy(ctx->ev2);
     cudaEventDestroy(ctx->ev3);
+    cudaStreamSynchronize(ctx->copy_stream);
+    cudaStreamDestroy(ctx->copy_stream);
     cudaStreamDestroy(ctx->stream);
     delete *pctx;
     *pctx = nullptr;
@@ -679,7 +685,18 @@ extern "C" int dplasma_b200_dsposv_ex(parsec_context_t *parsec, dplasma_enum_t u
     double *A0 = inplace ? (double *)A->mat : (double *)ctx->buffer(BUF_A0, g.elems() * sizeof(double));
     double *L = (double *)ctx->buffer(BUF_A, g.elems() * sizeof(double));
     if (!A0 || !L) return DPLASMA_ERR_OUT_OF_RESOURCES;
-    if (!inplace && (rc = upload_sym(ctx, A, uplo, g, A0))) return rc;
+    // a host matrix in pinned memory that already has the device tile layout
+    // is streamed in while the factorization runs (phases of tile columns)
+    const double *stream_src = nullptr;
+    if (!inplace && !ctx->no_stream && A->location == DPLASMA_B200_HOST && A->storage == PARSEC_MATRIX_TILE &&
+        A->uplo == dplasmaLower && uplo == dplasmaLower && A->mb == A->nb && g.nbi == g.nb && g.n % g.nb == 0 &&
+        A->lmt == g.mt) {
+        cudaPointerAttributes pa;
+        if (cudaPointerGetAttributes(&pa, A->mat) == cudaSuccess && pa.type == cudaMemoryTypeHost)
+            stream_src = (const double *)A->mat;
+        cudaGetLastError();
+    }
+    if (!inplace && !stream_src && (rc = upload_sym(ctx, A, uplo, g, A0))) return rc;
     const int nrhs_pad = ((B->n + 7) / 8) * 8;
     const int npad = g.mt * g.nbi;
     double *b = (double *)ctx->buffer(BUF_B0, (size_t)npad * nrhs_pad * sizeof(double));
@@ -695,7 +712,7 @@ extern "C" int dplasma_b200_dsposv_ex(parsec_context_t *parsec, dplasma_enum_t u
     ro.bwd_factor = o.bwdmax;
     ro.escalate = o.escalate != 0;
     RefineStats st;
-    rc = refine_solve(ctx, A0, L, g, b, x, npad, nrhs_pad, ro, st);
+    rc = refine_solve(ctx, A0, L, g, b, x, npad, nrhs_pad, ro, st, stream_src);
     if (stats) {
         stats->iter = st.iter;
         stats->inner_iters = st.inner_iters;

@@ -8,6 +8,8 @@
 #include <stdint.h>
 #include <stdio.h>
 
+#include <vector>
+
 #include "../../include/dplasma_b200.h"
 
 namespace db2 {
@@ -39,6 +41,7 @@ enum BufferId : int {
     BUF_BATCH_W,      // batched inverse: per-CTA padded factor and L^-1
     BUF_SELFCHECK,    // per-ticket run counters (self check)
     BUF_WX,           // second block row [Linv10 | W1] of the inverses of 256-wide diagonal tiles
+    BUF_TASKS_PH,     // phased ticket order of the streamed factorization
     BUF_COUNT
 };
 
@@ -54,6 +57,7 @@ struct Context {
     int device = 0;
     int sms = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t copy_stream = nullptr;      // host -> device copies that overlap the factorization
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr, ev3 = nullptr;
     int potrf_grid = 0;
     int potrf_grid_mixed = 0;
@@ -70,6 +74,11 @@ struct Context {
     int task_mixed = 0;                      // chunk size of the cached mixed task list (0: FP64 list)
     int mx_chunk = 0;                        // panels per mixed-precision update task (0: by operand form)
     int mx_block_w = 0, mx_block_h = 0;      // blocked order of the mixed update tasks (tile columns x rows; 0: by columns)
+    int stream_cb = 0;                       // tile columns per phase of the streamed factorization (0: 16)
+    bool no_stream = false;                  // DPLASMA_B200_NO_STREAM: upload host matrices before factoring
+    bool stream_trace = false;               // DPLASMA_B200_STREAM_TRACE: print the streamed phases' timeline
+    int ph_mt = -1, ph_chunk = -1, ph_cb = -1, ph_delay = -1;   // cached phased ticket order
+    std::vector<long long> ph_off;
     double last_factor_ms = 0.0, last_solve_ms = 0.0;
     int launches = 0;
     long long last_tasks_executed = 0;
@@ -132,6 +141,10 @@ int potrf_device(Context *ctx, double *dA, int mt, int nbi, int nb_user, int n_u
 // p16_fmt < 0: FP64 updates; 0/1/2: FP16/BF16/split-FP16 tensor-core updates (nbi == 256)
 int potrf_run(Context *ctx, double *dA, int mt, int nbi, int nb_user, int n_user, int *info, int p16_fmt);
 int potrf_max_blocks_per_sm(bool mixed);
+// mixed factorization of a host matrix (pinned, device tile layout) streamed in
+// by tile-column phases on the copy stream, overlapping the factorization
+int potrf_run_streamed(Context *ctx, const double *hA, double *A0, double *L, int mt, int nbi, int nb_user,
+                       int n_user, int *info, int p16_fmt);
 int encode_map_2d(Context *ctx, CUtensorMap *map, CUtensorMapDataType type, void *base, uint64_t dim0, uint64_t dim1,
                   uint64_t stride1, uint32_t box0, uint32_t box1, CUtensorMapSwizzle swz);
 
@@ -165,8 +178,10 @@ struct RefineStats {
     int iter = 0, inner_iters = 0, fallback = 0, solver_used = 0, fmt_used = 0;
     double backward_error = 0.0, factor_ms = 0.0, refine_ms = 0.0, anorm = 0.0;
 };
+// hostA (may be null): the matrix in pinned host memory in the device tile
+// layout, streamed into A0 and L while the factorization runs
 int refine_solve(Context *ctx, const double *A0, double *L, const Geom &g, double *b, double *x, int npad, int nc,
-                 const RefineOpts &o, RefineStats &st);
+                 const RefineOpts &o, RefineStats &st, const double *hostA = nullptr);
 int generate_cond(Context *ctx, double *dA, const Geom &g, double kappa, int nrefl, unsigned long long seed);
 int symm_tiles(Context *ctx, const double *dA, const Geom &g, const double *in, int ldin, double *out, int ldout,
                int ncols, double alpha, int *status);

@@ -1073,6 +1073,74 @@ std::vector<uint64_t> build_potrf_tasks_mixed(int mt, int nbs, int delay, int S,
     return v;
 }
 
+// Mixed-precision ticket order in phases of CB tile columns (CB a multiple
+// of S), for a matrix whose tile columns arrive over time: phase p touches
+// only tile columns [c0, c1) = [p CB, p CB + CB) and earlier ones, so it can
+// run as soon as those columns are on the device.  A phase first applies to
+// its columns every chunk closed in earlier phases (catch-up, chunk by chunk
+// so the tiles of a column proceed in parallel), then runs the steps k of
+// its own columns as the single-launch order does, with updates restricted
+// to the phase's columns; the later columns receive those chunks in their
+// own phase.  Each phase is a topological segment: every ticket depends only
+// on tickets of earlier phases or earlier in its own.
+std::vector<std::vector<uint64_t>> build_potrf_tasks_mixed_phased(int mt, int nbs, int delay, int S, int CB, int bw,
+                                                                  int bh)
+{
+    std::vector<std::vector<uint64_t>> phases;
+    if (mt <= 0 || S <= 0 || CB <= 0 || CB % S) return phases;
+    for (int c0 = 0; c0 < mt; c0 += CB) {
+        const int c1 = std::min(mt, c0 + CB);
+        std::vector<uint64_t> v;
+        auto push_trsm = [&](int k) {
+            for (int m = k + 1; m < mt; ++m)
+                for (int bi = 0; bi < nbs; ++bi) v.push_back(make_task(T_TRSM, k, m, k, bi, 0));
+        };
+        auto catch_up = [&](int n) {   // every chunk closed before c0, for tile column n
+            for (int c = 0; c < c0 / S; ++c)
+                for (int m = n; m < mt; ++m) v.push_back(make_task(T_GEMM, c, m, n, 0, 0));
+        };
+        // share[k - c0]: in-phase update tasks issued in step k
+        std::vector<std::vector<uint64_t>> share(c1 - c0);
+        for (int c = c0 / S; c * S + S - 1 < c1; ++c) {
+            const int k = c * S + S - 1;
+            long long work = 0;
+            for (int n = k + 2; n < c1; ++n) work += mt - n;
+            long long done = 0;
+            for (int n = k + 2; n < c1; ++n) {
+                int part = (int)((done * S) / (work > 0 ? work : 1));
+                part = std::min(part, std::min(S - 1, n - 2 - k));
+                for (int m = n; m < mt; ++m) share[k + part - c0].push_back(make_task(T_GEMM, c, m, n, 0, 0));
+                done += mt - n;
+            }
+        }
+        for (auto &sh : share) block_share(sh, bw, bh);
+        catch_up(c0);
+        v.push_back(make_task(T_POTRF, c0, c0, c0, 0, 0));
+        push_trsm(c0);
+        // the other columns chunk by chunk, each chunk's tiles in blocks (L2
+        // reuse of the 16-bit panels across the block's columns)
+        for (int c = 0; c < c0 / S; ++c) {
+            std::vector<uint64_t> ch;
+            for (int n = c0 + 1; n < c1; ++n)
+                for (int m = n; m < mt; ++m) ch.push_back(make_task(T_GEMM, c, m, n, 0, 0));
+            block_share(ch, bw, bh);
+            v.insert(v.end(), ch.begin(), ch.end());
+        }
+        for (int k = c0; k + 1 < c1; ++k) {
+            const int c = k / S;
+            for (int m = k + 1; m < mt; ++m) v.push_back(make_task(T_GEMM, c, m, k + 1, 0, 0));
+            v.push_back(make_task(T_POTRF, k + 1, k + 1, k + 1, 0, 0));
+            const std::vector<uint64_t> &rest = share[k - c0];
+            const size_t d = std::min<size_t>(rest.size(), (size_t)std::max(delay, 0));
+            v.insert(v.end(), rest.begin(), rest.begin() + d);
+            push_trsm(k + 1);
+            v.insert(v.end(), rest.begin() + d, rest.end());
+        }
+        phases.push_back(std::move(v));
+    }
+    return phases;
+}
+
 // ---------------------------------------------------------------------------
 // host: run one factorization of the device tiles
 // ---------------------------------------------------------------------------
@@ -1332,6 +1400,184 @@ int potrf_run(Context *ctx, double *dA, int mt, int nbi, int nb_user, int n_user
     return 0;
 }
 
+// ---------------------------------------------------------------------------
+// host: the mixed-precision factorization of a matrix streamed from pinned
+// host memory (lower tiles already in the device layout).  The tile columns
+// are copied in phases of cb columns on the context's copy stream into A0
+// (the untouched copy the refinement reads); phase p of the phased ticket
+// order runs as soon as its columns are on the device: the compute stream
+// waits for the copy stream's event of that phase, copies the phase's tiles
+// into L (the working copy) and launches the phase, so the host copies of
+// the next phases overlap the factorization of this one and no kernel ever
+// waits for a copy.  The diagonal tiles go first, for the 16-bit scales.
+// Dependency counters carry over from phase to phase; only the ticket
+// counter restarts.  DPLASMA_B200_STREAM_TRACE=1 prints the timeline.
+// ---------------------------------------------------------------------------
+int potrf_run_streamed(Context *ctx, const double *hA, double *A0, double *L, int mt, int nbi, int nb_user,
+                       int n_user, int *info, int p16_fmt)
+{
+    const int nbs = nbi / BLK;
+    cudaStream_t st = ctx->stream, cs = ctx->copy_stream;
+    const int grid = ctx->potrf_grid_mixed;
+    if (nbi != MX_NB || p16_fmt < 0 || p16_fmt > 2 || !cs || grid <= 0) {
+        ctx->set_error("streamed factorization: unsupported configuration");
+        return DPLASMA_ERR_NOT_SUPPORTED;
+    }
+    const int chunk = ctx->mx_chunk > 0 ? ctx->mx_chunk : (p16_fmt == 2 ? 8 : 16);
+    int cb = ctx->stream_cb > 0 ? ctx->stream_cb : 16;
+    cb = ((std::max(cb, chunk) + chunk - 1) / chunk) * chunk;
+    if (ctx->ph_mt != mt || ctx->ph_chunk != chunk || ctx->ph_cb != cb || ctx->ph_delay != ctx->potrf_delay) {
+        const auto ph = build_potrf_tasks_mixed_phased(mt, nbs, ctx->potrf_delay, chunk, cb, ctx->mx_block_w,
+                                                       ctx->mx_block_h);
+        std::vector<uint64_t> all;
+        ctx->ph_off.assign(1, 0);
+        for (const auto &v : ph) {
+            all.insert(all.end(), v.begin(), v.end());
+            ctx->ph_off.push_back((long long)all.size());
+        }
+        uint64_t *dt = (uint64_t *)ctx->buffer(BUF_TASKS_PH, all.size() * sizeof(uint64_t));
+        if (!dt) return DPLASMA_ERR_OUT_OF_RESOURCES;
+        CK(cudaMemcpyAsync(dt, all.data(), all.size() * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+        CK(cudaStreamSynchronize(st));
+        ctx->ph_mt = mt;
+        ctx->ph_chunk = chunk;
+        ctx->ph_cb = cb;
+        ctx->ph_delay = ctx->potrf_delay;
+    }
+    const int nph = (int)ctx->ph_off.size() - 1;
+    double *W = (double *)ctx->buffer(BUF_W, (size_t)mt * nbs * BLK * BLK * sizeof(double));
+    const size_t nctr = 8 + (size_t)mt + 2 * (size_t)mt * mt + grid;
+    int *ctr = (int *)ctx->buffer(BUF_COUNTERS, nctr * sizeof(int));
+    if (!W || !ctr) return DPLASMA_ERR_OUT_OF_RESOURCES;
+
+    PotrfArgs a;
+    memset(&a, 0, sizeof(a));
+    a.A = L;
+    a.W = W;
+    a.Wx = nullptr;
+    a.mt = mt;
+    a.nbi = nbi;
+    a.nbs = nbs;
+    a.nb_user = nb_user;
+    a.n_user = n_user;
+    a.ticket = ctr + 0;
+    a.info = ctr + 1;
+    a.abort_flag = ctr + 2;
+    a.status = ctr + 3;
+    a.diag = ctr + 4;
+    a.potrf_done = ctr + 8;
+    a.trsm_done = a.potrf_done + mt;
+    a.upd_done = a.trsm_done + (size_t)mt * mt;
+    a.task_count = a.upd_done + (size_t)mt * mt;
+    a.fail_potrf = -1;
+    a.skip_ticket = -1;
+    a.dep_limit_ns = ctx->dep_limit_ns;
+    a.pipe_limit_ns = ctx->pipe_limit_ns;
+    const bool split = p16_fmt == 2;
+    const size_t ntl = (size_t)mt * (mt + 1) / 2;
+    const size_t rows = ntl * (size_t)nbi;
+    const size_t pbytes = (split ? 2 : 1) * rows * nbi * 2, sbytes = (size_t)mt * nbs * sizeof(float);
+    unsigned char *pb = (unsigned char *)ctx->buffer(BUF_P16, pbytes + sbytes + 256);
+    if (!pb) return DPLASMA_ERR_OUT_OF_RESOURCES;
+    a.P16 = pb;
+    a.scl = (float *)(pb + ((pbytes + 255) / 256) * 256);
+    a.p16_fmt = p16_fmt == 1 ? 1 : 0;
+    a.mx_split = split ? 1 : 0;
+    a.mx_chunk = chunk;
+    a.p16_rows = (int)rows;
+    a.p16_target = p16_fmt == 1 ? 1.0f : 16384.0f;
+    CUtensorMap tmap;
+    memset(&tmap, 0, sizeof(tmap));
+    int e = make_p16_map(ctx, &tmap, pb, (split ? 2 : 1) * rows, nbi, a.p16_fmt, split);
+    if (e) return e;
+    const size_t smem = potrf_smem_bytes(true);
+    CK(cudaFuncSetAttribute(potrf_persistent_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+
+    struct Evs {
+        std::vector<cudaEvent_t> v;
+        ~Evs()
+        {
+            for (auto x : v)
+                if (x) cudaEventDestroy(x);
+        }
+    } ev;
+    // events: [0, nph) copy of phase p landed, [nph] diagonal tiles landed,
+    // [nph + 1 + p] phase p done
+    const bool tl = ctx->stream_trace;
+    ev.v.assign(2 * (nph + 1), nullptr);
+    for (auto &x : ev.v) CK(cudaEventCreateWithFlags(&x, tl ? 0 : cudaEventDisableTiming));
+    const size_t tile = (size_t)nbi * nbi;
+    CK(cudaMemsetAsync(ctr, 0, nctr * sizeof(int), st));
+    CK(cudaEventRecord(ctx->ev0, st));
+    CK(cudaStreamWaitEvent(cs, ctx->ev0, 0));
+    // the diagonal tiles first (the row scales of the 16-bit panels)
+    for (int k = 0; k < mt; ++k) {
+        const size_t off = (size_t)lower_tile_index(k, k, mt) * tile;
+        CK(cudaMemcpyAsync(A0 + off, hA + off, tile * sizeof(double), cudaMemcpyHostToDevice, cs));
+    }
+    CK(cudaEventRecord(ev.v[nph], cs));
+    CK(cudaStreamWaitEvent(st, ev.v[nph], 0));
+    p16_scale_kernel<<<mt, nbi, 0, st>>>(A0, mt, nbi, a.p16_target, a.scl);
+    CK(cudaGetLastError());
+    ctx->launches += 1;
+    // the phases: columns [c0, c1) are one contiguous run of tiles
+    const uint64_t *tasks = (const uint64_t *)ctx->buffer(BUF_TASKS_PH, 0);
+    auto tile_of_col = [&](int c) { return c < mt ? (size_t)lower_tile_index(c, c, mt) : ntl; };
+    for (int p = 0; p < nph; ++p) {
+        const size_t t0 = tile_of_col(p * cb), t1 = tile_of_col(std::min(mt, p * cb + cb));
+        CK(cudaMemcpyAsync(A0 + t0 * tile, hA + t0 * tile, (t1 - t0) * tile * sizeof(double), cudaMemcpyHostToDevice,
+                           cs));
+        CK(cudaEventRecord(ev.v[p], cs));
+    }
+    // Each phase is queued when the GPU starts the previous one (one phase of
+    // slack), together with the following phases whose copies have already
+    // landed: their tickets are contiguous, so they run as one launch with no
+    // drain between them.
+    for (int p = 0; p < nph;) {
+        if (p >= 2) CK(cudaEventSynchronize(ev.v[nph + 1 + p - 2]));
+        int q = p + 1;
+        while (q < nph && cudaEventQuery(ev.v[q]) == cudaSuccess) ++q;
+        cudaGetLastError();
+        const size_t t0 = tile_of_col(p * cb), t1 = tile_of_col(std::min(mt, q * cb));
+        CK(cudaStreamWaitEvent(st, ev.v[q - 1], 0));
+        CK(cudaMemcpyAsync(L + t0 * tile, A0 + t0 * tile, (t1 - t0) * tile * sizeof(double), cudaMemcpyDeviceToDevice,
+                           st));
+        CK(cudaMemsetAsync(ctr, 0, sizeof(int), st));      // the ticket counter restarts each launch
+        a.tasks = tasks + ctx->ph_off[p];
+        a.ntasks = (int)(ctx->ph_off[q] - ctx->ph_off[p]);
+        potrf_persistent_kernel<true><<<grid, NTHREADS, smem, st>>>(a, tmap);
+        CK(cudaGetLastError());
+        for (int r = p; r < q; ++r) CK(cudaEventRecord(ev.v[nph + 1 + r], st));   // phases p..q-1 done
+        ctx->launches += 1;
+        p = q;
+    }
+    CK(cudaEventRecord(ctx->ev1, st));
+    int hs[8];
+    CK(cudaMemcpyAsync(hs, ctr, 8 * sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    CK(cudaStreamSynchronize(cs));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    ctx->last_factor_ms = ms;
+    if (tl) {
+        // per phase: host copy landed, phase finished (ms from the start)
+        for (int p = 0; p < nph; ++p) {
+            float c = 0.f, f = 0.f;
+            cudaEventElapsedTime(&c, ctx->ev0, ev.v[p]);
+            cudaEventElapsedTime(&f, ctx->ev0, ev.v[nph + 1 + p]);
+            fprintf(stderr, "stream phase %d: copied %.2f finished %.2f ms (%lld tickets)\n", p, c, f,
+                    ctx->ph_off[p + 1] - ctx->ph_off[p]);
+        }
+    }
+    if (hs[3] != ST_OK) {
+        ctx->set_error("streamed potrf scheduler status %d; site %d cta %d values %d %d", hs[3], hs[4], hs[5], hs[6],
+                       hs[7]);
+        return DPLASMA_ERR_UNEXPECTED;
+    }
+    *info = hs[1];
+    return 0;
+}
+
 }  // namespace db2
 
 namespace db2 {
@@ -1473,6 +1719,22 @@ extern "C" int dplasma_b200_debug_task_list_blocked(int mixed_chunk, int mt, int
     const std::vector<uint64_t> v = db2::build_potrf_tasks_mixed(mt, nbs, delay, mixed_chunk, bw, bh);
     for (size_t i = 0; i < v.size() && (int)i < cap; ++i) out[i] = v[i];
     return (int)v.size();
+}
+
+// The phased order: all phases concatenated into `out`; ends[p] = end of phase p.
+extern "C" int dplasma_b200_debug_task_list_phased(int mixed_chunk, int mt, int nbs, int delay, int cb,
+                                                   unsigned long long *out, int cap, int *ends, int ends_cap)
+{
+    const auto ph = db2::build_potrf_tasks_mixed_phased(mt, nbs, delay, mixed_chunk, cb, 8, 32);
+    size_t n = 0;
+    for (size_t p = 0; p < ph.size(); ++p) {
+        for (uint64_t t : ph[p]) {
+            if ((int)n < cap) out[n] = t;
+            ++n;
+        }
+        if ((int)p < ends_cap) ends[p] = (int)n;
+    }
+    return (int)n;
 }
 
 extern "C" int dplasma_b200_debug_task_list(int mixed_chunk, int mt, int nbs, int delay, unsigned long long *out,

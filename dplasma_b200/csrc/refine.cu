@@ -697,7 +697,7 @@ static int gmres_correction(Refine &R, double *Vbuf, int mmax, double tol, int *
 // the driver
 // ---------------------------------------------------------------------------
 int refine_solve(Context *ctx, const double *A0, double *L, const Geom &g, double *b, double *x, int npad, int nc,
-                 const RefineOpts &o, RefineStats &st)
+                 const RefineOpts &o, RefineStats &st, const double *hostA)
 {
     int rc;
     Refine R;
@@ -743,12 +743,20 @@ int refine_solve(Context *ctx, const double *A0, double *L, const Geom &g, doubl
     double *nrm = (double *)ctx->buffer(BUF_NORM, ((size_t)g.n + 1) * sizeof(double));
     if (!nrm) return DPLASMA_ERR_OUT_OF_RESOURCES;
     CK(cudaEventRecord(e0, ctx->stream));
-    if ((rc = copy_lansy_inf(ctx, A0, L, g, nrm))) return rc;
     double anrm = 0.0;
-    CK(cudaMemcpyAsync(&anrm, nrm + g.n, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     int info = 0;
     st.fmt_used = o.fmt;
-    if ((rc = potrf_run(ctx, L, g.mt, g.nbi, g.nb, g.n, &info, o.fmt))) return rc;
+    if (hostA) {
+        // A arrives from the host while the factorization runs; the norm of
+        // the stopping test is formed from the complete copy afterwards
+        if ((rc = potrf_run_streamed(ctx, hostA, const_cast<double *>(A0), L, g.mt, g.nbi, g.nb, g.n, &info, o.fmt)))
+            return rc;
+        if ((rc = lansy_inf_device(ctx, A0, g, &anrm))) return rc;
+    } else {
+        if ((rc = copy_lansy_inf(ctx, A0, L, g, nrm))) return rc;
+        CK(cudaMemcpyAsync(&anrm, nrm + g.n, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        if ((rc = potrf_run(ctx, L, g.mt, g.nbi, g.nb, g.n, &info, o.fmt))) return rc;
+    }
     if (info != 0 && o.escalate && o.fmt != 2) {
         // the 16-bit rounding of the panels broke positive definiteness:
         // the split form (about 22 bits) before giving up on tensor cores

@@ -102,3 +102,34 @@ def test_mixed_blocked_ticket_order(mt, S, bw, bh):
     tl = tasks_blocked(S, mt, 2, 444, bw, bh)
     replay(tl, mt, 2, S)
     assert sorted(tl) == sorted(tasks(S, mt, 2, 444))
+
+
+def tasks_phased(chunk, mt, nbs, delay, cb):
+    L = db.lib()
+    f = L.dplasma_b200_debug_task_list_phased
+    f.argtypes = [ctypes.c_int] * 5 + [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int]
+    n = f(chunk, mt, nbs, delay, cb, None, 0, None, 0)
+    out = np.zeros(n, dtype=np.uint64)
+    nph = -(-mt // cb)
+    ends = np.zeros(nph, dtype=np.int32)
+    assert f(chunk, mt, nbs, delay, cb, out.ctypes.data, n, ends.ctypes.data, nph) == n
+    tl = [(int(t) & 0xF, (int(t) >> 4) & 0xFFFF, (int(t) >> 20) & 0xFFFF, (int(t) >> 36) & 0xFFFF,
+           (int(t) >> 52) & 0xF, (int(t) >> 56) & 0xF) for t in out]
+    return tl, [int(e) for e in ends]
+
+
+@pytest.mark.parametrize("mt,S,cb,delay", [(33, 4, 8, 100), (65, 8, 16, 444), (64, 16, 16, 444), (20, 8, 8, 0),
+                                           (7, 4, 8, 3), (1, 8, 16, 0)])
+def test_mixed_phased_ticket_order(mt, S, cb, delay):
+    # the phases in sequence are a valid order of all the tasks ...
+    tl, ends = tasks_phased(S, mt, 2, delay, cb)
+    replay(tl, mt, 2, S)
+    assert sorted(tl) == sorted(tasks(S, mt, 2, delay))
+    # ... and phase p touches only tile columns below (p + 1) * cb
+    start = 0
+    for p, e in enumerate(ends):
+        c1 = min(mt, (p + 1) * cb)
+        for ty, k, m, n, bi, bj in tl[start:e]:
+            assert n < c1 and k < c1, (p, ty, k, m, n)
+        start = e
+    assert start == len(tl)
