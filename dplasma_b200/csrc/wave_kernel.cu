@@ -38,7 +38,11 @@ namespace db2 {
 
 constexpr int WV_RMAX = 4;
 constexpr int WV_KS = 32;
-constexpr int WV_NST = 3;
+constexpr int WV_NST_MAX = 6;
+// Ring stages of 32 KB: as many as the shared memory left by the two Y
+// stages of NC columns allows (the sweep streams L at the rate the ring's
+// bytes in flight sustain against the memory latency).
+__host__ __device__ constexpr int wv_nst(int nc) { return nc <= 16 ? 6 : (nc <= 24 ? 5 : 4); }
 constexpr int WV_A_DOUBLES = 128 * 32;  // one stage: 32 KB of swizzled slabs
 constexpr int WV_YP = 132;             // Y stage [n][k], k < 128 (two of them)
 constexpr int WV_THREADS = 384;
@@ -54,11 +58,12 @@ struct WaveArgs {
     int *flags;
     int *status;
     uint64_t limit_ns;
+    uint32_t smem_bytes;   // dynamic shared memory of the launch
 };
 
 struct __align__(16) WaveCtl {
-    uint64_t full[WV_NST];
-    uint64_t empty[WV_NST];
+    uint64_t full[WV_NST_MAX];
+    uint64_t empty[WV_NST_MAX];
 };
 
 // Tensor-map coordinates of the 128x128 block (p, q) of L: x = row within
@@ -97,13 +102,19 @@ template <int NC, bool TRANS>
 __global__ void __launch_bounds__(WV_THREADS, 1)
     trsm_wave_kernel(WaveArgs a, const __grid_constant__ CUtensorMap lmap, const __grid_constant__ CUtensorMap wmap)
 {
+    constexpr int WV_NST = wv_nst(NC);
     extern __shared__ __align__(1024) unsigned char smraw[];
     WaveCtl *ctl = reinterpret_cast<WaveCtl *>(smraw);
     // stages 1024-byte aligned in the shared window (swizzle atoms)
     const uint32_t sbase = smem_u32(smraw);
     double *ring = reinterpret_cast<double *>(smraw + ((((sbase + 128 + 1023u) & ~1023u)) - sbase));
-    double *Ybuf = ring + WV_NST * WV_A_DOUBLES;   // two Y stages of 32 x WV_YP
+    double *Ybuf = ring + WV_NST * WV_A_DOUBLES;   // two Y stages of NC x WV_YP
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    // the stages are sized for a 1024-aligned window: refuse to run otherwise
+    if ((size_t)(reinterpret_cast<unsigned char *>(Ybuf + 2 * NC * WV_YP) - smraw) > a.smem_bytes) {
+        if (tid == 0) atomicCAS(a.status, ST_OK, ST_BAD_TASK);
+        return;
+    }
     const int c = blockIdx.x, G = gridDim.x, P = a.nblk;
     if (tid == 0) {
         for (int s = 0; s < WV_NST; ++s) {
@@ -270,9 +281,13 @@ __global__ void __launch_bounds__(WV_THREADS, 1)
                 Yst[col * WV_YP + r] = res[ni][e];
                 Yq[(int64_t)col * a.ldy + r] = res[ni][e];
             }
-        __threadfence();
+        // the barrier orders every thread's stores before thread 0's
+        // GPU-scope fence and release (one fence for the CTA, not one per thread)
         named_bar_sync(1, 256);
-        if (tid == 0) red_release_add(a.flags + q, 1);
+        if (tid == 0) {
+            __threadfence();
+            red_release_add(a.flags + q, 1);
+        }
     };
 
     // first block: its owner solves it right away
@@ -285,8 +300,8 @@ __global__ void __launch_bounds__(WV_THREADS, 1)
     for (int qi = 0; qi < P && ok; ++qi) {
         const int q = wv_block<TRANS>(qi, P);
         const int nq = (qi + 1 < P) ? wv_block<TRANS>(qi + 1, P) : -1;
-        double *Yq = Ybuf + (qi & 1) * (32 * WV_YP);          // holds Y_q
-        double *Ynext = Ybuf + ((qi + 1) & 1) * (32 * WV_YP); // receives Y_nq if owned
+        double *Yq = Ybuf + (qi & 1) * (NC * WV_YP);          // holds Y_q
+        double *Ynext = Ybuf + ((qi + 1) & 1) * (NC * WV_YP); // receives Y_nq if owned
         bool any = false;
 #pragma unroll
         for (int i = 0; i < WV_RMAX; ++i) {
@@ -297,7 +312,14 @@ __global__ void __launch_bounds__(WV_THREADS, 1)
         if (q % G != c) {
             // Y_q from its owner
             int good = 1;
-            if (tid == 0) good = wait_geq(a.flags + q, 1, a.status, a.status, a.limit_ns) ? 1 : 0;
+            if (tid == 0) {
+                // the flag is usually a few microseconds away: spin before the
+                // bounded wait with its backoff
+                int spins = 0;
+                while (ld_acquire(a.flags + q) < 1 && ++spins < 4096) {
+                }
+                good = wait_geq(a.flags + q, 1, a.status, a.status, a.limit_ns) ? 1 : 0;
+            }
             named_bar_sync(1, 256);
             if (ld_volatile(a.status) != ST_OK || !good) break;
             const double *Yg = a.Y + (int64_t)a.c0 * a.ldy + (int64_t)q * 128;
@@ -326,16 +348,17 @@ __global__ void __launch_bounds__(WV_THREADS, 1)
     }
 }
 
-static size_t wave_smem_bytes()
+static size_t wave_smem_bytes(int nc)
 {
-    // control block, worst-case alignment of the stages, stages, Y stages
-    return 128 + 1024 + (size_t)(WV_NST * WV_A_DOUBLES + 2 * 32 * WV_YP) * sizeof(double);
+    // stages 1024-aligned after the control block, stages, Y stages
+    return 1024 + (size_t)(wv_nst(nc) * WV_A_DOUBLES + 2 * nc * WV_YP) * sizeof(double);
 }
 
 template <int NC, bool TRANS>
 static int launch_wave(Context *ctx, WaveArgs &a, int grid, CUtensorMap &lmap, CUtensorMap &wmap)
 {
-    const size_t smem = wave_smem_bytes();
+    const size_t smem = wave_smem_bytes(NC);
+    a.smem_bytes = (uint32_t)smem;
     CK(cudaFuncSetAttribute(trsm_wave_kernel<NC, TRANS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     void *args[] = {&a, &lmap, &wmap};
     CK(cudaLaunchCooperativeKernel((const void *)trsm_wave_kernel<NC, TRANS>, dim3(grid), dim3(WV_THREADS), args, smem,
@@ -346,10 +369,15 @@ static int launch_wave(Context *ctx, WaveArgs &a, int grid, CUtensorMap &lmap, C
 
 int wave_max_blocks_per_sm()
 {
-    const size_t smem = wave_smem_bytes();
     int best = 1 << 30;
-    const void *fns[] = {(const void *)trsm_wave_kernel<32, false>, (const void *)trsm_wave_kernel<32, true>};
-    for (const void *fn : fns) {
+    const void *fns[] = {(const void *)trsm_wave_kernel<8, false>,  (const void *)trsm_wave_kernel<8, true>,
+                         (const void *)trsm_wave_kernel<16, false>, (const void *)trsm_wave_kernel<16, true>,
+                         (const void *)trsm_wave_kernel<24, false>, (const void *)trsm_wave_kernel<24, true>,
+                         (const void *)trsm_wave_kernel<32, false>, (const void *)trsm_wave_kernel<32, true>};
+    const int ncs[] = {8, 8, 16, 16, 24, 24, 32, 32};
+    for (int i = 0; i < 8; ++i) {
+        const void *fn = fns[i];
+        const size_t smem = wave_smem_bytes(ncs[i]);
         int n = 0;
         if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, WV_THREADS, smem) != cudaSuccess)
