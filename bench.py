@@ -505,6 +505,8 @@ def run_gpu(args):
     stats, launches = [], 0
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(dev) as clk:
+        # the NVTX range marks the timed steps for a profiler's launch list
+        torch.cuda.nvtx.range_push("timed")
         e0.record()
         t0 = time.perf_counter()
         for _ in range(args.steps):
@@ -513,6 +515,7 @@ def run_gpu(args):
         e1.record()
         torch.cuda.synchronize()
         wall = time.perf_counter() - t0
+        torch.cuda.nvtx.range_pop()
     if dist:
         dist.barrier()
     total_ms = max_over_ranks(e0.elapsed_time(e1), dist, "cuda")
