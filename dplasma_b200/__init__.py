@@ -46,7 +46,8 @@ class RefineOpts(ctypes.Structure):
     """dplasma_b200_refine_opts_t."""
 
     _fields_ = [("fmt", ctypes.c_int), ("solver", ctypes.c_int), ("itermax", ctypes.c_int), ("gmres_m", ctypes.c_int),
-                ("gmres_tol", ctypes.c_double), ("bwdmax", ctypes.c_double), ("escalate", ctypes.c_int)]
+                ("gmres_tol", ctypes.c_double), ("bwdmax", ctypes.c_double), ("escalate", ctypes.c_int),
+                ("shift", ctypes.c_double)]
 
 
 class RefineStats(ctypes.Structure):
@@ -415,12 +416,13 @@ class Context:
 
     def dsposv(self, uplo: int, A: Desc, B: Desc, X: Desc, fmt: int = FP16, solver: int = IR_AUTO,
                itermax: int = 30, gmres_m: int = 30, gmres_tol: float = 1e-4, bwdmax: float = 1.0,
-               escalate: bool = True):
+               escalate: bool = True, shift: float = 0.0):
         """Mixed-precision solve (dplasma_b200_dsposv_ex): returns (rc, stats dict)."""
         o = RefineOpts()
         lib().dplasma_b200_refine_opts_default(ctypes.byref(o))
         o.fmt, o.solver, o.itermax, o.gmres_m, o.gmres_tol, o.bwdmax = fmt, solver, itermax, gmres_m, gmres_tol, bwdmax
         o.escalate = 1 if escalate else 0
+        o.shift = shift
         st = RefineStats()
         rc = lib().dplasma_b200_dsposv_ex(self.h, uplo, ctypes.byref(A), ctypes.byref(B), ctypes.byref(X),
                                           ctypes.byref(o), ctypes.byref(st))

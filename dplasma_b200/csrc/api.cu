@@ -643,6 +643,7 @@ extern "C" void dplasma_b200_refine_opts_default(dplasma_b200_refine_opts_t *o)
     o->gmres_tol = 1e-4;
     o->bwdmax = 1.0;
     o->escalate = 1;
+    o->shift = 0.0;
 }
 
 extern "C" int dplasma_b200_dsposv_ex(parsec_context_t *parsec, dplasma_enum_t uplo, parsec_tiled_matrix_t *A,
@@ -658,7 +659,8 @@ extern "C" int dplasma_b200_dsposv_ex(parsec_context_t *parsec, dplasma_enum_t u
     dplasma_b200_refine_opts_default(&o);
     if (opts) o = *opts;
     if ((o.fmt != DPLASMA_B200_FP16 && o.fmt != DPLASMA_B200_BF16 && o.fmt != DPLASMA_B200_FP16_SPLIT) || o.solver < 0 || o.solver > 2 ||
-        o.itermax < 0 || o.gmres_m < 1 || o.gmres_m > 200 || !(o.gmres_tol > 0.0) || !(o.bwdmax > 0.0)) {
+        o.itermax < 0 || o.gmres_m < 1 || o.gmres_m > 200 || !(o.gmres_tol > 0.0) || !(o.bwdmax > 0.0) ||
+        !(o.shift >= 0.0 && o.shift < 1.0)) {
         dplasma_error("dplasma_dsposv", "illegal options");
         return DPLASMA_ERR_ILLEGAL_VALUE;
     }
@@ -688,7 +690,8 @@ extern "C" int dplasma_b200_dsposv_ex(parsec_context_t *parsec, dplasma_enum_t u
     // a host matrix in pinned memory that already has the device tile layout
     // is streamed in while the factorization runs (phases of tile columns)
     const double *stream_src = nullptr;
-    if (!inplace && !ctx->no_stream && A->location == DPLASMA_B200_HOST && A->storage == PARSEC_MATRIX_TILE &&
+    if (!inplace && !ctx->no_stream && o.shift == 0.0 && A->location == DPLASMA_B200_HOST &&
+        A->storage == PARSEC_MATRIX_TILE &&
         A->uplo == dplasmaLower && uplo == dplasmaLower && A->mb == A->nb && g.nbi == g.nb && g.n % g.nb == 0 &&
         A->lmt == g.mt) {
         cudaPointerAttributes pa;
@@ -711,6 +714,7 @@ extern "C" int dplasma_b200_dsposv_ex(parsec_context_t *parsec, dplasma_enum_t u
     ro.gmres_tol = o.gmres_tol;
     ro.bwd_factor = o.bwdmax;
     ro.escalate = o.escalate != 0;
+    ro.shift = o.shift;
     RefineStats st;
     rc = refine_solve(ctx, A0, L, g, b, x, npad, nrhs_pad, ro, st, stream_src);
     if (stats) {

@@ -42,6 +42,7 @@ enum BufferId : int {
     BUF_SELFCHECK,    // per-ticket run counters (self check)
     BUF_WX,           // second block row [Linv10 | W1] of the inverses of 256-wide diagonal tiles
     BUF_TASKS_PH,     // phased ticket order of the streamed factorization
+    BUF_WM,           // triangular sweeps: the critical path's products W_b L_{b,b-1}
     BUF_COUNT
 };
 
@@ -173,6 +174,7 @@ struct RefineOpts {
     int fmt = 0, solver = 0, itermax = 30, gmres_m = 30;
     double gmres_tol = 1e-4, bwd_factor = 1.0;
     bool escalate = true;
+    double shift = 0.0;       // relative diagonal shift of the 16-bit factorization (A + shift diag(A))
 };
 struct RefineStats {
     int iter = 0, inner_iters = 0, fallback = 0, solver_used = 0, fmt_used = 0;
@@ -183,6 +185,7 @@ struct RefineStats {
 int refine_solve(Context *ctx, const double *A0, double *L, const Geom &g, double *b, double *x, int npad, int nc,
                  const RefineOpts &o, RefineStats &st, const double *hostA = nullptr);
 int generate_cond(Context *ctx, double *dA, const Geom &g, double kappa, int nrefl, unsigned long long seed);
+int shift_diag(Context *ctx, double *L, const Geom &g, double f);
 int symm_tiles(Context *ctx, const double *dA, const Geom &g, const double *in, int ldin, double *out, int ldout,
                int ncols, double alpha, int *status);
 

@@ -379,62 +379,6 @@ __device__ __forceinline__ bool consume_job(const PotrfArgs &a, SmemCtl *ctl, co
 }
 
 // ---------------------------------------------------------------------------
-// C(128x128) = alpha A(128x128) B(128x128), column-major operands (A from
-// global memory through L2, B from global or shared memory), by the FP64
-// tensor cores; one warp per 32x32 output block.  A (B) lower triangular by
-// 32-blocks when lowA (lowB): the zero blocks of the K range are skipped.
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ void gemm128_tri(const double *A, int lda, bool lowA, const double *B, int ldb, bool lowB,
-                                            bool b_shared, double *C, int ldc, double alpha, int warp, int lane,
-                                            int nwarps)
-{
-    const int g = lane >> 2, t = lane & 3;
-    for (int blk = warp; blk < 16; blk += nwarps) {
-        const int bi = blk & 3, bj = blk >> 2;
-        const int l0 = lowB ? bj : 0, l1 = lowA ? bi : 3;
-        double acc[2][4][4];
-#pragma unroll
-        for (int mi = 0; mi < 2; ++mi)
-#pragma unroll
-            for (int ni = 0; ni < 4; ++ni)
-#pragma unroll
-                for (int q = 0; q < 4; ++q) acc[mi][ni][q] = 0.0;
-        for (int l = l0; l <= l1; ++l) {
-#pragma unroll
-            for (int kk = 0; kk < 32; kk += 4) {
-                const int kq = l * 32 + kk + t;
-                double af[2][2], bf[4];
-#pragma unroll
-                for (int mi = 0; mi < 2; ++mi) {
-                    const double *pa = A + (int64_t)kq * lda + bi * 32 + mi * 16 + g;
-                    af[mi][0] = __ldcg(pa);
-                    af[mi][1] = __ldcg(pa + 8);
-                }
-#pragma unroll
-                for (int ni = 0; ni < 4; ++ni) {
-                    const double *pb = B + (int64_t)(bj * 32 + ni * 8 + g) * ldb + kq;
-                    bf[ni] = b_shared ? *pb : __ldcg(pb);
-                }
-#pragma unroll
-                for (int mi = 0; mi < 2; ++mi)
-#pragma unroll
-                    for (int ni = 0; ni < 4; ++ni) dmma_16x8x4(acc[mi][ni], af[mi][0], af[mi][1], bf[ni]);
-            }
-        }
-#pragma unroll
-        for (int mi = 0; mi < 2; ++mi)
-#pragma unroll
-            for (int ni = 0; ni < 4; ++ni)
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const int r = bi * 32 + mi * 16 + g + ((q & 2) ? 8 : 0);
-                    const int c = bj * 32 + ni * 8 + 2 * t + (q & 1);
-                    C[(int64_t)c * ldc + r] = alpha * acc[mi][ni][q];
-                }
-    }
-}
-
-// ---------------------------------------------------------------------------
 // consumers: POTRF(k) of one diagonal tile + inverses of its 128x128 diagonal
 // blocks (src/zpotrf_L.jdf:194-206 computes the factor with
 // LAPACKE_dpotrf_work; the inverses feed the TRSM jobs).

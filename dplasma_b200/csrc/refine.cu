@@ -696,6 +696,24 @@ static int gmres_correction(Refine &R, double *Vbuf, int mmax, double tol, int *
 // ---------------------------------------------------------------------------
 // the driver
 // ---------------------------------------------------------------------------
+// L(i,i) *= f for the n valid rows (the identity padding is left alone)
+__global__ void shift_diag_kernel(double *L, int mt, int nbi, int nb, int n, double f)
+{
+    const int k = blockIdx.x, r = threadIdx.x;
+    if (r < nb && (int64_t)k * nb + r < n) {
+        double *T = L + lower_tile_index(k, k, mt) * (int64_t)nbi * nbi;
+        T[(int64_t)r * nbi + r] *= f;
+    }
+}
+
+int shift_diag(Context *ctx, double *L, const Geom &g, double f)
+{
+    shift_diag_kernel<<<g.mt, g.nbi, 0, ctx->stream>>>(L, g.mt, g.nbi, g.nb, g.n, f);
+    CK(cudaGetLastError());
+    ctx->launches++;
+    return 0;
+}
+
 int refine_solve(Context *ctx, const double *A0, double *L, const Geom &g, double *b, double *x, int npad, int nc,
                  const RefineOpts &o, RefineStats &st, const double *hostA)
 {
@@ -755,12 +773,19 @@ int refine_solve(Context *ctx, const double *A0, double *L, const Geom &g, doubl
     } else {
         if ((rc = copy_lansy_inf(ctx, A0, L, g, nrm))) return rc;
         CK(cudaMemcpyAsync(&anrm, nrm + g.n, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        // shifted factor (Higham and Pranesh, SISC 2021): the 16-bit
+        // factorization of A + s diag(A), i.e. of D^-1/2 A D^-1/2 + s I
+        // rescaled (the row scales of the 16-bit panels come from the same
+        // diagonal), which stays positive definite where A's own 16-bit
+        // factorization breaks down; the refinement (GMRES-IR) still solves A
+        if (o.shift > 0.0 && (rc = shift_diag(ctx, L, g, 1.0 + o.shift))) return rc;
         if ((rc = potrf_run(ctx, L, g.mt, g.nbi, g.nb, g.n, &info, o.fmt))) return rc;
     }
     if (info != 0 && o.escalate && o.fmt != 2) {
         // the 16-bit rounding of the panels broke positive definiteness:
         // the split form (about 22 bits) before giving up on tensor cores
         CK(cudaMemcpyAsync(L, A0, g.elems() * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+        if (o.shift > 0.0 && (rc = shift_diag(ctx, L, g, 1.0 + o.shift))) return rc;
         st.fmt_used = 2;
         if ((rc = potrf_run(ctx, L, g.mt, g.nbi, g.nb, g.n, &info, 2))) return rc;
     }

@@ -5,16 +5,19 @@
 // over 128-row blocks.  CTA c owns the blocks p = c, c+G, c+2G, ... (at most
 // WV_RMAX of them) and keeps their partial sums in registers.  For every
 // block q in solve order it
-//   * if it owns q: forms Y_q = W_qq^{op} acc_q (W_qq the inverse of the
-//     diagonal block), stores it and raises q's flag;
+//   * if it owns the next block nq: forms Z = W_nq^{op} acc_nq before Y_q is
+//     known (acc_nq then holds every term but q's), waits for Y_q and forms
+//     Y_nq = Z - M_nq Y_q with M_nq = W_nq^{op} op(L)_{nq,q} (prepared for
+//     every block before the sweep, wave_prep_kernel), stores it and raises
+//     nq's flag;
 //   * otherwise: waits for q's flag and stages Y_q in shared memory;
 //   * applies acc_p -= op(L)_pq Y_q to each owned block p still to solve.
 // Each owned accumulator is updated in increasing q by one CTA, so the result
-// is deterministic.  A producer warp streams the L blocks into a ring of
-// bulk copies ahead of the flags (they do not depend on Y), so the critical
-// path per block is one flag, one 128x128 update and the diagonal multiply,
-// while the bulk of L streams from HBM on all SMs at once.  CTAs wait on one
-// another, hence the cooperative launch.
+// is deterministic.  A producer warp streams the L, W and M blocks into a
+// ring of bulk copies ahead of the flags (they do not depend on Y), so the
+// critical path per block is one flag and one 128x128 product, while the bulk
+// of L streams from HBM on all SMs at once.  CTAs wait on one another, hence
+// the cooperative launch.
 //
 // L and W arrive by TMA tensor loads with the 128-byte swizzle (a stage of
 // 32 KB takes 8 or 2 loads).  The stage holds 16-row slabs of 128-byte lines
@@ -32,6 +35,7 @@
 
 #include "dev_common.cuh"
 #include "dev_tcgen05.cuh"
+#include "dev_trtri.cuh"
 #include "internal.h"
 
 namespace db2 {
@@ -100,7 +104,8 @@ __device__ __forceinline__ int wv_block(int qi, int P) { return TRANS ? P - 1 - 
 
 template <int NC, bool TRANS>
 __global__ void __launch_bounds__(WV_THREADS, 1)
-    trsm_wave_kernel(WaveArgs a, const __grid_constant__ CUtensorMap lmap, const __grid_constant__ CUtensorMap wmap)
+    trsm_wave_kernel(WaveArgs a, const __grid_constant__ CUtensorMap lmap, const __grid_constant__ CUtensorMap wmap,
+                     const __grid_constant__ CUtensorMap mmap)
 {
     constexpr int WV_NST = wv_nst(NC);
     extern __shared__ __align__(1024) unsigned char smraw[];
@@ -125,7 +130,7 @@ __global__ void __launch_bounds__(WV_THREADS, 1)
     __syncthreads();
 
     // Work of position qi for this CTA, in order:
-    //   [critical] if it owns the next block nq: L(nq, q) then W(nq)   (8 stages)
+    //   [critical] if it owns the next block nq: W(nq) then M(nq)       (8 stages)
     //   [rest]     L(p, q) for its other blocks p still to solve        (4 stages each)
     // plus, before position 0, W(first block) if it owns it.
     if (warp >= 8) {
@@ -136,6 +141,7 @@ __global__ void __launch_bounds__(WV_THREADS, 1)
         if (lane == 0) {
             tma_prefetch_desc(&lmap);
             tma_prefetch_desc(&wmap);
+            tma_prefetch_desc(&mmap);
         }
         // one 128x128 block whose element (row, col) of the A operand is at
         // map coordinates: forward (x0 + row, y0 + col), backward
@@ -177,8 +183,8 @@ __global__ void __launch_bounds__(WV_THREADS, 1)
             const int q = wv_block<TRANS>(qi, P);
             const int nq = (qi + 1 < P) ? wv_block<TRANS>(qi + 1, P) : -1;
             if (nq >= 0 && nq % G == c) {
-                issue_l(nq, q);
                 issue(&wmap, 0, nq * 128);
+                issue(&mmap, 0, nq * 128);
             }
             for (int i = 0; i < WV_RMAX && ok; ++i) {
                 const int p = c + i * G;
@@ -232,6 +238,61 @@ __global__ void __launch_bounds__(WV_THREADS, 1)
             __syncwarp();
             if (lane == 0) mbar_arrive(&ctl->empty[s]);
             ++it;
+        }
+    };
+    // res = op(W_qq) * ac (W streamed through the ring), ac staged in Yst; ac is cleared
+    auto wmul = [&](double (&ac)[NT][4], double *Yst, double (&res)[NT][4]) {
+#pragma unroll
+        for (int ni = 0; ni < NT; ++ni)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int r = (e & 2) ? rb : ra;
+                const int col = ni * 8 + 2 * t + (e & 1);
+                Yst[col * WV_YP + r] = ac[ni][e];
+                ac[ni][e] = 0.0;
+                res[ni][e] = 0.0;
+            }
+        named_bar_sync(1, 256);
+        for (int s0 = 0; s0 < 128 && ok; s0 += WV_KS) {
+            const uint32_t s = it % WV_NST, r = it / WV_NST;
+            if (!warp_mbar_wait(&ctl->full[s], r & 1, a.limit_ns)) {
+                if (lane == 0) atomicCAS(a.status, ST_OK, ST_MBAR_TIMEOUT);
+                ok = false;
+                break;
+            }
+            const double *As = ring + s * WV_A_DOUBLES;
+#pragma unroll
+            for (int kk = 0; kk < WV_KS; kk += 4) {   // A = W (forward) or W^T (backward)
+                const double a0 = As[wv_aidx<TRANS>(ra, kk + t)];
+                const double a1 = As[wv_aidx<TRANS>(rb, kk + t)];
+#pragma unroll
+                for (int ni = 0; ni < NT; ++ni) dmma_16x8x4(res[ni], a0, a1, Yst[(ni * 8 + g) * WV_YP + s0 + kk + t]);
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&ctl->empty[s]);
+            ++it;
+        }
+        named_bar_sync(1, 256);   // Yst is free again
+    };
+    // the solved block to shared memory (for this CTA's own updates), to
+    // global memory, then its flag
+    auto publish = [&](const double (&y)[NT][4], double *Yst, int q) {
+        double *Yq = a.Y + (int64_t)a.c0 * a.ldy + (int64_t)q * 128;
+#pragma unroll
+        for (int ni = 0; ni < NT; ++ni)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int r = (e & 2) ? rb : ra;
+                const int col = ni * 8 + 2 * t + (e & 1);
+                Yst[col * WV_YP + r] = y[ni][e];
+                Yq[(int64_t)col * a.ldy + r] = y[ni][e];
+            }
+        // the barrier orders every thread's stores before thread 0's
+        // GPU-scope fence and release (one fence for the CTA, not one per thread)
+        named_bar_sync(1, 256);
+        if (tid == 0) {
+            __threadfence();
+            red_release_add(a.flags + q, 1);
         }
     };
     // Y_q = op(W_qq) * acc (W streamed through the ring); result to Yst and global
@@ -309,6 +370,19 @@ __global__ void __launch_bounds__(WV_THREADS, 1)
             any |= (p < P) && (TRANS ? p < q : p > q);
         }
         if (!any) continue;
+        if (nq >= 0 && nq % G == c) {
+            // Z = op(W_nq) acc_nq while Y_q is not known yet (Ynext as staging)
+#pragma unroll
+            for (int i = 0; i < WV_RMAX; ++i) {
+                if (c + i * G != nq) continue;
+                double z[NT][4];
+                wmul(acc[i], Ynext, z);
+#pragma unroll
+                for (int ni = 0; ni < NT; ++ni)
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) acc[i][ni][e] = z[ni][e];
+            }
+        }
         if (q % G != c) {
             // Y_q from its owner
             int good = 1;
@@ -320,8 +394,8 @@ __global__ void __launch_bounds__(WV_THREADS, 1)
                 }
                 good = wait_geq(a.flags + q, 1, a.status, a.status, a.limit_ns) ? 1 : 0;
             }
-            named_bar_sync(1, 256);
-            if (ld_volatile(a.status) != ST_OK || !good) break;
+            // one decision for all consumer warps (the status may change between their reads)
+            if (named_bar_or(1, 256, !good || ld_volatile(a.status) != ST_OK)) break;
             const double *Yg = a.Y + (int64_t)a.c0 * a.ldy + (int64_t)q * 128;
             for (int e = tid; e < NC * 128; e += 256) {
                 const int col = e / 128, r = e % 128;
@@ -334,8 +408,11 @@ __global__ void __launch_bounds__(WV_THREADS, 1)
 #pragma unroll
             for (int i = 0; i < WV_RMAX; ++i) {
                 if (c + i * G != nq) continue;
-                update(acc[i], Yq);
-                if (ok) diag(acc[i], Ynext, nq);
+                update(acc[i], Yq);            // acc_nq -= M_nq Y_q, acc_nq = Z on entry
+                if (named_bar_or(1, 256, !ok))
+                    ok = false;
+                else
+                    publish(acc[i], Ynext, nq);
             }
         }
 #pragma unroll
@@ -344,8 +421,30 @@ __global__ void __launch_bounds__(WV_THREADS, 1)
             if (p >= P || p == nq || !(TRANS ? p < q : p > q)) continue;
             update(acc[i], Yq);
         }
-        named_bar_sync(1, 256);   // Yq is overwritten two positions later
+        // Yq is overwritten two positions later; every warp leaves the loop together
+        if (named_bar_or(1, 256, !ok)) ok = false;
     }
+}
+
+// The products of the critical path, formed before a sweep (128x128,
+// column-major, block b at M + b * 128^2):
+//   forward:  M_b = W_b L_{b,b-1},  b = 1 .. P-1;
+//   backward: M_b = L_{b+1,b} W_b,  b = 0 .. P-2 (the backward ring reads the
+//             transpose, W_b^T L_{b+1,b}^T).
+__global__ void __launch_bounds__(256) wave_prep_kernel(const double *A, const double *W, int mt, int nbi, int nbs,
+                                                        int transposed, double *M)
+{
+    const int b = transposed ? (int)blockIdx.x : (int)blockIdx.x + 1;
+    const int p = transposed ? b + 1 : b, q = transposed ? b : b - 1;     // the sub-diagonal block L_{p,q}
+    const double *Lpq = A + lower_tile_index(p / nbs, q / nbs, mt) * (int64_t)nbi * nbi +
+                        (int64_t)(q % nbs) * 128 * nbi + (p % nbs) * 128;
+    const double *Wb = W + (int64_t)b * 128 * 128;
+    double *Mb = M + (int64_t)b * 128 * 128;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (!transposed)
+        gemm128_tri(Wb, 128, true, Lpq, nbi, false, false, Mb, 128, 1.0, warp, lane, 8);
+    else
+        gemm128_tri(Lpq, nbi, false, Wb, 128, true, false, Mb, 128, 1.0, warp, lane, 8);
 }
 
 static size_t wave_smem_bytes(int nc)
@@ -355,12 +454,12 @@ static size_t wave_smem_bytes(int nc)
 }
 
 template <int NC, bool TRANS>
-static int launch_wave(Context *ctx, WaveArgs &a, int grid, CUtensorMap &lmap, CUtensorMap &wmap)
+static int launch_wave(Context *ctx, WaveArgs &a, int grid, CUtensorMap &lmap, CUtensorMap &wmap, CUtensorMap &mmap)
 {
     const size_t smem = wave_smem_bytes(NC);
     a.smem_bytes = (uint32_t)smem;
     CK(cudaFuncSetAttribute(trsm_wave_kernel<NC, TRANS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    void *args[] = {&a, &lmap, &wmap};
+    void *args[] = {&a, &lmap, &wmap, &mmap};
     CK(cudaLaunchCooperativeKernel((const void *)trsm_wave_kernel<NC, TRANS>, dim3(grid), dim3(WV_THREADS), args, smem,
                                    ctx->stream));
     ctx->launches++;
@@ -403,13 +502,24 @@ int trsm_wave(Context *ctx, const double *dA, const double *W, const Geom &g, do
     // L: rows of the tiles contiguous (nbi), one line per tile column;
     // W: 128x128 column-major blocks.  Boxes of 16 doubles (128 bytes, the
     // swizzle span) by 32 (forward: k columns) or 128 (backward: columns).
-    CUtensorMap lmap, wmap;
+    // the critical path's products W_b L_{b,b-1} (or L_{b+1,b} W_b)
+    double *M = (double *)ctx->buffer(BUF_WM, (size_t)nblk * 128 * 128 * sizeof(double));
+    if (!M) return DPLASMA_ERR_OUT_OF_RESOURCES;
+    if (nblk > 1) {
+        wave_prep_kernel<<<nblk - 1, 256, 0, ctx->stream>>>(dA, W, g.mt, g.nbi, g.nbi / 128, transposed, M);
+        CK(cudaGetLastError());
+        ctx->launches++;
+    }
+    CUtensorMap lmap, wmap, mmap;
     const uint32_t box1 = transposed ? 128 : WV_KS;
     int rc0 = encode_map_2d(ctx, &lmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, (void *)dA, (uint64_t)g.nbi,
                             (uint64_t)g.ntiles() * g.nbi, (uint64_t)g.nbi * sizeof(double), 16, box1,
                             CU_TENSOR_MAP_SWIZZLE_128B);
     if (!rc0)
         rc0 = encode_map_2d(ctx, &wmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, (void *)W, 128, (uint64_t)nblk * 128,
+                            128 * sizeof(double), 16, box1, CU_TENSOR_MAP_SWIZZLE_128B);
+    if (!rc0)
+        rc0 = encode_map_2d(ctx, &mmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, (void *)M, 128, (uint64_t)nblk * 128,
                             128 * sizeof(double), 16, box1, CU_TENSOR_MAP_SWIZZLE_128B);
     if (rc0) return rc0;
     for (int ch = 0; ch < nchunks; ++ch) {
@@ -430,15 +540,15 @@ int trsm_wave(Context *ctx, const double *dA, const double *W, const Geom &g, do
         const int nc = (nrhs - a.c0) < 32 ? (nrhs - a.c0) : 32;   // nrhs is a multiple of 8
         int rc;
         if (transposed)
-            rc = nc <= 8    ? launch_wave<8, true>(ctx, a, grid, lmap, wmap)
-                 : nc <= 16 ? launch_wave<16, true>(ctx, a, grid, lmap, wmap)
-                 : nc <= 24 ? launch_wave<24, true>(ctx, a, grid, lmap, wmap)
-                            : launch_wave<32, true>(ctx, a, grid, lmap, wmap);
+            rc = nc <= 8    ? launch_wave<8, true>(ctx, a, grid, lmap, wmap, mmap)
+                 : nc <= 16 ? launch_wave<16, true>(ctx, a, grid, lmap, wmap, mmap)
+                 : nc <= 24 ? launch_wave<24, true>(ctx, a, grid, lmap, wmap, mmap)
+                            : launch_wave<32, true>(ctx, a, grid, lmap, wmap, mmap);
         else
-            rc = nc <= 8    ? launch_wave<8, false>(ctx, a, grid, lmap, wmap)
-                 : nc <= 16 ? launch_wave<16, false>(ctx, a, grid, lmap, wmap)
-                 : nc <= 24 ? launch_wave<24, false>(ctx, a, grid, lmap, wmap)
-                            : launch_wave<32, false>(ctx, a, grid, lmap, wmap);
+            rc = nc <= 8    ? launch_wave<8, false>(ctx, a, grid, lmap, wmap, mmap)
+                 : nc <= 16 ? launch_wave<16, false>(ctx, a, grid, lmap, wmap, mmap)
+                 : nc <= 24 ? launch_wave<24, false>(ctx, a, grid, lmap, wmap, mmap)
+                            : launch_wave<32, false>(ctx, a, grid, lmap, wmap, mmap);
         if (rc) return rc;
     }
     int st = 0;

@@ -294,6 +294,9 @@ typedef struct dplasma_b200_refine_opts_s {
     double bwdmax;     /* LAPACK dsposv BWDMAX: stop when ||r_j|| < ||x_j|| ||A|| eps sqrt(n) bwdmax */
     int    escalate;   /* 1: when an FP16/BF16 factorization loses positive definiteness, retry in
                           the split-FP16 form before the FP64 fallback */
+    double shift;      /* s >= 0: the 16-bit factorization is of A + s diag(A) (the shifted, diagonally
+                          scaled factor of Higham and Pranesh, SISC 2021), kept positive definite at
+                          large condition numbers; the refinement solves A.  0: no shift */
 } dplasma_b200_refine_opts_t;
 
 typedef struct dplasma_b200_refine_stats_s {
@@ -309,7 +312,7 @@ typedef struct dplasma_b200_refine_stats_s {
     double anorm;          /* ||A||_inf of the FP64 matrix, the scale of the stopping test */
 } dplasma_b200_refine_stats_t;
 
-/* Defaults: FP16, IR_AUTO, itermax 30, gmres_m 30, gmres_tol 1e-4, bwdmax 1, escalate 1. */
+/* Defaults: FP16, IR_AUTO, itermax 30, gmres_m 30, gmres_tol 1e-4, bwdmax 1, escalate 1, shift 0. */
 void dplasma_b200_refine_opts_default(dplasma_b200_refine_opts_t *opts);
 
 /* dplasma_b200_dplgsy_cond: no dplasma counterpart; a test-matrix generator

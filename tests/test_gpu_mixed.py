@@ -196,3 +196,26 @@ def test_dplgsy_cond_spectrum(gpu_ctx, N, NB, uplo):
     assert np.allclose(ev, np.geomspace(1.0, kappa, N), rtol=1e-9, atol=1e-9 * kappa)
     # not diagonal: the reflectors mixed the coordinates
     assert np.abs(A - np.diag(np.diag(A))).max() > 1e-3
+
+
+@pytest.mark.parametrize("kappa,shift", [(1e6, 2.0 ** -8), (1e4, 2.0 ** -10)])
+def test_dsposv_shifted_fp16_gmres(gpu_ctx, kappa, shift):
+    # the shifted FP16 factor of A + s diag(A) (positive definite where A's own
+    # FP16 factor breaks down at kappa 1e6) refined by GMRES-IR to the dsposv accuracy
+    N, NB, NRHS = 2048, 256, 4
+    A = householder_spd(N, kappa)
+    B = np.random.default_rng(12).standard_normal((N, NRHS))
+    rc, st, X, _, _ = run_dsposv(gpu_ctx, A, B, NB, db.Lower, fmt=db.FP16, solver=db.IR_GMRES, shift=shift,
+                                 escalate=False, gmres_m=60)
+    assert rc == 0, gpu_ctx.last_error()
+    assert st["fallback"] == 0 and st["fmt_used"] == db.FP16 and st["solver_used"] == db.IR_GMRES, st
+    assert st["inner_iters"] > 0
+    assert st["backward_error"] < 10 * N * EPS, st
+    assert daxmb_ratio(A, X, B) < 10.0
+
+
+def test_dsposv_rejects_bad_shift(gpu_ctx):
+    N, NB = 512, 256
+    A = oracle.dplgsy(N, NB, 3872, bump=float(N))
+    rc, _, _, _, _ = run_dsposv(gpu_ctx, A, np.ones((N, 1)), NB, db.Lower, shift=-1.0)
+    assert rc == db.ERR_ILLEGAL_VALUE
