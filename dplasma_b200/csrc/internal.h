@@ -41,6 +41,7 @@ enum BufferId : int {
     BUF_BATCH_W,      // batched inverse: per-CTA padded factor and L^-1
     BUF_SELFCHECK,    // per-ticket run counters (self check)
     BUF_WX,           // second block row [Linv10 | W1] of the inverses of 256-wide diagonal tiles
+    BUF_LINV16,       // inverses of the diagonal tiles in split FP16 (tensor-core TRSM strips)
     BUF_TASKS_PH,     // phased ticket order of the streamed factorization
     BUF_WM,           // triangular sweeps: the critical path's products W_b L_{b,b-1}
     BUF_COUNT
@@ -69,6 +70,7 @@ struct Context {
     uint64_t pipe_limit_ns = 4000000000ull;  // 4 s
     bool self_check = false;
     bool trsm_inv = false;                   // DPLASMA_B200_TRSM_INV: 256-wide TRSM strips on the tile's whole inverse
+    bool trsm_tc = false;                    // DPLASMA_B200_TRSM_TC: mixed split-FP16 TRSM strips on the tensor cores
     void *bufs[BUF_COUNT] = {};
     size_t bufsz[BUF_COUNT] = {};
     int task_mt = -1, task_nbs = -1, task_delay = -1, ntasks = 0;

@@ -49,6 +49,14 @@ __device__ __forceinline__ int all_updates(const PotrfArgs &a, int m, int n)
     return n * step_blocks<MIXED>(a, m, n);
 }
 
+// Mixed split FP16 with tensor-core strips: every strip but those of the next
+// tile row (which run in FP64 as soon as the factor and W are out).
+template <bool MIXED>
+__device__ __forceinline__ bool tc_strip(const PotrfArgs &a, int k, int m)
+{
+    return MIXED && a.tc_trsm && m > k + 1;
+}
+
 template <bool MIXED>
 __device__ bool wait_deps(const PotrfArgs &a, uint64_t t)
 {
@@ -59,7 +67,8 @@ __device__ bool wait_deps(const PotrfArgs &a, uint64_t t)
         return wait_geq(a.upd_done + (int64_t)k * a.mt + k, all_updates<MIXED>(a, k, k), a.abort_flag, a.status,
                         a.dep_limit_ns);
     case T_TRSM:
-        return wait_geq(a.potrf_done + k, 1, a.abort_flag, a.status, a.dep_limit_ns) &&
+        // tensor-core strips also need the split FP16 inverse (second release of POTRF(k))
+        return wait_geq(a.potrf_done + k, tc_strip<MIXED>(a, k, m) ? 2 : 1, a.abort_flag, a.status, a.dep_limit_ns) &&
                wait_geq(a.upd_done + (int64_t)m * a.mt + k, all_updates<MIXED>(a, m, k), a.abort_flag, a.status,
                         a.dep_limit_ns);
     case T_GEMM:
@@ -95,13 +104,17 @@ __device__ __forceinline__ unsigned char *ring16_of(double *ring)
 // producer warp
 // ---------------------------------------------------------------------------
 template <bool MIXED>
-__device__ void producer_warp(const PotrfArgs &a, SmemCtl *ctl, double *ring, const CUtensorMap *tmap)
+__device__ void producer_warp(const PotrfArgs &a, SmemCtl *ctl, double *ring, const CUtensorMap *tmap,
+                              const CUtensorMap *lmap)
 {
     constexpr uint32_t NST = MIXED ? NSTAGE_MIXED : NSTAGE;
     const int lane = threadIdx.x & 31;
     uint32_t stage_it = 0, task_it = 0, epi_it = 0, st16 = 0;
     unsigned char *ring16 = MIXED ? ring16_of(ring) : nullptr;
-    if (MIXED && lane == 0) tma_prefetch_desc(tmap);
+    if (MIXED && lane == 0) {
+        tma_prefetch_desc(tmap);
+        if (a.tc_trsm) tma_prefetch_desc(lmap);
+    }
     bool pipe_ok = true;
     int prev_mode = -1;      // MIXED: 0 FP64 ring, 1 16-bit ring (same shared memory)
     while (true) {
@@ -164,7 +177,7 @@ __device__ void producer_warp(const PotrfArgs &a, SmemCtl *ctl, double *ring, co
         if (MIXED) {
             // the FP64 ring and the 16-bit ring share memory: before the
             // first load of the other kind, the previous task must be done
-            const int mode = ty == T_GEMM ? 1 : 0;
+            const int mode = (ty == T_GEMM || (ty == T_TRSM && tc_strip<MIXED>(a, task_k(t), task_m(t)))) ? 1 : 0;
             if (prev_mode >= 0 && mode != prev_mode && task_it >= 2) {
                 const uint32_t pit = task_it - 2, pslot = pit % TASKQ;
                 if (!warp_mbar_wait(&ctl->tempty[pslot], (pit / TASKQ) & 1, a.pipe_limit_ns)) {
@@ -176,6 +189,34 @@ __device__ void producer_warp(const PotrfArgs &a, SmemCtl *ctl, double *ring, co
             prev_mode = mode;
         }
         fence_proxy_async();
+        if (ty == T_TRSM && tc_strip<MIXED>(a, task_k(t), task_m(t))) {
+            // tensor-core TRSM strip: the B operand (the inverse of L(k,k) in
+            // split FP16, 256 rows) of each of the 8 stages of K = 32; the
+            // consumer warps stage the A operand themselves
+            const int k = task_k(t);
+            const int hrow = k * MX_NB, lrow = a.mt * MX_NB + k * MX_NB;
+            for (int kx = 0; kx < MX_NB && pipe_ok; kx += MX_KC_SPLIT) {
+                const uint32_t s = st16 % MX_NST, r = st16 / MX_NST;
+                if (r > 0 && !warp_mbar_wait(&ctl->empty16[s], (r - 1) & 1, a.pipe_limit_ns)) {
+                    if (lane == 0) report(a, ST_MBAR_TIMEOUT, 13, st16, tk);
+                    pipe_ok = false;
+                    break;
+                }
+                unsigned char *st = ring16 + s * MX_STAGE_BYTES;
+                if (lane == 0) {
+                    uint64_t *bar = &ctl->full16[s];
+                    mbar_arrive_expect_tx(bar, TC_B_BYTES);
+                    tma_load_2d(st + TC_B_OFF, lmap, kx, hrow, bar);
+                    tma_load_2d(st + TC_B_OFF + TC_A_BYTES, lmap, kx, hrow + BLK, bar);
+                    tma_load_2d(st + TC_BLO_OFF, lmap, kx, lrow, bar);
+                    tma_load_2d(st + TC_BLO_OFF + TC_A_BYTES, lmap, kx, lrow + BLK, bar);
+                }
+                __syncwarp();
+                st16++;
+            }
+            if (!pipe_ok) break;
+            continue;
+        }
         if (MIXED && ty == T_GEMM) {
             // 16-bit operands by TMA tensor loads (swizzled, canonical K-major
             // UMMA layout): for every panel j of the chunk, A = P16(m,j),
@@ -379,6 +420,105 @@ __device__ __forceinline__ bool consume_job(const PotrfArgs &a, SmemCtl *ctl, co
 }
 
 // ---------------------------------------------------------------------------
+// mixed precision, tensor-core TRSM: the whole inverse of L(k,k),
+//     Linv = [W0 0; Linv10 W1]   (W0, W1 the 128-block inverses, Linv10 = -W1 L10 W0),
+// as the B operand of the strips' products, B[n][q] = Linv(n, q) / t_q * s_b in
+// split FP16, row-major (K contiguous).  t_q = scl(k, q / 128) / target is the
+// column scale the strips apply to their A operand (a power of two that keeps
+// A(i, q) ~ sqrt(A(i,i) A(q,q)) in range), s_b a power of two that brings the
+// largest |Linv(n, q) / t_q| to the target.  Called by the consumer threads of
+// POTRF(k); `red` is shared scratch of 8 doubles.
+// ---------------------------------------------------------------------------
+// Thread n forms row n of B.  The inverse's blocks are column-major (entry
+// (n, q) of a block at q * 128 + n), so the warp's loads of one column are
+// coalesced; row n reads columns 0-127 from W0 (n < 128) or Linv10, and
+// columns 128-255 from W1 (n >= 128; zeros above it).  Two passes: the
+// largest |Linv(n, q)| / t_q, then the scaled split copy, 16 columns (two
+// 16-byte stores of hi and of lo) per group.
+static_assert(NCONS == MX_NB, "linv16_task: one consumer thread per row of the inverse");
+__device__ void linv16_task(const PotrfArgs &a, int k, const double *Wk, const double *Wxk, double *red)
+{
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int n = tid;
+    const double *src0 = n < BLK ? Wk + n : Wxk + (n - BLK);          // columns 0-127
+    const double *src1 = Wk + BLK * BLK + (n - BLK);                   // columns 128-255 (n >= 128)
+    const bool has1 = n >= BLK;
+    // t_q = scl(k, q / 128) / target: powers of two, so 1 / t_q is exact
+    const double rt0 = (double)a.p16_target / (double)a.scl[k * a.nbs];
+    const double rt1 = (double)a.p16_target / (double)a.scl[k * a.nbs + 1];
+    double m0 = 0.0, m1 = 0.0;
+#pragma unroll 1
+    for (int q0 = 0; q0 < BLK; q0 += 16) {
+        double v[16];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) v[i] = __ldcg(src0 + (q0 + i) * BLK);
+#pragma unroll
+        for (int i = 0; i < 16; ++i) m0 = fmax(m0, fabs(v[i]));
+    }
+    if (has1) {
+#pragma unroll 1
+        for (int q0 = 0; q0 < BLK; q0 += 16) {
+            double v[16];
+#pragma unroll
+            for (int i = 0; i < 16; ++i) v[i] = __ldcg(src1 + (q0 + i) * BLK);
+#pragma unroll
+            for (int i = 0; i < 16; ++i) m1 = fmax(m1, fabs(v[i]));
+        }
+    }
+    double mx = fmax(m0 * rt0, m1 * rt1);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if (lane == 0) red[warp] = mx;
+    named_bar_sync(1, NCONS);
+    mx = 0.0;
+    for (int w = 0; w < NCONS / 32; ++w) mx = fmax(mx, red[w]);
+    int e2 = 0;
+    if (mx > 0.0 && mx < INFINITY) {
+        frexp((double)a.p16_target / mx, &e2);
+        e2 = max(-120, min(120, e2 - 1));
+    }
+    const double sb = ldexp(1.0, e2);
+    unsigned short *hi = a.linv16 + (int64_t)k * MX_NB * MX_NB + (int64_t)n * MX_NB;
+    unsigned short *lo = hi + (int64_t)a.mt * MX_NB * MX_NB;      // the lo rows follow all hi rows
+#pragma unroll 1
+    for (int q0 = 0; q0 < MX_NB; q0 += 16) {
+        const bool second = q0 >= BLK;
+        const double f = sb * (second ? rt1 : rt0);
+        double v[16];
+        if (!second || has1) {
+            const double *src = second ? src1 + (q0 - BLK) * BLK : src0 + q0 * BLK;
+#pragma unroll
+            for (int i = 0; i < 16; ++i) v[i] = __ldcg(src + i * BLK);
+        } else {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) v[i] = 0.0;
+        }
+        uint32_t hw[8], lw[8];
+#pragma unroll
+        for (int i = 0; i < 16; i += 2) {
+            uint32_t h2 = 0, l2 = 0;
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const double x = v[i + e] * f;
+                const __half hh = __float2half_rn((float)x);
+                h2 |= (uint32_t)__half_as_ushort(hh) << (16 * e);
+                l2 |= (uint32_t)__half_as_ushort(__float2half_rn((float)(x - (double)__half2float(hh)))) << (16 * e);
+            }
+            hw[i / 2] = h2;
+            lw[i / 2] = l2;
+        }
+        uint4 *ph = reinterpret_cast<uint4 *>(hi + q0), *pl = reinterpret_cast<uint4 *>(lo + q0);
+        ph[0] = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+        ph[1] = make_uint4(hw[4], hw[5], hw[6], hw[7]);
+        pl[0] = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+        pl[1] = make_uint4(lw[4], lw[5], lw[6], lw[7]);
+    }
+    if (tid == 0) a.linv_scl[k] = (float)sb;
+    __threadfence();
+    named_bar_sync(1, NCONS);
+}
+
+// ---------------------------------------------------------------------------
 // consumers: POTRF(k) of one diagonal tile + inverses of its 128x128 diagonal
 // blocks (src/zpotrf_L.jdf:194-206 computes the factor with
 // LAPACKE_dpotrf_work; the inverses feed the TRSM jobs).
@@ -386,6 +526,7 @@ __device__ __forceinline__ bool consume_job(const PotrfArgs &a, SmemCtl *ctl, co
 // diagonal block in shared memory and inverts it, the panel solve and the
 // trailing update run on the FP64 tensor cores.
 // ---------------------------------------------------------------------------
+template <bool MIXED>
 __device__ void potrf_task(const PotrfArgs &a, SmemCtl *ctl, double *ring, int k)
 {
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -408,7 +549,7 @@ __device__ void potrf_task(const PotrfArgs &a, SmemCtl *ctl, double *ring, int k
     auto phase = [&](int i) {
         if (a.ptrace && tid == 0) {
             const unsigned long long now = globaltimer_ns();
-            a.ptrace[8 * k + i] += now - tp;
+            a.ptrace[PTRACE_W * k + i] += now - tp;
             tp = now;
         }
     };
@@ -420,7 +561,7 @@ __device__ void potrf_task(const PotrfArgs &a, SmemCtl *ctl, double *ring, int k
             auto sub = [&](int i) {
                 if (a.ptrace && lane == 0) {
                     const unsigned long long now = globaltimer_ns();
-                    a.ptrace[8 * k + 4 + i] += now - ts;
+                    a.ptrace[PTRACE_W * k + 4 + i] += now - ts;
                     ts = now;
                 }
             };
@@ -570,6 +711,15 @@ __device__ void potrf_task(const PotrfArgs &a, SmemCtl *ctl, double *ring, int k
 
     // Inverses of the 128x128 diagonal blocks from the 32x32 ones.
     assemble_w128(T, nbi, Wk, a.nbs, Sw, warp, lane, NCONS / 32, 1, NCONS);
+    if (MIXED && a.tc_trsm) {
+        // the factor and W are complete: the first release of POTRF(k) lets
+        // the FP64 strip of the next tile row (the one on the critical path)
+        // start while this CTA forms the split FP16 inverse for the others
+        __threadfence();
+        named_bar_sync(1, NCONS);
+        if (tid == 0) red_release_add(a.potrf_done + k, 1);
+    }
+    phase(3);
     if (a.nbs == 2 && a.Wx) {
         // the off-diagonal block of the tile's inverse, Linv10 = -W1 (L10 W0),
         // so the TRSM strips are two independent products; P = L10 W0 is kept
@@ -579,13 +729,20 @@ __device__ void potrf_task(const PotrfArgs &a, SmemCtl *ctl, double *ring, int k
         double *Wxk = a.Wx + (int64_t)k * (2 * BLK * BLK);
         gemm128_tri(T + BLK, nbi, false, Wk, BLK, true, false, P, SP, 1.0, warp, lane, NCONS / 32);
         named_bar_sync(1, NCONS);
+        phase(8);
         gemm128_tri(Wk + BLK * BLK, BLK, true, P, SP, false, true, Wxk, BLK, -1.0, warp, lane, NCONS / 32);
-        // W1 beside it, so the strip's second product reads one 128 x 256 operand
-        for (int e = tid; e < BLK * BLK; e += NCONS) Wxk[BLK * BLK + e] = __ldcg(Wk + BLK * BLK + e);
+        if (a.ptrace) named_bar_sync(1, NCONS);
+        phase(9);
+        if (!(MIXED && a.tc_trsm)) {
+            // W1 beside it, so the strip's second product reads one 128 x 256 operand
+            for (int e = tid; e < BLK * BLK; e += NCONS) Wxk[BLK * BLK + e] = __ldcg(Wk + BLK * BLK + e);
+        }
         __threadfence();
         named_bar_sync(1, NCONS);
+        phase(10);
+        if (MIXED && a.tc_trsm) linv16_task(a, k, Wk, Wxk, ring);
+        phase(11);
     }
-    phase(3);
 }
 
 // ---------------------------------------------------------------------------
@@ -741,6 +898,170 @@ __device__ bool mixed_update(const PotrfArgs &a, SmemCtl *ctl, unsigned char *ri
 }
 
 // ---------------------------------------------------------------------------
+// mixed precision, split FP16: TRSM strip bi of tile (m,k) on the tensor cores,
+//     X = A Linv^T      (A = rows bi*128.. of tile (m,k), 128 x 256),
+// src/zpotrf_L.jdf:330-333 with the inverse of L(k,k) that POTRF(k) left in
+// split FP16 (linv16_task).  The consumer warps stage A themselves, scaled by
+// s_m t_q (s_m the strip's row scale, t_q the column scale of linv16_task) and
+// split into hi + lo, in the 64-byte-swizzled K-major layout of the UMMA
+// descriptor (16-byte chunk c of row r at c ^ ((r >> 1) & 3)); the producer
+// brings B by TMA.  Eight stages of K = 32 through the 16-bit ring, three
+// products each (hi hi, hi lo, lo hi) into one 128 x 256 FP32 accumulator;
+// the epilogue writes X in FP64 over A and its split FP16 copy (times s_m)
+// into P16 for the updates.  Returns false if a wait gave up.
+// ---------------------------------------------------------------------------
+__device__ bool tc_trsm(const PotrfArgs &a, SmemCtl *ctl, unsigned char *ring16, uint64_t t, uint32_t &st16,
+                        uint32_t &mx_it, uint32_t &tcuse)
+{
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int k = task_k(t), m = task_m(t), bi = task_bi(t);
+    const int nbi = a.nbi;
+    const uint32_t tmem = ctl->tmem_base;
+    double *Amk = tile_ptr(a, m, k) + bi * BLK;
+    const double sm = (double)a.scl[m * a.nbs + bi];
+    const int r = tid & (BLK - 1), kh = tid >> 7;
+    const uint32_t sw = (r >> 1) & 3;
+    const unsigned long long tq0 = (a.ptrace && tid == 0) ? globaltimer_ns() : 0;
+    bool ok = true;
+    // the A values of the next stage are loaded while this one is staged
+    double v[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) v[j] = __ldcg(Amk + (int64_t)(kh * 16 + j) * nbi + r);
+    for (int s8 = 0; s8 < MX_NB / MX_KC_SPLIT; ++s8) {
+        const uint32_t sidx = st16 % MX_NST, rr = st16 / MX_NST;
+        const int q0 = s8 * MX_KC_SPLIT + kh * 16;
+        const double f = sm * (double)a.scl[k * a.nbs + q0 / BLK] / (double)a.p16_target;
+        uint32_t hw[8], lw[8];
+#pragma unroll
+        for (int j = 0; j < 16; j += 2) {
+            uint32_t h2 = 0, l2 = 0;
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const double x = v[j + e] * f;
+                const __half hh = __float2half_rn((float)x);
+                const __half ll = __float2half_rn((float)(x - (double)__half2float(hh)));
+                h2 |= (uint32_t)__half_as_ushort(hh) << (16 * e);
+                l2 |= (uint32_t)__half_as_ushort(ll) << (16 * e);
+            }
+            hw[j / 2] = h2;
+            lw[j / 2] = l2;
+        }
+        if (s8 + 1 < MX_NB / MX_KC_SPLIT) {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) v[j] = __ldcg(Amk + (int64_t)(q0 + MX_KC_SPLIT + j) * nbi + r);
+        }
+        if (rr > 0 && !warp_mbar_wait(&ctl->empty16[sidx], (rr - 1) & 1, a.pipe_limit_ns)) {
+            if (lane == 0) report(a, ST_MBAR_TIMEOUT, 14, st16, warp);
+            ok = false;
+        }
+        if (named_bar_or(1, NCONS, !ok)) {
+            // the MMAs of the earlier stages may still run: let them finish
+            if (warp == 4 && lane == 0) umma_commit(&ctl->tmem_full);
+            warp_mbar_wait(&ctl->tmem_full, mx_it & 1, a.pipe_limit_ns);
+            mx_it++;
+            return false;
+        }
+        unsigned char *st = ring16 + sidx * MX_STAGE_BYTES;
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+            const uint32_t off = (uint32_t)r * 64 + (((uint32_t)(2 * kh + c) ^ sw) << 4);
+            *reinterpret_cast<uint4 *>(st + off) = make_uint4(hw[4 * c], hw[4 * c + 1], hw[4 * c + 2], hw[4 * c + 3]);
+            *reinterpret_cast<uint4 *>(st + TC_A_BYTES + off) =
+                make_uint4(lw[4 * c], lw[4 * c + 1], lw[4 * c + 2], lw[4 * c + 3]);
+        }
+        fence_proxy_async();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&ctl->astage[sidx]);
+        if (warp == 4) {
+            if (lane == 0) {
+                if (!mbar_wait(&ctl->full16[sidx], rr & 1, a.pipe_limit_ns) ||
+                    !mbar_wait(&ctl->astage[sidx], (tcuse >> sidx) & 1, a.pipe_limit_ns)) {
+                    report(a, ST_MBAR_TIMEOUT, 15, st16, tid);
+                    ok = false;
+                } else {
+                    tc_fence_after();
+                    const uint32_t base = smem_u32(st);
+                    const uint32_t ah = base, al = base + TC_A_BYTES, bh = base + TC_B_OFF, bl = base + TC_BLO_OFF;
+                    const uint32_t idesc = umma_idesc_f16(0, BLK, MX_NB);
+#pragma unroll
+                    for (int k16 = 0; k16 < MX_KC_SPLIT / 16; ++k16) {
+                        const uint32_t o = k16 * 32, acc = (s8 | k16) != 0;
+                        const uint64_t ahd = umma_desc_k_sw64(ah + o), bhd = umma_desc_k_sw64(bh + o);
+                        umma_f16(tmem, ahd, bhd, idesc, acc);
+                        umma_f16(tmem, ahd, umma_desc_k_sw64(bl + o), idesc, 1);
+                        umma_f16(tmem, umma_desc_k_sw64(al + o), bhd, idesc, 1);
+                    }
+                    umma_commit(&ctl->empty16[sidx]);
+                }
+            }
+            ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+        }
+        tcuse ^= 1u << sidx;
+        st16++;
+    }
+    // also after a failed wait: the barrier fires once the MMAs already issued complete
+    if (warp == 4 && lane == 0) umma_commit(&ctl->tmem_full);
+    if (!warp_mbar_wait(&ctl->tmem_full, mx_it & 1, a.pipe_limit_ns)) {
+        if (lane == 0) report(a, ST_MBAR_TIMEOUT, 16, mx_it, warp);
+        ok = false;
+    }
+    mx_it++;
+    if (named_bar_or(1, NCONS, !ok || ld_volatile(a.abort_flag))) {
+        tc_fence_before();
+        return false;
+    }
+    tc_fence_after();
+    const unsigned long long tq1 = (a.ptrace && tid == 0) ? globaltimer_ns() : 0;
+    const int lb = (warp & 3) * 32, ch = warp >> 2, row = lb + lane;
+    const double binv = 1.0 / (double)a.linv_scl[k];         // powers of two: exact
+    const double inv = binv / sm;
+    double *X = Amk + row;
+    const int64_t prow = lower_tile_index(m, k, a.mt) * nbi + bi * BLK + row;
+    unsigned short *Ph = reinterpret_cast<unsigned short *>(a.P16) + prow * nbi;
+    unsigned short *Pl = Ph + (int64_t)a.p16_rows * nbi;
+    for (int c0 = 0; c0 < BLK; c0 += 32) {
+        float acc[32];
+        tmem_ld32(tmem + ((uint32_t)lb << 16) + (uint32_t)(ch * BLK + c0), acc);
+#pragma unroll
+        for (int j8 = 0; j8 < 32; j8 += 8) {
+            // 8 columns: FP64 X (coalesced across the warp's rows) and one
+            // 16-byte store each of the hi and lo halves of X times the row scale
+            const int col = ch * BLK + c0 + j8;
+            uint32_t hw[4], lw[4];
+#pragma unroll
+            for (int j = 0; j < 8; j += 2) {
+                uint32_t h2 = 0, l2 = 0;
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    X[(int64_t)(col + j + e) * nbi] = (double)acc[j8 + j + e] * inv;
+                    const double xs = (double)acc[j8 + j + e] * binv;
+                    const __half hh = __float2half_rn((float)xs);
+                    const __half ll = __float2half_rn((float)(xs - (double)__half2float(hh)));
+                    h2 |= (uint32_t)__half_as_ushort(hh) << (16 * e);
+                    l2 |= (uint32_t)__half_as_ushort(ll) << (16 * e);
+                }
+                hw[j / 2] = h2;
+                lw[j / 2] = l2;
+            }
+            *reinterpret_cast<uint4 *>(Ph + col) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+            *reinterpret_cast<uint4 *>(Pl + col) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
+        }
+    }
+    __threadfence();
+    tc_fence_before();
+    if (a.ptrace) {
+        named_bar_sync(1, NCONS);
+        if (tid == 0) {
+            unsigned long long *pt = a.ptrace + PTRACE_W * k;
+            atomicAdd(pt + 12, 1ull);
+            atomicAdd(pt + 13, tq1 - tq0);
+            atomicAdd(pt + 14, globaltimer_ns() - tq1);
+        }
+    }
+    return true;
+}
+
+// ---------------------------------------------------------------------------
 // consumers: task loop.  Every decision to stop is taken after a barrier
 // that ORs the failure flags of all consumer warps, so no warp is ever left
 // waiting alone at a named barrier.
@@ -749,7 +1070,7 @@ template <bool MIXED>
 __device__ void consumer_warps(const PotrfArgs &a, SmemCtl *ctl, double *ring)
 {
     const int tid = threadIdx.x;
-    uint32_t stage_it = 0, task_it = 0, st16 = 0, mx_it = 0;
+    uint32_t stage_it = 0, task_it = 0, st16 = 0, mx_it = 0, tcuse = 0;
     unsigned char *ring16 = MIXED ? ring16_of(ring) : nullptr;
     int executed = 0;
     while (true) {
@@ -772,8 +1093,11 @@ __device__ void consumer_warps(const PotrfArgs &a, SmemCtl *ctl, double *ring)
         int *release = nullptr;
         bool ok = true;
         if (ty == T_POTRF) {
-            potrf_task(a, ctl, ring, k);
+            potrf_task<MIXED>(a, ctl, ring, k);
             if (!ctl->fail) release = a.potrf_done + k;
+        } else if (ty == T_TRSM && tc_strip<MIXED>(a, k, m)) {
+            ok = tc_trsm(a, ctl, ring16, t, st16, mx_it, tcuse);
+            release = a.trsm_done + (int64_t)m * a.mt + k;
         } else if (MIXED && ty == T_GEMM) {
             ok = mixed_update(a, ctl, ring16, t, st16, mx_it);
             release = a.upd_done + (int64_t)m * a.mt + n;
@@ -825,7 +1149,8 @@ __device__ void consumer_warps(const PotrfArgs &a, SmemCtl *ctl, double *ring)
 // the 16-bit panel copies); the FP64 instantiation ignores tmap.
 template <bool MIXED>
 __global__ void __launch_bounds__(NTHREADS, 1)
-    potrf_persistent_kernel(PotrfArgs a, const __grid_constant__ CUtensorMap tmap)
+    potrf_persistent_kernel(PotrfArgs a, const __grid_constant__ CUtensorMap tmap,
+                            const __grid_constant__ CUtensorMap lmap)
 {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     SmemCtl *ctl = reinterpret_cast<SmemCtl *>(smem_raw);
@@ -843,6 +1168,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         for (int s = 0; s < MX_NST; ++s) {
             mbar_init(&ctl->full16[s], 1);
             mbar_init(&ctl->empty16[s], 1);
+            mbar_init(&ctl->astage[s], NCONS / 32);
         }
         mbar_init(&ctl->tmem_full, 1);
         mbar_init(&ctl->epi, 1);
@@ -857,7 +1183,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
     if (threadIdx.x >= NCONS) {
         asm volatile("setmaxnreg.dec.sync.aligned.u32 %0;\n" ::"n"(PRODUCER_REGS));
         if (threadIdx.x < NCONS + 32) {
-            producer_warp<MIXED>(a, ctl, ring, &tmap);
+            producer_warp<MIXED>(a, ctl, ring, &tmap, &lmap);
             if (a.trace && threadIdx.x == NCONS) a.trace_exit[8 * blockIdx.x] = globaltimer_ns();
         }
     } else {
@@ -1136,6 +1462,24 @@ int potrf_device(Context *ctx, double *dA, int mt, int nbi, int nb_user, int n_u
     return potrf_run(ctx, dA, mt, nbi, nb_user, n_user, info, -1);
 }
 
+// Tensor-core TRSM strips (split FP16 only): the inverses of the diagonal
+// tiles in split FP16 (rows of 256, hi rows of all tiles then lo rows) with
+// one scale per tile, and their tensor map (boxes of 32 x 128, 64-byte
+// swizzle, the K-major layout of the strips' B operand).
+static int setup_tc_trsm(Context *ctx, PotrfArgs &a, CUtensorMap *lmap, int mt)
+{
+    const size_t hbytes = (size_t)2 * mt * MX_NB * MX_NB * sizeof(unsigned short);
+    unsigned char *lb = (unsigned char *)ctx->buffer(BUF_LINV16, hbytes + 256 + (size_t)mt * sizeof(float));
+    if (!lb) return DPLASMA_ERR_OUT_OF_RESOURCES;
+    a.linv16 = (unsigned short *)lb;
+    a.linv_scl = (float *)(lb + ((hbytes + 255) / 256) * 256);
+    const int e = encode_map_2d(ctx, lmap, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, lb, MX_NB, (uint64_t)2 * mt * MX_NB,
+                                MX_NB * sizeof(unsigned short), MX_KC_SPLIT, BLK, CU_TENSOR_MAP_SWIZZLE_64B);
+    if (e) return e;
+    a.tc_trsm = 1;
+    return 0;
+}
+
 // p16_fmt < 0: FP64 updates; 0: FP16; 1: BF16; 2: split FP16 (hi + lo).
 int potrf_run(Context *ctx, double *dA, int mt, int nbi, int nb_user, int n_user, int *info, int p16_fmt)
 {
@@ -1175,10 +1519,13 @@ int potrf_run(Context *ctx, double *dA, int mt, int nbi, int nb_user, int n_user
     // opt-in: TRSM strips of 256-wide tiles as two independent products on the
     // tile's whole inverse (strips 84 -> 70 us, but POTRF +55 us on the
     // critical path: no net gain at N = 32768 .. 65536)
-    double *Wx = nbs == 2 && ctx->trsm_inv
+    // opt-in: mixed split FP16 TRSM strips on the tensor cores (the inverse's
+    // second block row is then needed as well)
+    const bool tc = mixed && nbs == 2 && p16_fmt == 2 && ctx->trsm_tc;
+    double *Wx = nbs == 2 && (ctx->trsm_inv || tc)
                      ? (double *)ctx->buffer(BUF_WX, (size_t)mt * 2 * BLK * BLK * sizeof(double))
                      : nullptr;
-    if (nbs == 2 && ctx->trsm_inv && !Wx) return DPLASMA_ERR_OUT_OF_RESOURCES;
+    if (nbs == 2 && (ctx->trsm_inv || tc) && !Wx) return DPLASMA_ERR_OUT_OF_RESOURCES;
     const size_t nctr = 8 + (size_t)mt + 2 * (size_t)mt * mt + grid;
     int *ctr = (int *)ctx->buffer(BUF_COUNTERS, nctr * sizeof(int));
     if (!W || !ctr) return DPLASMA_ERR_OUT_OF_RESOURCES;
@@ -1223,9 +1570,9 @@ int potrf_run(Context *ctx, double *dA, int mt, int nbi, int nb_user, int n_user
         a.trace_exit = a.trace + (size_t)a.ntasks * 4;
         a.trace_cta = (int *)(a.trace_exit + 8 * (size_t)grid);
         CK(cudaMemsetAsync(a.trace, 0, tbytes, st));
-        a.ptrace = (unsigned long long *)ctx->buffer(BUF_PTRACE, (size_t)mt * 8 * sizeof(unsigned long long));
+        a.ptrace = (unsigned long long *)ctx->buffer(BUF_PTRACE, (size_t)mt * PTRACE_W * sizeof(unsigned long long));
         if (!a.ptrace) return DPLASMA_ERR_OUT_OF_RESOURCES;
-        CK(cudaMemsetAsync(a.ptrace, 0, (size_t)mt * 8 * sizeof(unsigned long long), st));
+        CK(cudaMemsetAsync(a.ptrace, 0, (size_t)mt * PTRACE_W * sizeof(unsigned long long), st));
     }
     a.dep_limit_ns = ctx->dep_limit_ns;
     a.pipe_limit_ns = ctx->pipe_limit_ns;
@@ -1256,6 +1603,15 @@ int potrf_run(Context *ctx, double *dA, int mt, int nbi, int nb_user, int n_user
         const int e = make_p16_map(ctx, &tmap, pb, (split ? 2 : 1) * rows, nbi, a.p16_fmt, split);
         if (e) return e;
     }
+    CUtensorMap lmap;
+    memset(&lmap, 0, sizeof(lmap));
+    a.tc_trsm = 0;
+    a.linv16 = nullptr;
+    a.linv_scl = nullptr;
+    if (tc) {
+        const int e = setup_tc_trsm(ctx, a, &lmap, mt);
+        if (e) return e;
+    }
 
     const size_t smem = potrf_smem_bytes(mixed);
     CK(cudaEventRecord(ctx->ev0, st));
@@ -1264,10 +1620,10 @@ int potrf_run(Context *ctx, double *dA, int mt, int nbi, int nb_user, int n_user
         CK(cudaGetLastError());
         ctx->launches += 1;
         CK(cudaFuncSetAttribute(potrf_persistent_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        potrf_persistent_kernel<true><<<grid, NTHREADS, smem, st>>>(a, tmap);
+        potrf_persistent_kernel<true><<<grid, NTHREADS, smem, st>>>(a, tmap, lmap);
     } else {
         CK(cudaFuncSetAttribute(potrf_persistent_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        potrf_persistent_kernel<false><<<grid, NTHREADS, smem, st>>>(a, tmap);
+        potrf_persistent_kernel<false><<<grid, NTHREADS, smem, st>>>(a, tmap, lmap);
     }
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->ev1, st));
@@ -1326,12 +1682,15 @@ int potrf_run(Context *ctx, double *dA, int mt, int nbi, int nb_user, int n_user
                         task_n(t), task_bi(t), task_bj(t), rel(tr[4 * i]), rel(tr[4 * i + 1]), rel(tr[4 * i + 2]),
                         rel(tr[4 * i + 3]), tc[i]);
             }
-            std::vector<unsigned long long> pt((size_t)mt * 8);
+            std::vector<unsigned long long> pt((size_t)mt * PTRACE_W);
             cudaMemcpy(pt.data(), a.ptrace, pt.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost);
-            for (int k = 0; k < mt; ++k)
+            for (int k = 0; k < mt; ++k) {
+                const unsigned long long *q = pt.data() + (size_t)PTRACE_W * k;
                 fprintf(f, "# potrf %d diag_ns %llu panel_ns %llu update_ns %llu inverse_ns %llu load_ns %llu chol_ns %llu "
-                           "store_ns %llu inv32_ns %llu\n", k, pt[8 * k], pt[8 * k + 1], pt[8 * k + 2], pt[8 * k + 3],
-                        pt[8 * k + 4], pt[8 * k + 5], pt[8 * k + 6], pt[8 * k + 7]);
+                           "store_ns %llu inv32_ns %llu l10w0_ns %llu linv10_ns %llu w1copy_ns %llu linv16_ns %llu "
+                           "tc_strips %llu tc_stage_ns %llu tc_epilogue_ns %llu\n",
+                        k, q[0], q[1], q[2], q[3], q[4], q[5], q[6], q[7], q[8], q[9], q[10], q[11], q[12], q[13], q[14]);
+            }
             for (int c = 0; c < grid; ++c)
                 fprintf(f, "# cta %d producer_exit %lld consumer_exit %lld potrf_wait_done %lld end_pushed %lld end_seen %lld "
                            "mixed_tasks %llu mixed_wait_plus_epilogue_ns %llu mixed_epilogue_ns %llu\n", c,
@@ -1394,11 +1753,15 @@ int potrf_run_streamed(Context *ctx, const double *hA, double *A0, double *L, in
     int *ctr = (int *)ctx->buffer(BUF_COUNTERS, nctr * sizeof(int));
     if (!W || !ctr) return DPLASMA_ERR_OUT_OF_RESOURCES;
 
+    const bool tc = nbs == 2 && p16_fmt == 2 && ctx->trsm_tc;
+    double *Wx = tc ? (double *)ctx->buffer(BUF_WX, (size_t)mt * 2 * BLK * BLK * sizeof(double)) : nullptr;
+    if (tc && !Wx) return DPLASMA_ERR_OUT_OF_RESOURCES;
+
     PotrfArgs a;
     memset(&a, 0, sizeof(a));
     a.A = L;
     a.W = W;
-    a.Wx = nullptr;
+    a.Wx = Wx;
     a.mt = mt;
     a.nbi = nbi;
     a.nbs = nbs;
@@ -1434,6 +1797,9 @@ int potrf_run_streamed(Context *ctx, const double *hA, double *A0, double *L, in
     memset(&tmap, 0, sizeof(tmap));
     int e = make_p16_map(ctx, &tmap, pb, (split ? 2 : 1) * rows, nbi, a.p16_fmt, split);
     if (e) return e;
+    CUtensorMap lmap;
+    memset(&lmap, 0, sizeof(lmap));
+    if (tc && (e = setup_tc_trsm(ctx, a, &lmap, mt)) != 0) return e;
     const size_t smem = potrf_smem_bytes(true);
     CK(cudaFuncSetAttribute(potrf_persistent_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 
@@ -1489,7 +1855,7 @@ int potrf_run_streamed(Context *ctx, const double *hA, double *A0, double *L, in
         CK(cudaMemsetAsync(ctr, 0, sizeof(int), st));      // the ticket counter restarts each launch
         a.tasks = tasks + ctx->ph_off[p];
         a.ntasks = (int)(ctx->ph_off[q] - ctx->ph_off[p]);
-        potrf_persistent_kernel<true><<<grid, NTHREADS, smem, st>>>(a, tmap);
+        potrf_persistent_kernel<true><<<grid, NTHREADS, smem, st>>>(a, tmap, lmap);
         CK(cudaGetLastError());
         for (int r = p; r < q; ++r) CK(cudaEventRecord(ev.v[nph + 1 + r], st));   // phases p..q-1 done
         ctx->launches += 1;
@@ -1633,13 +1999,16 @@ int potrf_launch_prealloc(cudaStream_t st, double *dA, int mt, int nbi, int nb_u
     a.mx_split = 0;
     a.mx_chunk = 1;
     a.p16_rows = 0;
+    a.tc_trsm = 0;
+    a.linv16 = nullptr;
+    a.linv_scl = nullptr;
     CUtensorMap tmap;
     memset(&tmap, 0, sizeof(tmap));
     const size_t smem = potrf_smem_bytes(false);
     if (cudaFuncSetAttribute(potrf_persistent_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
         cudaSuccess)
         return DPLASMA_ERR_UNEXPECTED;
-    potrf_persistent_kernel<false><<<grid, NTHREADS, smem, st>>>(a, tmap);
+    potrf_persistent_kernel<false><<<grid, NTHREADS, smem, st>>>(a, tmap, tmap);
     if (cudaGetLastError() != cudaSuccess) return DPLASMA_ERR_UNEXPECTED;
     int hs[8];
     if (cudaMemcpyAsync(hs, ctr, sizeof(hs), cudaMemcpyDeviceToHost, st) != cudaSuccess) return DPLASMA_ERR_UNEXPECTED;

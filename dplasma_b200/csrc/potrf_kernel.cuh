@@ -61,6 +61,18 @@ constexpr int MX_BLOCK = BLK * MX_KC * 2;          // 16 KB: 128 rows of a singl
 constexpr int MX_SPLIT_BLOCK = BLK * MX_KC_SPLIT * 2;   // 8 KB: 128 rows of one split half
 constexpr int MX_TMEM_COLS = 512;                  // two 128 x 256 FP32 accumulators
 constexpr int MX_NB = 256;
+// Tensor-core TRSM stage (K = 32 of the strip, split form) inside a 64 KB slot:
+//   A_hi rows 0-127 | A_lo rows 0-127 | B_hi rows 0-255 | B_lo rows 0-255
+constexpr int TC_A_BYTES = BLK * MX_KC_SPLIT * 2;   // 8 KB, written by the consumer warps
+constexpr int TC_B_OFF = 2 * TC_A_BYTES;            // B by TMA (Linv in split FP16)
+constexpr int TC_BLO_OFF = TC_B_OFF + 2 * TC_A_BYTES;
+constexpr int TC_B_BYTES = 4 * TC_A_BYTES;          // 32 KB per stage
+// Trace slots per step k (ptrace): POTRF(k) diagonal blocks, panels, updates,
+// 128-block inverses, and inside the diagonal blocks load, factor, store,
+// 32-block inverse; then the tile inverse's parts (L10 W0, -W1 (L10 W0), W1
+// copy, split FP16 copy) and the tensor-core TRSM strips of step k (count, ns
+// until the accumulator was ready, ns of the epilogue).
+constexpr int PTRACE_W = 16;
 
 // Task encoding (64 bits): type[0:4) k[4:20) m[20:36) n[36:52) bi[52:56) bj[56:60)
 enum : int { T_END = 0, T_POTRF = 1, T_TRSM = 2, T_GEMM = 3 };
@@ -102,7 +114,7 @@ struct PotrfArgs {
     unsigned long long *trace; // opt-in, 4 per ticket: fetched, dependencies met, started, finished (ns); may be null
     unsigned long long *trace_exit; // 2 per CTA: producer and consumer exit times
     int *trace_cta;        // CTA that ran each ticket
-    unsigned long long *ptrace; // opt-in, 4 per POTRF(k): ns spent in its diagonal blocks, panels, updates, inverses
+    unsigned long long *ptrace; // opt-in, PTRACE_W per step k: ns spent in the parts of POTRF(k), TRSM strips of step k
     uint64_t dep_limit_ns; // bounded dependency waits
     uint64_t pipe_limit_ns;// bounded pipeline waits
     // mixed precision: 16-bit K-major copies of the panel tiles and their
@@ -114,6 +126,13 @@ struct PotrfArgs {
     int mx_split;          // 1: each panel value is hi + lo (two fp16), lo rows follow at +p16_rows
     int mx_chunk;          // panels accumulated in tensor memory per update task
     int p16_rows;          // rows of the hi part of P16
+    // mixed precision, TRSM strips on the 16-bit tensor cores (nbs == 2): POTRF(k)
+    // writes the whole inverse of L(k,k) in split FP16 (hi rows of every tile,
+    // then the lo rows: row k*256 + n holds Linv(n, :) scaled) and its
+    // power-of-two scale linv_scl[k]
+    int tc_trsm;
+    unsigned short *linv16;
+    float *linv_scl;
 };
 
 __device__ __forceinline__ double *tile_ptr(const PotrfArgs &a, int m, int n)
@@ -148,7 +167,7 @@ __device__ __forceinline__ int task_njobs(const PotrfArgs &a, uint64_t t)
 {
     int ty = task_type(t);
     if (ty == T_GEMM) return 1;
-    if (ty == T_TRSM) return (a.nbs == 2 && a.Wx) ? 2 : 2 * a.nbs - 1;
+    if (ty == T_TRSM) return (a.nbs == 2 && a.Wx && !a.tc_trsm) ? 2 : 2 * a.nbs - 1;
     return 0;
 }
 __device__ __forceinline__ Job task_job(const PotrfArgs &a, uint64_t t, int j)
@@ -167,7 +186,7 @@ __device__ __forceinline__ Job task_job(const PotrfArgs &a, uint64_t t, int j)
         jb.signal = false;
         jb.p16 = nullptr;
         jb.p16_scale = 1.f;
-    } else if (a.nbs == 2 && a.Wx) {
+    } else if (a.nbs == 2 && a.Wx && !a.tc_trsm) {
         // TRSM strip bi of a 256-wide tile (m,k) with the whole inverse of
         // L(k,k) = [L00 0; L10 L11]:  L^-1 = [W0 0; Linv10 W1],
         //   X1 = A0 Linv10^T + A1 W1^T  (job 0, K = 256),   X0 = A0 W0^T  (job 1, K = 128).
@@ -236,6 +255,7 @@ struct __align__(16) SmemCtl {
     uint64_t task[TASKQ];
     uint64_t full16[MX_NST];
     uint64_t empty16[MX_NST];
+    uint64_t astage[MX_NST];   // tensor-core TRSM: the consumer warps staged the A operand
     uint64_t tmem_full;
     int tick[TASKQ];
     int fail;

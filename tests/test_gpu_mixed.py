@@ -219,3 +219,55 @@ def test_dsposv_rejects_bad_shift(gpu_ctx):
     A = oracle.dplgsy(N, NB, 3872, bump=float(N))
     rc, _, _, _, _ = run_dsposv(gpu_ctx, A, np.ones((N, 1)), NB, db.Lower, shift=-1.0)
     assert rc == db.ERR_ILLEGAL_VALUE
+
+
+@pytest.fixture
+def tc_ctx():
+    """A context with the tensor-core TRSM strips (DPLASMA_B200_TRSM_TC=1):
+    the mixed split-FP16 factorization solves its panels as X = A Linv^T on
+    the 16-bit tensor cores instead of FP64 DMMA."""
+    import os
+    old = os.environ.get("DPLASMA_B200_TRSM_TC")
+    os.environ["DPLASMA_B200_TRSM_TC"] = "1"
+    try:
+        ctx = db.Context(0)
+    finally:
+        if old is None:
+            del os.environ["DPLASMA_B200_TRSM_TC"]
+        else:
+            os.environ["DPLASMA_B200_TRSM_TC"] = old
+    yield ctx
+    ctx.close()
+
+
+@pytest.mark.parametrize("N,kappa", [(2048, 1e2), (2048, 1e6), (4096, 1e6), (1536, 1e4)])
+def test_dsposv_tensor_core_trsm(gpu_ctx, tc_ctx, N, kappa):
+    # the panels in split FP16 products (about 2^-22 relative) keep the factor
+    # as good a preconditioner as the FP64 panels: at most one more refinement
+    # step, and the same dsposv accuracy
+    NB, NRHS = 256, 8
+    A = householder_spd(N, kappa)
+    Xt = np.random.default_rng(8).standard_normal((N, NRHS))
+    B = A @ Xt
+    rc0, st0, X0, _, _ = run_dsposv(gpu_ctx, A, B, NB, db.Lower, fmt=db.FP16_SPLIT)
+    rc, st, X, _, _ = run_dsposv(tc_ctx, A, B, NB, db.Lower, fmt=db.FP16_SPLIT)
+    assert rc0 == 0 and rc == 0, tc_ctx.last_error()
+    assert st["fallback"] == 0 and st["fmt_used"] == db.FP16_SPLIT, st
+    assert st["iter"] <= st0["iter"] + 1, (st, st0)
+    assert st["backward_error"] < 10 * N * EPS, st
+    assert daxmb_ratio(A, X, B) < 10.0
+    X64 = run_dposv(gpu_ctx, A, B, NB, db.Lower)
+    assert np.abs(X - X64).max() / np.abs(X64).max() <= max(kappa * N * EPS, 1e-12)
+    print(f"N={N} kappa={kappa:.0e}: iterations {st['iter']} (FP64 panels {st0['iter']})")
+
+
+def test_dsposv_tensor_core_trsm_dplgsy_ragged(tc_ctx):
+    # nb 200 -> 256-wide internal tiles with an identity-padded last tile
+    N, NB, NRHS = 1300, 200, 3
+    A = oracle.dplgsy(N, NB, 3872, bump=float(N))
+    B = oracle.dplrnt(N, NRHS, NB, NB, 3873)
+    rc, st, X, _, _ = run_dsposv(tc_ctx, A, B, NB, db.Lower, fmt=db.FP16_SPLIT)
+    assert rc == 0, tc_ctx.last_error()
+    assert st["fallback"] == 0 and st["fmt_used"] == db.FP16_SPLIT, st
+    assert st["backward_error"] < 10 * N * EPS
+    assert daxmb_ratio(A, X, B) < 10.0
