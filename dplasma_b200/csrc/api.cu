@@ -159,7 +159,7 @@ extern "C" parsec_context_t *dplasma_b200_init(int device)
     ctx->solve_grid = ctx->sms * (occs < 1 ? 1 : occs);
     ctx->self_check = getenv_int("DPLASMA_B200_SELFCHECK", 0) != 0;
     ctx->trsm_inv = getenv_int("DPLASMA_B200_TRSM_INV", 0) != 0;
-    ctx->trsm_tc = getenv_int("DPLASMA_B200_TRSM_TC", 0) != 0;
+    ctx->trsm_tc = getenv_int("DPLASMA_B200_TRSM_TC", 1) != 0;
     if (const char *tp = getenv("DPLASMA_B200_TRACE")) snprintf(ctx->trace_path, sizeof(ctx->trace_path), "%s", tp);
     const int lim_ms = getenv_int("DPLASMA_B200_WAIT_LIMIT_MS", 4000);
     ctx->dep_limit_ns = (uint64_t)lim_ms * 1000000ull;

@@ -70,7 +70,7 @@ struct Context {
     uint64_t pipe_limit_ns = 4000000000ull;  // 4 s
     bool self_check = false;
     bool trsm_inv = false;                   // DPLASMA_B200_TRSM_INV: 256-wide TRSM strips on the tile's whole inverse
-    bool trsm_tc = false;                    // DPLASMA_B200_TRSM_TC: mixed split-FP16 TRSM strips on the tensor cores
+    bool trsm_tc = true;                     // DPLASMA_B200_TRSM_TC (default 1): split-FP16 TRSM strips on the tensor cores
     void *bufs[BUF_COUNT] = {};
     size_t bufsz[BUF_COUNT] = {};
     int task_mt = -1, task_nbs = -1, task_delay = -1, ntasks = 0;

@@ -221,27 +221,40 @@ def test_dsposv_rejects_bad_shift(gpu_ctx):
     assert rc == db.ERR_ILLEGAL_VALUE
 
 
-@pytest.fixture
-def tc_ctx():
-    """A context with the tensor-core TRSM strips (DPLASMA_B200_TRSM_TC=1):
-    the mixed split-FP16 factorization solves its panels as X = A Linv^T on
-    the 16-bit tensor cores instead of FP64 DMMA."""
+def _ctx_with_trsm_tc(value):
     import os
     old = os.environ.get("DPLASMA_B200_TRSM_TC")
-    os.environ["DPLASMA_B200_TRSM_TC"] = "1"
+    os.environ["DPLASMA_B200_TRSM_TC"] = value
     try:
-        ctx = db.Context(0)
+        return db.Context(0)
     finally:
         if old is None:
             del os.environ["DPLASMA_B200_TRSM_TC"]
         else:
             os.environ["DPLASMA_B200_TRSM_TC"] = old
+
+
+@pytest.fixture
+def tc_ctx():
+    """A context with the tensor-core TRSM strips (DPLASMA_B200_TRSM_TC=1, the
+    default): the mixed split-FP16 factorization solves its panels as
+    X = A Linv^T on the 16-bit tensor cores instead of FP64 DMMA."""
+    ctx = _ctx_with_trsm_tc("1")
+    yield ctx
+    ctx.close()
+
+
+@pytest.fixture
+def fp64_strip_ctx():
+    """A context whose split-FP16 factorization keeps its TRSM strips in FP64
+    (DPLASMA_B200_TRSM_TC=0)."""
+    ctx = _ctx_with_trsm_tc("0")
     yield ctx
     ctx.close()
 
 
 @pytest.mark.parametrize("N,kappa", [(2048, 1e2), (2048, 1e6), (4096, 1e6), (1536, 1e4)])
-def test_dsposv_tensor_core_trsm(gpu_ctx, tc_ctx, N, kappa):
+def test_dsposv_tensor_core_trsm(fp64_strip_ctx, tc_ctx, N, kappa):
     # the panels in split FP16 products (about 2^-22 relative) keep the factor
     # as good a preconditioner as the FP64 panels: at most one more refinement
     # step, and the same dsposv accuracy
@@ -249,14 +262,14 @@ def test_dsposv_tensor_core_trsm(gpu_ctx, tc_ctx, N, kappa):
     A = householder_spd(N, kappa)
     Xt = np.random.default_rng(8).standard_normal((N, NRHS))
     B = A @ Xt
-    rc0, st0, X0, _, _ = run_dsposv(gpu_ctx, A, B, NB, db.Lower, fmt=db.FP16_SPLIT)
+    rc0, st0, X0, _, _ = run_dsposv(fp64_strip_ctx, A, B, NB, db.Lower, fmt=db.FP16_SPLIT)
     rc, st, X, _, _ = run_dsposv(tc_ctx, A, B, NB, db.Lower, fmt=db.FP16_SPLIT)
     assert rc0 == 0 and rc == 0, tc_ctx.last_error()
     assert st["fallback"] == 0 and st["fmt_used"] == db.FP16_SPLIT, st
     assert st["iter"] <= st0["iter"] + 1, (st, st0)
     assert st["backward_error"] < 10 * N * EPS, st
     assert daxmb_ratio(A, X, B) < 10.0
-    X64 = run_dposv(gpu_ctx, A, B, NB, db.Lower)
+    X64 = run_dposv(tc_ctx, A, B, NB, db.Lower)
     assert np.abs(X - X64).max() / np.abs(X64).max() <= max(kappa * N * EPS, 1e-12)
     print(f"N={N} kappa={kappa:.0e}: iterations {st['iter']} (FP64 panels {st0['iter']})")
 
