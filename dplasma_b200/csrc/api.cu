@@ -161,6 +161,8 @@ extern "C" parsec_context_t *dplasma_b200_init(int device)
     ctx->trsm_inv = getenv_int("DPLASMA_B200_TRSM_INV", 0) != 0;
     ctx->trsm_tc = getenv_int("DPLASMA_B200_TRSM_TC", 1) != 0;
     if (const char *tp = getenv("DPLASMA_B200_TRACE")) snprintf(ctx->trace_path, sizeof(ctx->trace_path), "%s", tp);
+    if (const char *tp = getenv("DPLASMA_B200_WAVE_TRACE"))
+        snprintf(ctx->wave_trace_path, sizeof(ctx->wave_trace_path), "%s", tp);
     const int lim_ms = getenv_int("DPLASMA_B200_WAIT_LIMIT_MS", 4000);
     ctx->dep_limit_ns = (uint64_t)lim_ms * 1000000ull;
     ctx->pipe_limit_ns = (uint64_t)lim_ms * 1000000ull;

@@ -42,6 +42,7 @@ enum BufferId : int {
     BUF_SELFCHECK,    // per-ticket run counters (self check)
     BUF_WX,           // second block row [Linv10 | W1] of the inverses of 256-wide diagonal tiles
     BUF_LINV16,       // inverses of the diagonal tiles in split FP16 (tensor-core TRSM strips)
+    BUF_WTRACE,       // opt-in trace of the triangular sweeps
     BUF_TASKS_PH,     // phased ticket order of the streamed factorization
     BUF_WM,           // triangular sweeps: the critical path's products W_b L_{b,b-1}
     BUF_COUNT
@@ -92,6 +93,7 @@ struct Context {
     BatchGraph bt_graph[2];                  // FP64, FP32
     char errmsg[512] = {0};
     char trace_path[512] = {0};   // DPLASMA_B200_TRACE: per-task timestamps of the scheduler
+    char wave_trace_path[512] = {0};   // DPLASMA_B200_WAVE_TRACE: per-sweep summary of the triangular sweeps
 
     // grow-only device buffer; bytes == 0 returns the current one
     void *buffer(int id, size_t bytes)

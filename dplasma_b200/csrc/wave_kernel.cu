@@ -38,6 +38,9 @@
 #include "dev_trtri.cuh"
 #include "internal.h"
 
+#include <stdio.h>
+#include <vector>
+
 namespace db2 {
 
 constexpr int WV_RMAX = 4;
@@ -63,7 +66,10 @@ struct WaveArgs {
     int *status;
     uint64_t limit_ns;
     uint32_t smem_bytes;   // dynamic shared memory of the launch
+    // opt-in trace: per CTA WV_TR_SLOTS ns counters, then the publish time of every block
+    unsigned long long *trace;
 };
+constexpr int WV_TR_SLOTS = 8;   // flag wait, Y staging, M + publish, deferred, L(nnq) + Z, rest, positions, -
 
 struct __align__(16) WaveCtl {
     uint64_t full[WV_NST_MAX];
@@ -98,9 +104,11 @@ __device__ __forceinline__ int wv_aidx(int r, int k)
     return (TRANS ? slab * 2048 : slab * 512) + line * 16 + ((((j >> 1) ^ (line & 7)) << 1) | (j & 1));
 }
 
-// Solve order position qi -> block q, and its successor.
+// Solve order position qi -> block q, and block p -> its position.
 template <bool TRANS>
 __device__ __forceinline__ int wv_block(int qi, int P) { return TRANS ? P - 1 - qi : qi; }
+template <bool TRANS>
+__device__ __forceinline__ int wv_pos(int p, int P) { return TRANS ? P - 1 - p : p; }
 
 template <int NC, bool TRANS>
 __global__ void __launch_bounds__(WV_THREADS, 1)
@@ -177,19 +185,43 @@ __global__ void __launch_bounds__(WV_THREADS, 1)
             else wv_lcoord(a, p, q, x, y);
             issue(&lmap, x, y);
         };
+        // the consumers' order: W of the first block (its owner), W of the
+        // second (Z before position 0); per position: M(nq) if owned, the
+        // products deferred at the previous position, then either L(nnq, q)
+        // and W(nnq) if nnq is owned (the other products deferred) or L(p, q)
+        // for every other owned block still to solve
         const int first = wv_block<TRANS>(0, P);
         if (first % G == c) issue(&wmap, 0, first * 128);
+        if (P > 1 && wv_block<TRANS>(1, P) % G == c) issue(&wmap, 0, wv_block<TRANS>(1, P) * 128);
         for (int qi = 0; qi < P && ok; ++qi) {
             const int q = wv_block<TRANS>(qi, P);
             const int nq = (qi + 1 < P) ? wv_block<TRANS>(qi + 1, P) : -1;
-            if (nq >= 0 && nq % G == c) {
-                issue(&wmap, 0, nq * 128);
-                issue(&mmap, 0, nq * 128);
-            }
-            for (int i = 0; i < WV_RMAX && ok; ++i) {
+            const int nnq = (qi + 2 < P) ? wv_block<TRANS>(qi + 2, P) : -1;
+            bool any = false;
+            for (int i = 0; i < WV_RMAX; ++i) {
                 const int p = c + i * G;
-                if (p >= P || p == nq || !(TRANS ? p < q : p > q)) continue;
-                issue_l(p, q);
+                any |= (p < P) && (TRANS ? p < q : p > q);
+            }
+            if (!any) continue;
+            if (nq >= 0 && nq % G == c) {
+                issue(&mmap, 0, nq * 128);
+                if (qi >= 1) {
+                    const int pq = wv_block<TRANS>(qi - 1, P);
+                    for (int i = 0; i < WV_RMAX && ok; ++i) {
+                        const int p = c + i * G;
+                        if (p < P && wv_pos<TRANS>(p, P) > qi + 1) issue_l(p, pq);
+                    }
+                }
+            }
+            if (nnq >= 0 && nnq % G == c) {
+                issue_l(nnq, q);
+                issue(&wmap, 0, nnq * 128);
+            } else {
+                for (int i = 0; i < WV_RMAX && ok; ++i) {
+                    const int p = c + i * G;
+                    if (p >= P || p == nq || !(TRANS ? p < q : p > q)) continue;
+                    issue_l(p, q);
+                }
             }
         }
         const uint32_t fst = it > WV_NST ? it - WV_NST : 0;
@@ -219,7 +251,19 @@ __global__ void __launch_bounds__(WV_THREADS, 1)
     bool ok = true;
 
     // acc_i -= op(L) * Ystage, four stages from the ring
+    // The Y stages hold -Y, so the products accumulate without negating
+    // their fragments; up to 16 columns, two partial sums (even and odd k
+    // steps) give each warp four or more independent accumulator chains,
+    // added to ac at the end (one partial sum above: the registers).
+    constexpr int NPART = NT <= 2 ? 2 : 1;
     auto update = [&](double (&ac)[NT][4], const double *Yst) {
+        double part[NPART][NT][4];
+#pragma unroll
+        for (int h = 0; h < NPART; ++h)
+#pragma unroll
+            for (int ni = 0; ni < NT; ++ni)
+#pragma unroll
+                for (int e = 0; e < 4; ++e) part[h][ni][e] = 0.0;
         for (int s0 = 0; s0 < 128 && ok; s0 += WV_KS) {
             const uint32_t s = it % WV_NST, r = it / WV_NST;
             if (!warp_mbar_wait(&ctl->full[s], r & 1, a.limit_ns)) {
@@ -233,12 +277,17 @@ __global__ void __launch_bounds__(WV_THREADS, 1)
                 const double a0 = As[wv_aidx<TRANS>(ra, kk + t)];
                 const double a1 = As[wv_aidx<TRANS>(rb, kk + t)];
 #pragma unroll
-                for (int ni = 0; ni < NT; ++ni) dmma_16x8x4(ac[ni], -a0, -a1, Yst[(ni * 8 + g) * WV_YP + s0 + kk + t]);
+                for (int ni = 0; ni < NT; ++ni)
+                    dmma_16x8x4(part[(kk >> 2) % NPART][ni], a0, a1, Yst[(ni * 8 + g) * WV_YP + s0 + kk + t]);
             }
             __syncwarp();
             if (lane == 0) mbar_arrive(&ctl->empty[s]);
             ++it;
         }
+#pragma unroll
+        for (int ni = 0; ni < NT; ++ni)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) ac[ni][e] += NPART == 2 ? part[0][ni][e] + part[NPART - 1][ni][e] : part[0][ni][e];
     };
     // res = op(W_qq) * ac (W streamed through the ring), ac staged in Yst; ac is cleared
     auto wmul = [&](double (&ac)[NT][4], double *Yst, double (&res)[NT][4]) {
@@ -274,9 +323,10 @@ __global__ void __launch_bounds__(WV_THREADS, 1)
         }
         named_bar_sync(1, 256);   // Yst is free again
     };
-    // the solved block to shared memory (for this CTA's own updates), to
-    // global memory, then its flag
-    auto publish = [&](const double (&y)[NT][4], double *Yst, int q) {
+    // the solved block to global memory, then its flag; its copy in shared
+    // memory (for this CTA's own updates) is written afterwards by own_stage,
+    // once the deferred products no longer read that buffer
+    auto publish = [&](const double (&y)[NT][4], int q) {
         double *Yq = a.Y + (int64_t)a.c0 * a.ldy + (int64_t)q * 128;
 #pragma unroll
         for (int ni = 0; ni < NT; ++ni)
@@ -284,7 +334,6 @@ __global__ void __launch_bounds__(WV_THREADS, 1)
             for (int e = 0; e < 4; ++e) {
                 const int r = (e & 2) ? rb : ra;
                 const int col = ni * 8 + 2 * t + (e & 1);
-                Yst[col * WV_YP + r] = y[ni][e];
                 Yq[(int64_t)col * a.ldy + r] = y[ni][e];
             }
         // the barrier orders every thread's stores before thread 0's
@@ -294,6 +343,17 @@ __global__ void __launch_bounds__(WV_THREADS, 1)
             __threadfence();
             red_release_add(a.flags + q, 1);
         }
+    };
+    auto own_stage = [&](const double (&y)[NT][4], double *Yst) {
+        named_bar_sync(1, 256);      // the buffer's last readers are done
+#pragma unroll
+        for (int ni = 0; ni < NT; ++ni)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int r = (e & 2) ? rb : ra;
+                const int col = ni * 8 + 2 * t + (e & 1);
+                Yst[col * WV_YP + r] = -y[ni][e];
+            }
     };
     // Y_q = op(W_qq) * acc (W streamed through the ring); result to Yst and global
     auto diag = [&](double (&ac)[NT][4], double *Yst, int q) {
@@ -339,7 +399,7 @@ __global__ void __launch_bounds__(WV_THREADS, 1)
             for (int e = 0; e < 4; ++e) {
                 const int r = (e & 2) ? rb : ra;
                 const int col = ni * 8 + 2 * t + (e & 1);
-                Yst[col * WV_YP + r] = res[ni][e];
+                Yst[col * WV_YP + r] = -res[ni][e];      // the stage holds -Y for the updates
                 Yq[(int64_t)col * a.ldy + r] = res[ni][e];
             }
         // the barrier orders every thread's stores before thread 0's
@@ -348,6 +408,7 @@ __global__ void __launch_bounds__(WV_THREADS, 1)
         if (tid == 0) {
             __threadfence();
             red_release_add(a.flags + q, 1);
+            if (a.trace) a.trace[(int64_t)G * WV_TR_SLOTS + q] = globaltimer_ns();
         }
     };
 
@@ -358,11 +419,35 @@ __global__ void __launch_bounds__(WV_THREADS, 1)
         for (int i = 0; i < WV_RMAX; ++i)
             if (c + i * G == first) diag(acc[i], Ybuf, first);
     }
+    // the owner of the second block forms its Z before position 0
+    if (P > 1 && wv_block<TRANS>(1, P) % G == c) {
+        const int b1 = wv_block<TRANS>(1, P);
+#pragma unroll
+        for (int i = 0; i < WV_RMAX; ++i) {
+            if (c + i * G != b1) continue;
+            double z[NT][4];
+            wmul(acc[i], Ybuf + NC * WV_YP, z);
+#pragma unroll
+            for (int ni = 0; ni < NT; ++ni)
+#pragma unroll
+                for (int e = 0; e < 4; ++e) acc[i][ni][e] = z[ni][e];
+        }
+    }
+    unsigned long long *tr = a.trace ? a.trace + (int64_t)c * WV_TR_SLOTS : nullptr;
+    unsigned long long tnow = (tr && tid == 0) ? globaltimer_ns() : 0;
+    auto tmark = [&](int slot) {
+        if (tr && tid == 0) {
+            const unsigned long long t1 = globaltimer_ns();
+            tr[slot] += t1 - tnow;
+            tnow = t1;
+        }
+    };
     for (int qi = 0; qi < P && ok; ++qi) {
         const int q = wv_block<TRANS>(qi, P);
         const int nq = (qi + 1 < P) ? wv_block<TRANS>(qi + 1, P) : -1;
+        const int nnq = (qi + 2 < P) ? wv_block<TRANS>(qi + 2, P) : -1;
         double *Yq = Ybuf + (qi & 1) * (NC * WV_YP);          // holds Y_q
-        double *Ynext = Ybuf + ((qi + 1) & 1) * (NC * WV_YP); // receives Y_nq if owned
+        double *Ynext = Ybuf + ((qi + 1) & 1) * (NC * WV_YP); // Y of the previous position, then Y_nq if owned
         bool any = false;
 #pragma unroll
         for (int i = 0; i < WV_RMAX; ++i) {
@@ -370,19 +455,9 @@ __global__ void __launch_bounds__(WV_THREADS, 1)
             any |= (p < P) && (TRANS ? p < q : p > q);
         }
         if (!any) continue;
-        if (nq >= 0 && nq % G == c) {
-            // Z = op(W_nq) acc_nq while Y_q is not known yet (Ynext as staging)
-#pragma unroll
-            for (int i = 0; i < WV_RMAX; ++i) {
-                if (c + i * G != nq) continue;
-                double z[NT][4];
-                wmul(acc[i], Ynext, z);
-#pragma unroll
-                for (int ni = 0; ni < NT; ++ni)
-#pragma unroll
-                    for (int e = 0; e < 4; ++e) acc[i][ni][e] = z[ni][e];
-            }
-        }
+        tmark(5);
+        if (tr && tid == 0) tr[6] += 1;
+        const bool own_nq = nq >= 0 && nq % G == c, own_nnq = nnq >= 0 && nnq % G == c;
         if (q % G != c) {
             // Y_q from its owner
             int good = 1;
@@ -396,30 +471,65 @@ __global__ void __launch_bounds__(WV_THREADS, 1)
             }
             // one decision for all consumer warps (the status may change between their reads)
             if (named_bar_or(1, 256, !good || ld_volatile(a.status) != ST_OK)) break;
+            tmark(0);
             const double *Yg = a.Y + (int64_t)a.c0 * a.ldy + (int64_t)q * 128;
             for (int e = tid; e < NC * 128; e += 256) {
                 const int col = e / 128, r = e % 128;
-                Yq[col * WV_YP + r] = __ldcg(Yg + (int64_t)col * a.ldy + r);
+                Yq[col * WV_YP + r] = -__ldcg(Yg + (int64_t)col * a.ldy + r);
             }
             named_bar_sync(1, 256);
+            tmark(1);
         }
-        // critical path first: the next block, if owned
-        if (nq >= 0 && nq % G == c) {
+        if (own_nq) {
+            // critical path: Y_nq = Z - M_nq Y_q (Z formed one position
+            // earlier), published at once; then the products this CTA
+            // deferred at the previous position (on Y of that position,
+            // still in Ynext), then Y_nq into Ynext for this CTA's own use
 #pragma unroll
             for (int i = 0; i < WV_RMAX; ++i) {
                 if (c + i * G != nq) continue;
-                update(acc[i], Yq);            // acc_nq -= M_nq Y_q, acc_nq = Z on entry
+                update(acc[i], Yq);
                 if (named_bar_or(1, 256, !ok))
                     ok = false;
                 else
-                    publish(acc[i], Ynext, nq);
+                    publish(acc[i], nq);
             }
-        }
+            if (tr && tid == 0) a.trace[(int64_t)G * WV_TR_SLOTS + nq] = globaltimer_ns();
+            tmark(2);
+            if (qi >= 1) {
 #pragma unroll
-        for (int i = 0; i < WV_RMAX; ++i) {
-            const int p = c + i * G;
-            if (p >= P || p == nq || !(TRANS ? p < q : p > q)) continue;
-            update(acc[i], Yq);
+                for (int i = 0; i < WV_RMAX; ++i) {
+                    const int p = c + i * G;
+                    if (p < P && wv_pos<TRANS>(p, P) > qi + 1) update(acc[i], Ynext);
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < WV_RMAX; ++i)
+                if (c + i * G == nq) own_stage(acc[i], Ynext);
+            tmark(3);
+        }
+        if (own_nnq) {
+            // the block after next: its product with Y_q, then its Z before
+            // Y_nq is known; the other blocks' products wait one position
+#pragma unroll
+            for (int i = 0; i < WV_RMAX; ++i) {
+                if (c + i * G != nnq) continue;
+                update(acc[i], Yq);
+                double z[NT][4];
+                wmul(acc[i], Ynext, z);
+#pragma unroll
+                for (int ni = 0; ni < NT; ++ni)
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) acc[i][ni][e] = z[ni][e];
+            }
+            tmark(4);
+        } else {
+#pragma unroll
+            for (int i = 0; i < WV_RMAX; ++i) {
+                const int p = c + i * G;
+                if (p >= P || p == nq || !(TRANS ? p < q : p > q)) continue;
+                update(acc[i], Yq);
+            }
         }
         // Yq is overwritten two positions later; every warp leaves the loop together
         if (named_bar_or(1, 256, !ok)) ok = false;
@@ -492,8 +602,10 @@ int trsm_wave(Context *ctx, const double *dA, const double *W, const Geom &g, do
               int transposed, double alpha)
 {
     const int nblk = g.mt * (g.nbi / 128);
+    // at least two CTAs: consecutive blocks then have different owners,
+    // which the schedule's deferral relies on
     const int grid = ctx->sms * (ctx->wave_occ > 0 ? 1 : 0);
-    if (grid < 1 || nblk > WV_RMAX * grid) return 1;
+    if (grid < 2 || nblk > WV_RMAX * grid) return 1;
     const int nchunks = (nrhs + 31) / 32;
     const size_t per = (size_t)nblk + 4;
     int *ctr = (int *)ctx->buffer(BUF_SOLVE_CTR, per * nchunks * sizeof(int));
@@ -537,6 +649,13 @@ int trsm_wave(Context *ctx, const double *dA, const double *W, const Geom &g, do
         a.status = ctr + per * ch;
         a.flags = ctr + per * ch + 4;
         a.limit_ns = ctx->dep_limit_ns;
+        a.trace = nullptr;
+        if (ctx->wave_trace_path[0]) {
+            const size_t tb = ((size_t)grid * WV_TR_SLOTS + nblk) * sizeof(unsigned long long);
+            a.trace = (unsigned long long *)ctx->buffer(BUF_WTRACE, tb);
+            if (!a.trace) return DPLASMA_ERR_OUT_OF_RESOURCES;
+            CK(cudaMemsetAsync(a.trace, 0, tb, ctx->stream));
+        }
         const int nc = (nrhs - a.c0) < 32 ? (nrhs - a.c0) : 32;   // nrhs is a multiple of 8
         int rc;
         if (transposed)
@@ -550,6 +669,31 @@ int trsm_wave(Context *ctx, const double *dA, const double *W, const Geom &g, do
                  : nc <= 24 ? launch_wave<24, false>(ctx, a, grid, lmap, wmap, mmap)
                             : launch_wave<32, false>(ctx, a, grid, lmap, wmap, mmap);
         if (rc) return rc;
+        if (a.trace) {
+            // one line per sweep: CTA-summed ns per part, and the mean step of
+            // the wavefront (ns between consecutive publishes) per eighth of the blocks
+            std::vector<unsigned long long> h((size_t)grid * WV_TR_SLOTS + nblk);
+            CK(cudaMemcpyAsync(h.data(), a.trace, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                               ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+            unsigned long long sum[WV_TR_SLOTS] = {0};
+            for (int b = 0; b < grid; ++b)
+                for (int k = 0; k < WV_TR_SLOTS; ++k) sum[k] += h[(size_t)b * WV_TR_SLOTS + k];
+            if (FILE *f = fopen(ctx->wave_trace_path, "a")) {
+                fprintf(f, "sweep trans %d nblk %d nc %d cta_ns wait %llu stage %llu crit %llu deferred %llu znext %llu "
+                           "rest %llu positions %llu steps_ns",
+                        transposed, nblk, nc, sum[0], sum[1], sum[2], sum[3], sum[4], sum[5], sum[6]);
+                const unsigned long long *pt = h.data() + (size_t)grid * WV_TR_SLOTS;
+                for (int e = 0; e < 8; ++e) {
+                    const int q0 = e * nblk / 8, q1 = (e + 1) * nblk / 8;
+                    const int b0 = transposed ? nblk - 1 - q0 : q0, b1 = transposed ? nblk - q1 : q1 - 1;
+                    const long long d = (long long)pt[b1] - (long long)pt[b0];
+                    fprintf(f, " %lld", q1 - 1 > q0 ? d / (q1 - 1 - q0) : 0);
+                }
+                fprintf(f, "\n");
+                fclose(f);
+            }
+        }
     }
     int st = 0;
     for (int ch = 0; ch < nchunks; ++ch) {
