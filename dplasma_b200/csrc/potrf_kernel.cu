@@ -554,56 +554,118 @@ __device__ void potrf_task(const PotrfArgs &a, SmemCtl *ctl, double *ring, int k
         }
     };
 
-    for (int p0 = 0; p0 < nbi; p0 += 32) {
-        // (a) 32x32 diagonal block: unblocked Cholesky, lane i owns row i
-        if (warp == 0) {
-            unsigned long long ts = (a.ptrace && lane == 0) ? globaltimer_ns() : 0;
-            auto sub = [&](int i) {
-                if (a.ptrace && lane == 0) {
-                    const unsigned long long now = globaltimer_ns();
-                    a.ptrace[PTRACE_W * k + 4 + i] += now - ts;
-                    ts = now;
-                }
-            };
-            double d[32];
-#pragma unroll
-            for (int c = 0; c < 32; ++c) d[c] = (c <= lane) ? __ldcg(T + (int64_t)(p0 + c) * nbi + p0 + lane) : 0.0;
-            // phase trace only: a use of the loaded values, so they have arrived at the timestamp
-            if (a.ptrace) { double z = 0; for (int c = 0; c < 32; ++c) z += d[c]; if (z == 12345.0) colb[0] = z; }
-            sub(0);
-            double rdiag = 0.0;      // lane j: 1 / L(j,j)
-            const int failcol = chol32_blk<double>(d, lane, rdiag, Lb);
-            __syncwarp();
-            sub(1);
-            if (failcol >= 0) {
-                if (lane == 0) {
-                    ctl->fail = 1;
-                    const int col = p0 + failcol;   // tile-local column; padding follows the valid part
-                    if (col < a.nb_user && k * a.nb_user + col < a.n_user) atomicCAS(a.info, 0, k * a.nb_user + col + 1);
-                    atomicExch(a.abort_flag, 1);
-                }
-            } else {
-#pragma unroll 8
-                for (int c = 0; c < 32; ++c)
-                    if (c <= lane) T[(int64_t)(p0 + c) * nbi + p0 + lane] = Lb[(c >> 2) * 128 + lane * 4 + (c & 3)];
-                sub(2);
-                // inverse of the 32x32 lower block (Dv row-major: Dv[i*33 + c] =
-                // Dinv(i, c)) and its place in the 128-block inverse W
-                const int b = p0 / BLK, q0 = p0 % BLK;
-                double *Wb = Wk + (int64_t)b * BLK * BLK;
-                inv32_blk<double>(Lb, lane, rdiag, [&](int i, int c, double x) {
-                    Dv[i * 33 + c] = x;
-                    Wb[(int64_t)(q0 + c) * BLK + q0 + i] = x;
-                });
-                // phase trace only: the inverse is complete at the timestamp
-                if (a.ptrace) { __syncwarp(); if (Dv[lane * 33] == 12345.0) colb[1] = 0; }
-                sub(3);
+    // (a) 32x32 diagonal block at column p0 by warp 0: unblocked Cholesky,
+    // lane i owns row i, then its inverse (Dv) and its place in W
+    auto diag_block = [&](int p0) {
+        unsigned long long ts = (a.ptrace && lane == 0) ? globaltimer_ns() : 0;
+        auto sub = [&](int i) {
+            if (a.ptrace && lane == 0) {
+                const unsigned long long now = globaltimer_ns();
+                a.ptrace[PTRACE_W * k + 4 + i] += now - ts;
+                ts = now;
             }
+        };
+        double d[32];
+#pragma unroll
+        for (int c = 0; c < 32; ++c) d[c] = (c <= lane) ? __ldcg(T + (int64_t)(p0 + c) * nbi + p0 + lane) : 0.0;
+        // phase trace only: a use of the loaded values, so they have arrived at the timestamp
+        if (a.ptrace) { double z = 0; for (int c = 0; c < 32; ++c) z += d[c]; if (z == 12345.0) colb[0] = z; }
+        sub(0);
+        double rdiag = 0.0;      // lane j: 1 / L(j,j)
+        const int failcol = chol32_blk<double>(d, lane, rdiag, Lb);
+        __syncwarp();
+        sub(1);
+        if (failcol >= 0) {
+            if (lane == 0) {
+                ctl->fail = 1;
+                const int col = p0 + failcol;   // tile-local column; padding follows the valid part
+                if (col < a.nb_user && k * a.nb_user + col < a.n_user) atomicCAS(a.info, 0, k * a.nb_user + col + 1);
+                atomicExch(a.abort_flag, 1);
+            }
+        } else {
+#pragma unroll 8
+            for (int c = 0; c < 32; ++c)
+                if (c <= lane) T[(int64_t)(p0 + c) * nbi + p0 + lane] = Lb[(c >> 2) * 128 + lane * 4 + (c & 3)];
+            sub(2);
+            // inverse of the 32x32 lower block (Dv row-major: Dv[i*33 + c] =
+            // Dinv(i, c)) and its place in the 128-block inverse W
+            const int b = p0 / BLK, q0 = p0 % BLK;
+            double *Wb = Wk + (int64_t)b * BLK * BLK;
+            inv32_blk<double>(Lb, lane, rdiag, [&](int i, int c, double x) {
+                Dv[i * 33 + c] = x;
+                Wb[(int64_t)(q0 + c) * BLK + q0 + i] = x;
+            });
+            // phase trace only: the inverse is complete at the timestamp
+            if (a.ptrace) { __syncwarp(); if (Dv[lane * 33] == 12345.0) colb[1] = 0; }
+            sub(3);
         }
-        named_bar_sync(1, NCONS);
-        phase(0);
-        if (ctl->fail) return;
+    };
+    // (c) one 32x32 block (bi, bj) of the trailing update of step p0:
+    // T22 -= X X^T (DMMA from the panel copy Xs)
+    auto update_item = [&](int it, int p0) {
+        int bi = (int)((sqrtf(8.0f * it + 1.0f) - 1.0f) * 0.5f);
+        while ((bi + 1) * (bi + 2) / 2 <= it) ++bi;
+        while (bi * (bi + 1) / 2 > it) --bi;
+        const int bj = it - bi * (bi + 1) / 2;
+        double acc[2][4][4];
+#pragma unroll
+        for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) acc[mi][ni][q] = 0.0;
+#pragma unroll
+        for (int kk = 0; kk < 32; kk += 4) {
+            const double *xr = Xs + (kk + t) * XP;
+            double af[2][2], bf[4];
+#pragma unroll
+            for (int mi = 0; mi < 2; ++mi) {
+                af[mi][0] = xr[bi * 32 + mi * 16 + g];
+                af[mi][1] = xr[bi * 32 + mi * 16 + g + 8];
+            }
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni) bf[ni] = xr[bj * 32 + ni * 8 + g];
+#pragma unroll
+            for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni) dmma_16x8x4(acc[mi][ni], af[mi][0], af[mi][1], bf[ni]);
+        }
+        // all loads first, then the stores: interleaved, every load would
+        // wait for the previous store (the compiler cannot tell the
+        // addresses apart) and the update would take one L2 round trip
+        // per element
+        double old[2][4][4];
+#pragma unroll
+        for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int r = p0 + 32 + bi * 32 + mi * 16 + g + ((q & 2) ? 8 : 0);
+                    const int c = p0 + 32 + bj * 32 + ni * 8 + 2 * t + (q & 1);
+                    old[mi][ni][q] = (r >= c) ? __ldcg(T + (int64_t)c * nbi + r) : 0.0;
+                }
+#pragma unroll
+        for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int r = p0 + 32 + bi * 32 + mi * 16 + g + ((q & 2) ? 8 : 0);
+                    const int c = p0 + 32 + bj * 32 + ni * 8 + 2 * t + (q & 1);
+                    if (r >= c) T[(int64_t)c * nbi + r] = old[mi][ni][q] - acc[mi][ni][q];
+                }
+    };
 
+    // Look-ahead: after the panel of step p0, warp 0 updates the next
+    // diagonal block (item 0) and factors it while warps 1-7 update the rest
+    // of the trailing part, so the 32x32 factorization and inverse (the
+    // serial part of the task) overlap the update instead of following it.
+    if (warp == 0) diag_block(0);
+    named_bar_sync(1, NCONS);
+    phase(0);
+    if (ctl->fail) return;
+    for (int p0 = 0; p0 < nbi; p0 += 32) {
         // (b) panel below the block: X = P * Dinv^T (P = T[p0+32:, p0:p0+32])
         // on the FP64 tensor cores, one 32-row block of X per warp and turn
         const int R = nbi - p0 - 32;
@@ -648,65 +710,20 @@ __device__ void potrf_task(const PotrfArgs &a, SmemCtl *ctl, double *ring, int k
         named_bar_sync(1, NCONS);
         phase(1);
 
-        // (c) trailing update of the lower part: T22 -= X X^T (DMMA, 32x32 blocks)
-        const int nb32 = R / 32;
-        const int nitems = nb32 * (nb32 + 1) / 2;
-        for (int it = warp; it < nitems; it += NCONS / 32) {
-            int bi = (int)((sqrtf(8.0f * it + 1.0f) - 1.0f) * 0.5f);
-            while ((bi + 1) * (bi + 2) / 2 <= it) ++bi;
-            while (bi * (bi + 1) / 2 > it) --bi;
-            const int bj = it - bi * (bi + 1) / 2;
-            double acc[2][4][4];
-#pragma unroll
-            for (int mi = 0; mi < 2; ++mi)
-#pragma unroll
-                for (int ni = 0; ni < 4; ++ni)
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) acc[mi][ni][q] = 0.0;
-#pragma unroll
-            for (int kk = 0; kk < 32; kk += 4) {
-                const double *xr = Xs + (kk + t) * XP;
-                double af[2][2], bf[4];
-#pragma unroll
-                for (int mi = 0; mi < 2; ++mi) {
-                    af[mi][0] = xr[bi * 32 + mi * 16 + g];
-                    af[mi][1] = xr[bi * 32 + mi * 16 + g + 8];
-                }
-#pragma unroll
-                for (int ni = 0; ni < 4; ++ni) bf[ni] = xr[bj * 32 + ni * 8 + g];
-#pragma unroll
-                for (int mi = 0; mi < 2; ++mi)
-#pragma unroll
-                    for (int ni = 0; ni < 4; ++ni) dmma_16x8x4(acc[mi][ni], af[mi][0], af[mi][1], bf[ni]);
+        if (p0 + 32 < nbi) {
+            const int nb32 = R / 32;
+            const int nitems = nb32 * (nb32 + 1) / 2;
+            if (warp == 0) {
+                update_item(0, p0);
+                __syncwarp();          // the block's new values, written by every lane, before the reload
+                diag_block(p0 + 32);
+            } else {
+                for (int it = warp; it < nitems; it += NCONS / 32 - 1) update_item(it, p0);
             }
-            // all loads first, then the stores: interleaved, every load would
-            // wait for the previous store (the compiler cannot tell the
-            // addresses apart) and the update would take one L2 round trip
-            // per element
-            double old[2][4][4];
-#pragma unroll
-            for (int mi = 0; mi < 2; ++mi)
-#pragma unroll
-                for (int ni = 0; ni < 4; ++ni)
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const int r = p0 + 32 + bi * 32 + mi * 16 + g + ((q & 2) ? 8 : 0);
-                        const int c = p0 + 32 + bj * 32 + ni * 8 + 2 * t + (q & 1);
-                        old[mi][ni][q] = (r >= c) ? __ldcg(T + (int64_t)c * nbi + r) : 0.0;
-                    }
-#pragma unroll
-            for (int mi = 0; mi < 2; ++mi)
-#pragma unroll
-                for (int ni = 0; ni < 4; ++ni)
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const int r = p0 + 32 + bi * 32 + mi * 16 + g + ((q & 2) ? 8 : 0);
-                        const int c = p0 + 32 + bj * 32 + ni * 8 + 2 * t + (q & 1);
-                        if (r >= c) T[(int64_t)c * nbi + r] = old[mi][ni][q] - acc[mi][ni][q];
-                    }
+            named_bar_sync(1, NCONS);
+            phase(2);
+            if (ctl->fail) return;
         }
-        named_bar_sync(1, NCONS);
-        phase(2);
     }
 
     // Inverses of the 128x128 diagonal blocks from the 32x32 ones.
