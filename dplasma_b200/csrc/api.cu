@@ -148,12 +148,16 @@ extern "C" parsec_context_t *dplasma_b200_init(int device)
     // blocked order of the mixed update tasks: 8 tile columns x 32 tile rows
     // keep a block's 16-bit panel operands in L2 (factorization 325 -> 308 ms
     // at N=65536)
-    ctx->mx_block_w = getenv_int("DPLASMA_B200_MX_BLOCK_W", 8);
-    ctx->mx_block_h = getenv_int("DPLASMA_B200_MX_BLOCK_H", 32);
+    // mixed ticket order: blocks of 16 tile rows x 16 tile columns per chunk
+    // share, and the next step's POTRF 6 x grid tickets into the current share
+    // (N = 65536: 302 -> 285 ms against 8 x 32 and 3 x grid)
+    ctx->mx_block_w = getenv_int("DPLASMA_B200_MX_BLOCK_W", 16);
+    ctx->mx_block_h = getenv_int("DPLASMA_B200_MX_BLOCK_H", 16);
     ctx->stream_cb = getenv_int("DPLASMA_B200_STREAM_CB", 16);
     ctx->no_stream = getenv_int("DPLASMA_B200_NO_STREAM", 0) != 0;
     ctx->stream_trace = getenv_int("DPLASMA_B200_STREAM_TRACE", 0) != 0;
     ctx->potrf_delay = getenv_int("DPLASMA_B200_DELAY", 3 * ctx->potrf_grid);
+    ctx->mx_delay = getenv_int("DPLASMA_B200_MX_DELAY", 6 * ctx->potrf_grid);
     ctx->wave_occ = getenv_int("DPLASMA_B200_NO_WAVE", 0) ? 0 : wave_max_blocks_per_sm();
     int occs = sweep_max_blocks_per_sm();
     ctx->solve_grid = ctx->sms * (occs < 1 ? 1 : occs);

@@ -64,7 +64,8 @@ struct Context {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr, ev3 = nullptr;
     int potrf_grid = 0;
     int potrf_grid_mixed = 0;
-    int potrf_delay = 0;
+    int potrf_delay = 0;                     // FP64 ticket order: POTRF(k+1) this many tickets into step k's updates
+    int mx_delay = 0;                        // the same for the mixed-precision ticket orders
     int solve_grid = 0;
     int wave_occ = 0;                        // CTAs per SM of the wavefront solve (0: not usable)
     uint64_t dep_limit_ns = 4000000000ull;   // 4 s

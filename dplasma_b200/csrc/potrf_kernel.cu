@@ -1519,8 +1519,9 @@ int potrf_run(Context *ctx, double *dA, int mt, int nbi, int nb_user, int n_user
     // 7, 16: 8); single 16-bit operands are limited by their own rounding
     // and take 16 (same refinement steps as 8, 15% faster factorization)
     const int chunk = !mixed ? 0 : (ctx->mx_chunk > 0 ? ctx->mx_chunk : (p16_fmt == 2 ? 8 : 16));
-    if (ctx->task_mt != mt || ctx->task_nbs != nbs || ctx->task_delay != ctx->potrf_delay || ctx->task_mixed != chunk) {
-        std::vector<uint64_t> tasks = mixed ? build_potrf_tasks_mixed(mt, nbs, ctx->potrf_delay, chunk, ctx->mx_block_w,
+    const int delay = mixed ? ctx->mx_delay : ctx->potrf_delay;
+    if (ctx->task_mt != mt || ctx->task_nbs != nbs || ctx->task_delay != delay || ctx->task_mixed != chunk) {
+        std::vector<uint64_t> tasks = mixed ? build_potrf_tasks_mixed(mt, nbs, delay, chunk, ctx->mx_block_w,
                                                                       ctx->mx_block_h)
                                             : build_potrf_tasks(mt, nbs, ctx->potrf_delay);
         uint64_t *dt = (uint64_t *)ctx->buffer(BUF_TASKS, tasks.size() * sizeof(uint64_t));
@@ -1528,7 +1529,7 @@ int potrf_run(Context *ctx, double *dA, int mt, int nbi, int nb_user, int n_user
         CK(cudaMemcpyAsync(dt, tasks.data(), tasks.size() * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
         ctx->task_mt = mt;
         ctx->task_nbs = nbs;
-        ctx->task_delay = ctx->potrf_delay;
+        ctx->task_delay = delay;
         ctx->task_mixed = chunk;
         ctx->ntasks = (int)tasks.size();
     }
@@ -1746,8 +1747,8 @@ int potrf_run_streamed(Context *ctx, const double *hA, double *A0, double *L, in
     const int chunk = ctx->mx_chunk > 0 ? ctx->mx_chunk : (p16_fmt == 2 ? 8 : 16);
     int cb = ctx->stream_cb > 0 ? ctx->stream_cb : 16;
     cb = ((std::max(cb, chunk) + chunk - 1) / chunk) * chunk;
-    if (ctx->ph_mt != mt || ctx->ph_chunk != chunk || ctx->ph_cb != cb || ctx->ph_delay != ctx->potrf_delay) {
-        const auto ph = build_potrf_tasks_mixed_phased(mt, nbs, ctx->potrf_delay, chunk, cb, ctx->mx_block_w,
+    if (ctx->ph_mt != mt || ctx->ph_chunk != chunk || ctx->ph_cb != cb || ctx->ph_delay != ctx->mx_delay) {
+        const auto ph = build_potrf_tasks_mixed_phased(mt, nbs, ctx->mx_delay, chunk, cb, ctx->mx_block_w,
                                                        ctx->mx_block_h);
         std::vector<uint64_t> all;
         ctx->ph_off.assign(1, 0);
@@ -1762,7 +1763,7 @@ int potrf_run_streamed(Context *ctx, const double *hA, double *A0, double *L, in
         ctx->ph_mt = mt;
         ctx->ph_chunk = chunk;
         ctx->ph_cb = cb;
-        ctx->ph_delay = ctx->potrf_delay;
+        ctx->ph_delay = ctx->mx_delay;
     }
     const int nph = (int)ctx->ph_off.size() - 1;
     double *W = (double *)ctx->buffer(BUF_W, (size_t)mt * nbs * BLK * BLK * sizeof(double));
@@ -2055,7 +2056,7 @@ extern "C" int dplasma_b200_debug_task_list_blocked(int mixed_chunk, int mt, int
 extern "C" int dplasma_b200_debug_task_list_phased(int mixed_chunk, int mt, int nbs, int delay, int cb,
                                                    unsigned long long *out, int cap, int *ends, int ends_cap)
 {
-    const auto ph = db2::build_potrf_tasks_mixed_phased(mt, nbs, delay, mixed_chunk, cb, 8, 32);
+    const auto ph = db2::build_potrf_tasks_mixed_phased(mt, nbs, delay, mixed_chunk, cb, 16, 16);
     size_t n = 0;
     for (size_t p = 0; p < ph.size(); ++p) {
         for (uint64_t t : ph[p]) {

@@ -96,12 +96,13 @@ def tasks_blocked(chunk, mt, nbs, delay, bw, bh):
              (int(t) >> 52) & 0xF, (int(t) >> 56) & 0xF) for t in out]
 
 
-@pytest.mark.parametrize("mt,S,bw,bh", [(33, 4, 4, 8), (65, 8, 4, 32), (65, 8, 1, 1), (40, 3, 7, 5)])
-def test_mixed_blocked_ticket_order(mt, S, bw, bh):
+@pytest.mark.parametrize("mt,S,bw,bh,delay", [(33, 4, 4, 8, 444), (65, 8, 4, 32, 444), (65, 8, 1, 1, 444),
+                                              (40, 3, 7, 5, 444), (65, 8, 16, 16, 888)])
+def test_mixed_blocked_ticket_order(mt, S, bw, bh, delay):
     # the blocked order permutes each step's share: same tasks, same dependency guarantees
-    tl = tasks_blocked(S, mt, 2, 444, bw, bh)
+    tl = tasks_blocked(S, mt, 2, delay, bw, bh)
     replay(tl, mt, 2, S)
-    assert sorted(tl) == sorted(tasks(S, mt, 2, 444))
+    assert sorted(tl) == sorted(tasks(S, mt, 2, delay))
 
 
 def tasks_phased(chunk, mt, nbs, delay, cb):
