@@ -34,35 +34,39 @@ namespace db2 {
 //
 // Persistent: CTA b streams the lower tiles [b*T/G, (b+1)*T/G) in storage
 // order (one tile column after the other, a contiguous stretch of memory).
-// Each tile (m,n) is read once, in panels of 16 columns, and used twice:
-//   y_m += A(m,n) x_n     warps 4-7, 64 rows each, in registers for the tile,
-//                         added to out at the tile's end (L2 reductions);
-//   y_n += A(m,n)^T x_m   warps 0-3, partial sums over 64 rows each, combined
-//                         through shared memory per panel into per-thread
-//                         registers that live for the whole tile column:
-//                         thread i owns (column 16p + c(i), rhs j(i)) of every
-//                         panel p, added to out when the column ends.
-// A diagonal tile has its upper triangle zeroed and its diagonal halved in
-// shared memory, so the two uses add up to the symmetric product.  Warp 8
-// streams the panels by bulk copies, with the x slices on a tile's first
-// panel: x_m (two buffers, by tile parity) and, when the column changes, x_n
-// (once the consumers have released the previous column's).
+// Each tile (m,n) is read once, in panels of 8 columns, and used twice:
+//   y_m += A(m,n) x_n     warps 4-7, 64 rows each, every panel (K = 8), in
+//                         registers for the tile, added to out at the tile's
+//                         end (L2 reductions);
+//   y_n += A(m,n)^T x_m   warps 0-3, warp w the panels p = w (mod 4), each a
+//                         whole K = 256 product y_n^T = x_m^T P (four partial
+//                         sums), kept in registers for the tile column and
+//                         added to out when the column ends.
+// No warp waits for another: a panel stage is released by its five users
+// (the y_m warps and the panel's y_n warp).  A diagonal tile is read with
+// its upper triangle as zero and its diagonal halved, so the two uses add up
+// to the symmetric product.  Warp 8 streams the panels by bulk copies into a
+// 6-stage ring, the x slice of the tile row on its own barrier (two buffers,
+// by tile parity) and, when the column changes, the x slice of the column
+// with the column's first panel (once the y_m warps have released the
+// previous column's).
 // ---------------------------------------------------------------------------
 constexpr int SY_NBI = 256;
-constexpr int SY_PC = 16;                 // columns per panel
+constexpr int SY_PC = 8;                  // columns per panel
 constexpr int SY_NP = SY_NBI / SY_PC;     // panels per tile
-constexpr int SY_NST = 3;                 // panel stages
+constexpr int SY_NST = 6;                 // panel stages
 constexpr int SY_PP = SY_NBI + 4;         // pitch (doubles), == 4 mod 16: conflict-free fragments
 constexpr int SY_NC = 16;                 // right-hand-side columns per launch
 constexpr int SY_THREADS = 288;           // 8 consumer warps + the producer warp
 constexpr int SY_SLICE = SY_NC * SY_PP;   // one x slice, [rhs][row]
+constexpr int SY_YN_PANELS = SY_NP / 4;   // panels of one y_n warp per tile
 struct SyCtl {
     uint64_t full[SY_NST];
     uint64_t empty[SY_NST];
+    uint64_t xfull[2];
     uint64_t xn_free;
 };
-constexpr size_t SY_SMEM =
-    (size_t)(SY_NST * SY_PC * SY_PP + 3 * SY_SLICE + 2 * 4 * 256) * sizeof(double) + sizeof(SyCtl);
+constexpr size_t SY_SMEM = (size_t)(SY_NST * SY_PC * SY_PP + 3 * SY_SLICE) * sizeof(double) + sizeof(SyCtl);
 
 // tile column n and row m of the lower tile with storage index t
 __device__ __forceinline__ void sy_tile_of(int64_t t, int mt, int &m, int &n)
@@ -73,6 +77,12 @@ __device__ __forceinline__ void sy_tile_of(int64_t t, int mt, int &m, int &n)
     m = c + (int)(t - lower_tile_index(c, c, mt));
 }
 
+// element (row, col) of a diagonal tile as the symmetric product reads it
+__device__ __forceinline__ double sy_diag(double v, int row, int col)
+{
+    return row > col ? v : (row == col ? 0.5 * v : 0.0);
+}
+
 __global__ void __launch_bounds__(SY_THREADS, 1)
     symm_stream_kernel(const double *__restrict__ A, int mt, const double *__restrict__ in, int ldin,
                        double *__restrict__ out, int ldout, int nc, double alpha, int *status, uint64_t limit_ns)
@@ -81,8 +91,7 @@ __global__ void __launch_bounds__(SY_THREADS, 1)
     double *P = sy;                                 // [stage][c][PP]
     double *Xm = P + SY_NST * SY_PC * SY_PP;        // [2][rhs][PP]: x rows of tile row m
     double *Xn = Xm + 2 * SY_SLICE;                 // [rhs][PP]: x rows of tile column n
-    double *red = Xn + SY_SLICE;                    // [2][4 warps][256]
-    SyCtl *ctl = reinterpret_cast<SyCtl *>(red + 2 * 4 * 256);
+    SyCtl *ctl = reinterpret_cast<SyCtl *>(Xn + SY_SLICE);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int g = lane >> 2, t4 = lane & 3;
     const int64_t T = (int64_t)mt * (mt + 1) / 2;
@@ -91,9 +100,11 @@ __global__ void __launch_bounds__(SY_THREADS, 1)
     if (tid == 0) {
         for (int s = 0; s < SY_NST; ++s) {
             mbar_init(&ctl->full[s], 1);
-            mbar_init(&ctl->empty[s], 8);
+            mbar_init(&ctl->empty[s], 5);          // the four y_m warps and the panel's y_n warp
         }
-        mbar_init(&ctl->xn_free, 1);
+        mbar_init(&ctl->xfull[0], 1);
+        mbar_init(&ctl->xfull[1], 1);
+        mbar_init(&ctl->xn_free, 4);               // the y_m warps
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     // right-hand sides beyond nc stay zero in every x slice
@@ -118,6 +129,13 @@ __global__ void __launch_bounds__(SY_THREADS, 1)
                 ok = false;
                 break;
             }
+            // the x slice of the tile row (buffer xb last read two tiles ago:
+            // the ring keeps the producer within a few panels of every warp)
+            if (lane == 0) mbar_arrive_expect_tx(&ctl->xfull[xb], (uint32_t)nc * SY_NBI * sizeof(double));
+            __syncwarp();
+            if (lane < nc)
+                bulk_g2s(Xm + xb * SY_SLICE + lane * SY_PP, in + (int64_t)lane * ldin + (int64_t)m * SY_NBI,
+                         SY_NBI * sizeof(double), &ctl->xfull[xb]);
             for (int p = 0; p < SY_NP; ++p) {
                 const uint32_t s = it % SY_NST, r = it / SY_NST;
                 if (r > 0 && !warp_mbar_wait(&ctl->empty[s], (r - 1) & 1, limit_ns)) {
@@ -126,19 +144,16 @@ __global__ void __launch_bounds__(SY_THREADS, 1)
                     break;
                 }
                 uint32_t bytes = SY_PC * SY_NBI * sizeof(double);
-                if (p == 0) bytes += (uint32_t)nc * SY_NBI * sizeof(double) * (new_col ? 2 : 1);
+                if (p == 0 && new_col) bytes += (uint32_t)nc * SY_NBI * sizeof(double);
                 if (lane == 0) mbar_arrive_expect_tx(&ctl->full[s], bytes);
                 __syncwarp();
                 if (lane < SY_PC) {
                     bulk_g2s(P + (s * SY_PC + lane) * SY_PP, Tt + (int64_t)(p * SY_PC + lane) * SY_NBI,
                              SY_NBI * sizeof(double), &ctl->full[s]);
-                } else if (p == 0 && lane - SY_PC < nc) {
+                } else if (p == 0 && new_col && lane - SY_PC < nc) {
                     const int j = lane - SY_PC;
-                    bulk_g2s(Xm + xb * SY_SLICE + j * SY_PP, in + (int64_t)j * ldin + (int64_t)m * SY_NBI,
-                             SY_NBI * sizeof(double), &ctl->full[s]);
-                    if (new_col)
-                        bulk_g2s(Xn + j * SY_PP, in + (int64_t)j * ldin + (int64_t)n * SY_NBI, SY_NBI * sizeof(double),
-                                 &ctl->full[s]);
+                    bulk_g2s(Xn + j * SY_PP, in + (int64_t)j * ldin + (int64_t)n * SY_NBI, SY_NBI * sizeof(double),
+                             &ctl->full[s]);
                 }
                 ++it;
             }
@@ -154,114 +169,58 @@ __global__ void __launch_bounds__(SY_THREADS, 1)
         // copies already issued land before the CTA may exit
         const uint32_t first = it > SY_NST ? it - SY_NST : 0;
         for (uint32_t k = first; k < it; ++k) warp_mbar_wait(&ctl->full[k % SY_NST], (k / SY_NST) & 1, limit_ns);
+        const int64_t ntl = t1 - t0;
+        for (int64_t i = ntl > 2 ? ntl - 2 : 0; i < ntl; ++i)
+            warp_mbar_wait(&ctl->xfull[i & 1], (uint32_t)((i >> 1) & 1), limit_ns);
         return;
     }
 
-    // consumers
     int m, n;
     sy_tile_of(t0, mt, m, n);
-    double yacc[SY_NP];                   // y_n outputs of this thread, one per panel
-#pragma unroll
-    for (int p = 0; p < SY_NP; ++p) yacc[p] = 0.0;
-    const int rl = tid & 31, rni = (tid >> 5) & 1, rq = (tid >> 6) & 3;
-    const int rc = (rl >> 2) + ((rq & 2) ? 8 : 0), rj = rni * 8 + 2 * (rl & 3) + (rq & 1);
     uint32_t it = 0;
-    for (int64_t t = t0; t < t1; ++t) {
-        const double *xm = Xm + (int)((t - t0) & 1) * SY_SLICE;
-        double ym[4][2][4];
+    if (warp >= 4) {
+        // y_m warps: rows R0..R0+63 of every tile, K = the panel's 8 columns
+        const int R0 = (warp - 4) * 64;
+        for (int64_t t = t0; t < t1; ++t) {
+            double ym[4][2][4];
 #pragma unroll
-        for (int mi = 0; mi < 4; ++mi)
+            for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
-            for (int ni = 0; ni < 2; ++ni)
+                for (int ni = 0; ni < 2; ++ni)
 #pragma unroll
-                for (int q = 0; q < 4; ++q) ym[mi][ni][q] = 0.0;
-        bool ok = true;
-        // a rolled panel loop (an unrolled one outgrows the instruction
-        // cache); yacc rotates by one per panel, so the current panel's
-        // accumulator is always yacc[0] and the order is restored after
-        // SY_NP panels
+                    for (int q = 0; q < 4; ++q) ym[mi][ni][q] = 0.0;
+            const bool diag = (m == n);
 #pragma unroll 1
-        for (int p = 0; p < SY_NP; ++p) {
-            const uint32_t s = it % SY_NST;
-            const bool got = warp_mbar_wait(&ctl->full[s], (it / SY_NST) & 1, limit_ns);
-            double *Ps = P + s * SY_PC * SY_PP;
-            if (m == n) {
-                // every warp reads the whole panel: fix it up between two barriers
-                if (named_bar_or(1, 256, !got)) {
-                    ok = false;
-                    break;
+            for (int p = 0; p < SY_NP; ++p) {
+                const uint32_t s = it % SY_NST;
+                if (!warp_mbar_wait(&ctl->full[s], (it / SY_NST) & 1, limit_ns)) {
+                    if (lane == 0) atomicCAS(status, ST_OK, ST_MBAR_TIMEOUT);
+                    return;
                 }
-                for (int e = tid; e < SY_PC * SY_NBI; e += 256) {
-                    const int c = e / SY_NBI, r = e % SY_NBI;
-                    double &v = Ps[c * SY_PP + r];
-                    if (r < p * SY_PC + c) v = 0.0;
-                    else if (r == p * SY_PC + c) v *= 0.5;
-                }
-                fence_proxy_async();   // the stage is refilled by the async proxy
-                named_bar_sync(1, 256);
-            }
-            if (got) {
-                if (warp < 4) {
-                    // y_n(16 panel columns, rhs) partial over rows 64w..64w+63: P^T x_m
-                    const int R0 = warp * 64;
-                    double yn[2][2][4];
+                const double *Ps = P + s * SY_PC * SY_PP;
+                const int c0 = p * SY_PC;
 #pragma unroll
-                    for (int h = 0; h < 2; ++h)
+                for (int kk = 0; kk < SY_PC; kk += 4) {
+                    double bf[2];
 #pragma unroll
-                        for (int ni = 0; ni < 2; ++ni)
+                    for (int ni = 0; ni < 2; ++ni) bf[ni] = Xn[(ni * 8 + g) * SY_PP + c0 + kk + t4];
 #pragma unroll
-                            for (int q = 0; q < 4; ++q) yn[h][ni][q] = 0.0;
-#pragma unroll
-                    for (int kk = 0; kk < 64; kk += 4) {
-                        const int r = R0 + kk + t4;
-                        const double a0 = Ps[g * SY_PP + r], a1 = Ps[(g + 8) * SY_PP + r];
-#pragma unroll
-                        for (int ni = 0; ni < 2; ++ni)
-                            dmma_16x8x4(yn[(kk >> 2) & 1][ni], a0, a1, xm[(ni * 8 + g) * SY_PP + r]);
-                    }
-                    double *rb = red + (p & 1) * 1024 + warp * 256 + lane * 8;
-#pragma unroll
-                    for (int ni = 0; ni < 2; ++ni)
-#pragma unroll
-                        for (int q = 0; q < 4; ++q) rb[ni * 4 + q] = yn[0][ni][q] + yn[1][ni][q];
-                } else {
-                    // y_m(rows 64(w-4).., rhs) += P(rows, 16 columns) x_n(16 columns, rhs)
-                    const int R0 = (warp - 4) * 64, c0 = p * SY_PC;
-#pragma unroll
-                    for (int kk = 0; kk < SY_PC; kk += 4) {
-                        double bf[2];
-#pragma unroll
-                        for (int ni = 0; ni < 2; ++ni) bf[ni] = Xn[(ni * 8 + g) * SY_PP + c0 + kk + t4];
-#pragma unroll
-                        for (int mi = 0; mi < 4; ++mi) {
-                            const double a0 = Ps[(kk + t4) * SY_PP + R0 + mi * 16 + g];
-                            const double a1 = Ps[(kk + t4) * SY_PP + R0 + mi * 16 + g + 8];
-#pragma unroll
-                            for (int ni = 0; ni < 2; ++ni) dmma_16x8x4(ym[mi][ni], a0, a1, bf[ni]);
+                    for (int mi = 0; mi < 4; ++mi) {
+                        const int row = R0 + mi * 16 + g, col = c0 + kk + t4;
+                        double a0 = Ps[(kk + t4) * SY_PP + row];
+                        double a1 = Ps[(kk + t4) * SY_PP + row + 8];
+                        if (diag) {
+                            a0 = sy_diag(a0, row, col);
+                            a1 = sy_diag(a1, row + 8, col);
                         }
+#pragma unroll
+                        for (int ni = 0; ni < 2; ++ni) dmma_16x8x4(ym[mi][ni], a0, a1, bf[ni]);
                     }
                 }
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&ctl->empty[s]);
+                ++it;
             }
-            ++it;
-            if (named_bar_or(1, 256, !got)) {
-                ok = false;
-                break;
-            }
-            // the four partial sums of this panel's y_n
-            const double *rr = red + (p & 1) * 1024 + rl * 8 + rni * 4 + rq;
-            const double y0 = yacc[0] + ((rr[0] + rr[256]) + (rr[512] + rr[768]));
-#pragma unroll
-            for (int q = 0; q < SY_NP - 1; ++q) yacc[q] = yacc[q + 1];
-            yacc[SY_NP - 1] = y0;
-        }
-        if (!ok) {
-            if (tid == 0) atomicCAS(status, ST_OK, ST_MBAR_TIMEOUT);
-            return;
-        }
-        if (warp >= 4) {
-            const int R0 = (warp - 4) * 64;
 #pragma unroll
             for (int mi = 0; mi < 4; ++mi)
 #pragma unroll
@@ -272,16 +231,83 @@ __global__ void __launch_bounds__(SY_THREADS, 1)
                         const int j = ni * 8 + 2 * t4 + (q & 1);
                         if (j < nc) red_add_f64(out + (int64_t)j * ldout + (int64_t)m * SY_NBI + r, alpha * ym[mi][ni][q]);
                     }
+            // this warp is done with the column's x slice
+            if (m + 1 == mt && lane == 0) mbar_arrive(&ctl->xn_free);
+            if (++m == mt) {
+                ++n;
+                m = n;
+            }
         }
+        return;
+    }
+
+    // y_n warps: y_n^T (16 rhs x 8 panel columns) = x_m^T P over the tile's
+    // 256 rows for the panels p = warp (mod 4).  yacc[j] holds this warp's
+    // j-th panel of the column; the loop is rolled and yacc rotates by one
+    // per panel, so the current panel's sum is always yacc[0] (the order is
+    // restored after a tile).
+    double yacc[SY_YN_PANELS][4];
+#pragma unroll
+    for (int j = 0; j < SY_YN_PANELS; ++j)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) yacc[j][q] = 0.0;
+    for (int64_t t = t0; t < t1; ++t) {
+        const int xb = (int)((t - t0) & 1);
+        if (!warp_mbar_wait(&ctl->xfull[xb], (uint32_t)(((t - t0) >> 1) & 1), limit_ns)) {
+            if (lane == 0) atomicCAS(status, ST_OK, ST_MBAR_TIMEOUT);
+            return;
+        }
+        const double *xm = Xm + xb * SY_SLICE;
+        const bool diag = (m == n);
+        const uint32_t base = it;                       // ring position of the tile's panel 0
+#pragma unroll 1
+        for (int p = warp; p < SY_NP; p += 4) {
+            const uint32_t pi = base + p;
+            const uint32_t s = pi % SY_NST;
+            if (!warp_mbar_wait(&ctl->full[s], (pi / SY_NST) & 1, limit_ns)) {
+                if (lane == 0) atomicCAS(status, ST_OK, ST_MBAR_TIMEOUT);
+                return;
+            }
+            const double *Ps = P + s * SY_PC * SY_PP;
+            const int col = p * SY_PC + g;              // this lane's B column (the panel's column g)
+            double part[4][4];
+#pragma unroll
+            for (int h = 0; h < 4; ++h)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) part[h][q] = 0.0;
+#pragma unroll 16
+            for (int kk = 0; kk < SY_NBI; kk += 4) {
+                const int r = kk + t4;
+                const double a0 = xm[g * SY_PP + r], a1 = xm[(g + 8) * SY_PP + r];
+                double b = Ps[g * SY_PP + r];
+                if (diag) b = sy_diag(b, r, col);
+                dmma_16x8x4(part[(kk >> 2) & 3], a0, a1, b);
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&ctl->empty[s]);
+            double y0[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) y0[q] = yacc[0][q] + ((part[0][q] + part[1][q]) + (part[2][q] + part[3][q]));
+#pragma unroll
+            for (int j = 0; j < SY_YN_PANELS - 1; ++j)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) yacc[j][q] = yacc[j + 1][q];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) yacc[SY_YN_PANELS - 1][q] = y0[q];
+        }
+        it = base + SY_NP;
         const bool col_end = (m + 1 == mt);
         if (col_end || t + 1 == t1) {
+            // fragment (rhs g / g+8, panel columns 2 t4, 2 t4 + 1) of panel warp + 4 j
 #pragma unroll
-            for (int p = 0; p < SY_NP; ++p) {
-                if (rj < nc) red_add_f64(out + (int64_t)rj * ldout + (int64_t)n * SY_NBI + p * SY_PC + rc, alpha * yacc[p]);
-                yacc[p] = 0.0;
-            }
-            // every consumer warp passed the last panel's barrier: x_n is free
-            if (col_end && tid == 0) mbar_arrive(&ctl->xn_free);
+            for (int j = 0; j < SY_YN_PANELS; ++j)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int rhs = g + ((q & 2) ? 8 : 0);
+                    const int c = (warp + 4 * j) * SY_PC + 2 * t4 + (q & 1);
+                    if (rhs < nc) red_add_f64(out + (int64_t)rhs * ldout + (int64_t)n * SY_NBI + c, alpha * yacc[j][q]);
+                    yacc[j][q] = 0.0;
+                }
         }
         if (++m == mt) {
             ++n;
