@@ -54,7 +54,7 @@ namespace db2 {
 constexpr int SY_NBI = 256;
 constexpr int SY_PC = 8;                  // columns per panel
 constexpr int SY_NP = SY_NBI / SY_PC;     // panels per tile
-constexpr int SY_NST = 6;                 // panel stages
+constexpr int SY_NST = 7;                 // panel stages
 constexpr int SY_PP = SY_NBI + 4;         // pitch (doubles), == 4 mod 16: conflict-free fragments
 constexpr int SY_NC = 16;                 // right-hand-side columns per launch
 constexpr int SY_THREADS = 288;           // 8 consumer warps + the producer warp
