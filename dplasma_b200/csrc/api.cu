@@ -189,6 +189,7 @@ extern "C" void dplasma_b200_fini(parsec_context_t **pctx)
     cudaEventDestroy(ctx->ev3);
     cudaStreamSynchronize(ctx->copy_stream);
     cudaStreamDestroy(ctx->copy_stream);
+    if (ctx->host_one) cudaFreeHost(ctx->host_one);
     cudaStreamDestroy(ctx->stream);
     delete *pctx;
     *pctx = nullptr;

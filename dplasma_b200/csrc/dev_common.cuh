@@ -133,6 +133,14 @@ __device__ __forceinline__ int ld_volatile(const int *p)
 {
     return *reinterpret_cast<const volatile int *>(p);
 }
+// Acquire at system scope: for flags written by a copy engine (host to device
+// copies on another stream).
+__device__ __forceinline__ int ld_acquire_sys(const int *p)
+{
+    int v;
+    asm volatile("ld.acquire.sys.global.b32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
 
 // Bounded wait until *ctr >= target.  Gives up early when *abort_flag is set
 // (returns false) or after limit_ns (sets *status and returns false).
@@ -151,6 +159,24 @@ __device__ __forceinline__ bool wait_geq(const int *ctr, int target, const int *
         }
         __nanosleep(ns);
         if (ns < 256) ns <<= 1;
+    }
+}
+
+// Bounded wait until a copy-engine flag is set (same give-up rules as wait_geq).
+__device__ __forceinline__ bool wait_flag_sys(const int *flag, const int *abort_flag, int *status, uint64_t limit_ns)
+{
+    if (ld_acquire_sys(flag) != 0) return true;
+    const uint64_t t0 = globaltimer_ns();
+    unsigned ns = 64;
+    while (true) {
+        if (ld_acquire_sys(flag) != 0) return true;
+        if (ld_volatile(abort_flag)) return false;
+        if (globaltimer_ns() - t0 > limit_ns) {
+            atomicCAS(status, ST_OK, ST_DEP_TIMEOUT);
+            return false;
+        }
+        __nanosleep(ns);
+        if (ns < 1024) ns <<= 1;
     }
 }
 

@@ -43,6 +43,7 @@ enum BufferId : int {
     BUF_WX,           // second block row [Linv10 | W1] of the inverses of 256-wide diagonal tiles
     BUF_LINV16,       // inverses of the diagonal tiles in split FP16 (tensor-core TRSM strips)
     BUF_WTRACE,       // opt-in trace of the triangular sweeps
+    BUF_ARRIVED,      // streamed factorization: per-phase arrival flags
     BUF_TASKS_PH,     // phased ticket order of the streamed factorization
     BUF_WM,           // triangular sweeps: the critical path's products W_b L_{b,b-1}
     BUF_COUNT
@@ -61,6 +62,7 @@ struct Context {
     int sms = 0;
     cudaStream_t stream = nullptr;
     cudaStream_t copy_stream = nullptr;      // host -> device copies that overlap the factorization
+    int *host_one = nullptr;                 // pinned host word holding 1 (source of the arrival flags)
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev2 = nullptr, ev3 = nullptr;
     int potrf_grid = 0;
     int potrf_grid_mixed = 0;

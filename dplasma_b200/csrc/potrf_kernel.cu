@@ -62,6 +62,15 @@ __device__ bool wait_deps(const PotrfArgs &a, uint64_t t)
 {
     const int k = task_k(t), m = task_m(t), n = task_n(t);
     const int nbs = a.nbs;
+    if (MIXED && a.A0) {
+        // streamed matrix: a task that reads the untouched copy waits until
+        // its tile column has arrived (POTRF(0) and the strips of column 0,
+        // the first update chunk (k == 0) of tile (m, n))
+        const int ty = task_type(t);
+        const int col = (ty == T_GEMM) ? (k == 0 ? n : -1) : (k == 0 ? 0 : -1);
+        if (col >= 0 && !wait_flag_sys(a.arrived + col / a.stream_cb, a.abort_flag, a.status, a.dep_limit_ns))
+            return false;
+    }
     switch (task_type(t)) {
     case T_POTRF:
         return wait_geq(a.upd_done + (int64_t)k * a.mt + k, all_updates<MIXED>(a, k, k), a.abort_flag, a.status,
@@ -377,6 +386,8 @@ __device__ __forceinline__ bool consume_job(const PotrfArgs &a, SmemCtl *ctl, co
                 double *p = jb.C + (int64_t)c * jb.ldc + r;
                 if (jb.mode == J_STORE) {
                     *p = acc[mi][ni][q];
+                } else if (jb.mode == J_SUB_SRC) {
+                    *p = __ldcg(jb.src + (int64_t)c * jb.ldc + r) - acc[mi][ni][q];
                 } else if (jb.mode == J_SUB || r >= c) {
                     atomicAdd(p, -acc[mi][ni][q]);
                 }
@@ -543,6 +554,12 @@ __device__ void potrf_task(const PotrfArgs &a, SmemCtl *ctl, double *ring, int k
     double *Lb = Xs + 32 * XP;       // [8][32][4]: blocked copy of the 32x32 factor
 
     for (int e = tid; e < a.nbs * BLK * BLK; e += NCONS) Wk[e] = 0.0;
+    if (MIXED && a.A0 && k == 0) {
+        // streamed matrix: the first touch of tile (0, 0) copies it from the untouched copy
+        const double2 *S = reinterpret_cast<const double2 *>(a.A0 + (T - a.A));
+        double2 *D = reinterpret_cast<double2 *>(T);
+        for (int e = tid; e < nbi * nbi / 2; e += NCONS) D[e] = __ldcg(S + e);
+    }
     if (tid == 0) ctl->fail = 0;
     named_bar_sync(1, NCONS);
     unsigned long long tp = (a.ptrace && tid == 0) ? globaltimer_ns() : 0;
@@ -879,6 +896,8 @@ __device__ bool mixed_update(const PotrfArgs &a, SmemCtl *ctl, unsigned char *ri
         const int lb = (warp & 3) * 32, half = warp >> 2;
         const int row = half * BLK + lb + lane;                    // within the tile
         double *C = tile_ptr(a, m, n) + row;                       // column stride nbi
+        // streamed matrix: the first chunk writes the tile from the untouched copy
+        const double *S = (a.A0 && kc == 0) ? a.A0 + (C - a.A) : nullptr;
         const double sr = (double)a.scl[m * a.nbs + half];
         // the update goes to L2 as FP64 reductions: no read of C, so no
         // round trip to memory on the epilogue's path.  Chunks of one tile are
@@ -893,10 +912,19 @@ __device__ bool mixed_update(const PotrfArgs &a, SmemCtl *ctl, unsigned char *ri
                 const int cb = c0 + 32 * h;
                 // row and column scales are the same for every panel
                 const double inv = -1.0 / (sr * (double)a.scl[n * a.nbs + cb / BLK]);
+                if (S) {
 #pragma unroll
-                for (int j = 0; j < 32; ++j) {
-                    const int col = cb + j;
-                    if (m != n || row >= col) red_add_f64(C + (int64_t)col * a.nbi, (double)v[h][j] * inv);
+                    for (int j = 0; j < 32; ++j) {
+                        const int col = cb + j;
+                        if (m != n || row >= col)
+                            C[(int64_t)col * a.nbi] = __ldcg(S + (int64_t)col * a.nbi) + (double)v[h][j] * inv;
+                    }
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        const int col = cb + j;
+                        if (m != n || row >= col) red_add_f64(C + (int64_t)col * a.nbi, (double)v[h][j] * inv);
+                    }
                 }
             }
         }
@@ -935,6 +963,8 @@ __device__ bool tc_trsm(const PotrfArgs &a, SmemCtl *ctl, unsigned char *ring16,
     const int nbi = a.nbi;
     const uint32_t tmem = ctl->tmem_base;
     double *Amk = tile_ptr(a, m, k) + bi * BLK;
+    // a streamed matrix's column 0 is read from the untouched copy (the strip's first touch)
+    const double *Asrc = (a.A0 && k == 0) ? a.A0 + (Amk - a.A) : Amk;
     const double sm = (double)a.scl[m * a.nbs + bi];
     const int r = tid & (BLK - 1), kh = tid >> 7;
     const uint32_t sw = (r >> 1) & 3;
@@ -943,7 +973,7 @@ __device__ bool tc_trsm(const PotrfArgs &a, SmemCtl *ctl, unsigned char *ring16,
     // the A values of the next stage are loaded while this one is staged
     double v[16];
 #pragma unroll
-    for (int j = 0; j < 16; ++j) v[j] = __ldcg(Amk + (int64_t)(kh * 16 + j) * nbi + r);
+    for (int j = 0; j < 16; ++j) v[j] = __ldcg(Asrc + (int64_t)(kh * 16 + j) * nbi + r);
     for (int s8 = 0; s8 < MX_NB / MX_KC_SPLIT; ++s8) {
         const uint32_t sidx = st16 % MX_NST, rr = st16 / MX_NST;
         const int q0 = s8 * MX_KC_SPLIT + kh * 16;
@@ -965,7 +995,7 @@ __device__ bool tc_trsm(const PotrfArgs &a, SmemCtl *ctl, unsigned char *ring16,
         }
         if (s8 + 1 < MX_NB / MX_KC_SPLIT) {
 #pragma unroll
-            for (int j = 0; j < 16; ++j) v[j] = __ldcg(Amk + (int64_t)(q0 + MX_KC_SPLIT + j) * nbi + r);
+            for (int j = 0; j < 16; ++j) v[j] = __ldcg(Asrc + (int64_t)(q0 + MX_KC_SPLIT + j) * nbi + r);
         }
         if (rr > 0 && !warp_mbar_wait(&ctl->empty16[sidx], (rr - 1) & 1, a.pipe_limit_ns)) {
             if (lane == 0) report(a, ST_MBAR_TIMEOUT, 14, st16, warp);
@@ -1361,30 +1391,44 @@ std::vector<uint64_t> build_potrf_tasks_mixed(int mt, int nbs, int delay, int S,
 }
 
 // Mixed-precision ticket order in phases of CB tile columns (CB a multiple
-// of S), for a matrix whose tile columns arrive over time: phase p touches
-// only tile columns [c0, c1) = [p CB, p CB + CB) and earlier ones, so it can
-// run as soon as those columns are on the device.  A phase first applies to
-// its columns every chunk closed in earlier phases (catch-up, chunk by chunk
-// so the tiles of a column proceed in parallel), then runs the steps k of
-// its own columns as the single-launch order does, with updates restricted
-// to the phase's columns; the later columns receive those chunks in their
-// own phase.  Each phase is a topological segment: every ticket depends only
-// on tickets of earlier phases or earlier in its own.
+// of S), for a matrix whose tile columns arrive over time and one launch over
+// all phases: phase p's own tickets touch only tile columns [c0, c1) =
+// [p CB, p CB + CB) and earlier ones.  A phase first applies to its columns
+// the chunks closed during the previous phase (catch-up, chunk by chunk so
+// the tiles of a column proceed in parallel), then runs the steps k of its
+// own columns as the single-launch order does, with updates restricted to
+// the phase's columns.  Interleaved with those steps (whose tasks mostly wait
+// on the POTRF -> TRSM chain) it applies to the NEXT phase's columns every
+// chunk closed before this phase began: work that depends on nothing of this
+// phase, only on the next columns' arrival, so the CTAs have work while the
+// chain runs.  Each phase is a topological segment: every ticket depends only
+// on tickets of earlier phases or earlier in its own; every tile receives its
+// chunks in increasing order.
 std::vector<std::vector<uint64_t>> build_potrf_tasks_mixed_phased(int mt, int nbs, int delay, int S, int CB, int bw,
                                                                   int bh)
 {
     std::vector<std::vector<uint64_t>> phases;
     if (mt <= 0 || S <= 0 || CB <= 0 || CB % S) return phases;
+    // chunks c < lo(c0) of the columns of the phase starting at c0 are applied
+    // during the previous phase (those closed before that phase began)
+    auto lo = [&](int c0) { return c0 >= CB ? (c0 - CB) / S : 0; };
+    // chunks [cb, ce) applied to tile columns [n0, n1), chunk by chunk, each
+    // chunk's tiles in blocks
+    auto chunks_to = [&](std::vector<uint64_t> &out, int cb, int ce, int n0, int n1) {
+        for (int c = cb; c < ce; ++c) {
+            std::vector<uint64_t> ch;
+            for (int n = n0; n < n1; ++n)
+                for (int m = n; m < mt; ++m) ch.push_back(make_task(T_GEMM, c, m, n, 0, 0));
+            block_share(ch, bw, bh);
+            out.insert(out.end(), ch.begin(), ch.end());
+        }
+    };
     for (int c0 = 0; c0 < mt; c0 += CB) {
         const int c1 = std::min(mt, c0 + CB);
         std::vector<uint64_t> v;
         auto push_trsm = [&](int k) {
             for (int m = k + 1; m < mt; ++m)
                 for (int bi = 0; bi < nbs; ++bi) v.push_back(make_task(T_TRSM, k, m, k, bi, 0));
-        };
-        auto catch_up = [&](int n) {   // every chunk closed before c0, for tile column n
-            for (int c = 0; c < c0 / S; ++c)
-                for (int m = n; m < mt; ++m) v.push_back(make_task(T_GEMM, c, m, n, 0, 0));
         };
         // share[k - c0]: in-phase update tasks issued in step k
         std::vector<std::vector<uint64_t>> share(c1 - c0);
@@ -1401,18 +1445,22 @@ std::vector<std::vector<uint64_t>> build_potrf_tasks_mixed_phased(int mt, int nb
             }
         }
         for (auto &sh : share) block_share(sh, bw, bh);
-        catch_up(c0);
+        // the next phase's columns, chunks closed before this phase began
+        std::vector<uint64_t> next;
+        if (c1 < mt) chunks_to(next, 0, lo(c1), c1, std::min(mt, c1 + CB));
+        const int nsteps = c1 - c0 - 1;
+        size_t nx = 0;
+        auto filler = [&](int i) {   // the part of `next` issued after own step i of nsteps
+            const size_t e = nsteps > 0 ? next.size() * (size_t)(i + 1) / (size_t)nsteps : next.size();
+            v.insert(v.end(), next.begin() + nx, next.begin() + e);
+            nx = e;
+        };
+        // catch-up: chunks closed during the previous phase, first for column
+        // c0 (its POTRF follows), then for the others
+        chunks_to(v, lo(c0), c0 / S, c0, c0 + 1);
         v.push_back(make_task(T_POTRF, c0, c0, c0, 0, 0));
         push_trsm(c0);
-        // the other columns chunk by chunk, each chunk's tiles in blocks (L2
-        // reuse of the 16-bit panels across the block's columns)
-        for (int c = 0; c < c0 / S; ++c) {
-            std::vector<uint64_t> ch;
-            for (int n = c0 + 1; n < c1; ++n)
-                for (int m = n; m < mt; ++m) ch.push_back(make_task(T_GEMM, c, m, n, 0, 0));
-            block_share(ch, bw, bh);
-            v.insert(v.end(), ch.begin(), ch.end());
-        }
+        chunks_to(v, lo(c0), c0 / S, c0 + 1, c1);
         for (int k = c0; k + 1 < c1; ++k) {
             const int c = k / S;
             for (int m = k + 1; m < mt; ++m) v.push_back(make_task(T_GEMM, c, m, k + 1, 0, 0));
@@ -1422,7 +1470,9 @@ std::vector<std::vector<uint64_t>> build_potrf_tasks_mixed_phased(int mt, int nb
             v.insert(v.end(), rest.begin(), rest.begin() + d);
             push_trsm(k + 1);
             v.insert(v.end(), rest.begin() + d, rest.end());
+            filler(k - c0);
         }
+        if (nsteps <= 0) filler(0);
         phases.push_back(std::move(v));
     }
     return phases;
@@ -1601,6 +1651,9 @@ int potrf_run(Context *ctx, double *dA, int mt, int nbi, int nb_user, int n_user
     a.mx_split = 0;
     a.mx_chunk = 1;
     a.p16_rows = 0;
+    a.A0 = nullptr;
+    a.arrived = nullptr;
+    a.stream_cb = 1;
     CUtensorMap tmap;
     memset(&tmap, 0, sizeof(tmap));
     if (mixed) {
@@ -1829,13 +1882,28 @@ int potrf_run_streamed(Context *ctx, const double *hA, double *A0, double *L, in
                 if (x) cudaEventDestroy(x);
         }
     } ev;
-    // events: [0, nph) copy of phase p landed, [nph] diagonal tiles landed,
-    // [nph + 1 + p] phase p done
+    // events: [0, nph) copy of phase p landed, [nph] diagonal tiles landed
     const bool tl = ctx->stream_trace;
-    ev.v.assign(2 * (nph + 1), nullptr);
+    ev.v.assign(nph + 1, nullptr);
     for (auto &x : ev.v) CK(cudaEventCreateWithFlags(&x, tl ? 0 : cudaEventDisableTiming));
+    // per-phase arrival flags, set by 4-byte copies from a pinned host word
+    // on the copy stream right after each phase's tiles (copy engine only:
+    // nothing on that stream needs an SM while the factorization runs)
+    int *arrived = (int *)ctx->buffer(BUF_ARRIVED, (size_t)nph * sizeof(int));
+    if (!arrived) return DPLASMA_ERR_OUT_OF_RESOURCES;
+    if (!ctx->host_one) {
+        if (cudaHostAlloc((void **)&ctx->host_one, sizeof(int), cudaHostAllocDefault) != cudaSuccess) {
+            ctx->host_one = nullptr;
+            return DPLASMA_ERR_OUT_OF_RESOURCES;
+        }
+        *ctx->host_one = 1;
+    }
+    a.A0 = A0;
+    a.arrived = arrived;
+    a.stream_cb = cb;
     const size_t tile = (size_t)nbi * nbi;
     CK(cudaMemsetAsync(ctr, 0, nctr * sizeof(int), st));
+    CK(cudaMemsetAsync(arrived, 0, (size_t)nph * sizeof(int), st));
     CK(cudaEventRecord(ctx->ev0, st));
     CK(cudaStreamWaitEvent(cs, ctx->ev0, 0));
     // the diagonal tiles first (the row scales of the 16-bit panels)
@@ -1848,36 +1916,22 @@ int potrf_run_streamed(Context *ctx, const double *hA, double *A0, double *L, in
     p16_scale_kernel<<<mt, nbi, 0, st>>>(A0, mt, nbi, a.p16_target, a.scl);
     CK(cudaGetLastError());
     ctx->launches += 1;
-    // the phases: columns [c0, c1) are one contiguous run of tiles
-    const uint64_t *tasks = (const uint64_t *)ctx->buffer(BUF_TASKS_PH, 0);
+    // One launch over all phases (their ticket orders concatenated): a task
+    // that first touches a tile column waits for that column's phase to have
+    // arrived, so the work of the next phase starts while this one's last
+    // steps run.  The columns of phase p are one contiguous run of tiles.
+    a.tasks = (const uint64_t *)ctx->buffer(BUF_TASKS_PH, 0);
+    a.ntasks = (int)ctx->ph_off[nph];
+    potrf_persistent_kernel<true><<<grid, NTHREADS, smem, st>>>(a, tmap, lmap);
+    CK(cudaGetLastError());
+    ctx->launches += 1;
     auto tile_of_col = [&](int c) { return c < mt ? (size_t)lower_tile_index(c, c, mt) : ntl; };
     for (int p = 0; p < nph; ++p) {
         const size_t t0 = tile_of_col(p * cb), t1 = tile_of_col(std::min(mt, p * cb + cb));
         CK(cudaMemcpyAsync(A0 + t0 * tile, hA + t0 * tile, (t1 - t0) * tile * sizeof(double), cudaMemcpyHostToDevice,
                            cs));
+        CK(cudaMemcpyAsync(arrived + p, ctx->host_one, sizeof(int), cudaMemcpyHostToDevice, cs));
         CK(cudaEventRecord(ev.v[p], cs));
-    }
-    // Each phase is queued when the GPU starts the previous one (one phase of
-    // slack), together with the following phases whose copies have already
-    // landed: their tickets are contiguous, so they run as one launch with no
-    // drain between them.
-    for (int p = 0; p < nph;) {
-        if (p >= 2) CK(cudaEventSynchronize(ev.v[nph + 1 + p - 2]));
-        int q = p + 1;
-        while (q < nph && cudaEventQuery(ev.v[q]) == cudaSuccess) ++q;
-        cudaGetLastError();
-        const size_t t0 = tile_of_col(p * cb), t1 = tile_of_col(std::min(mt, q * cb));
-        CK(cudaStreamWaitEvent(st, ev.v[q - 1], 0));
-        CK(cudaMemcpyAsync(L + t0 * tile, A0 + t0 * tile, (t1 - t0) * tile * sizeof(double), cudaMemcpyDeviceToDevice,
-                           st));
-        CK(cudaMemsetAsync(ctr, 0, sizeof(int), st));      // the ticket counter restarts each launch
-        a.tasks = tasks + ctx->ph_off[p];
-        a.ntasks = (int)(ctx->ph_off[q] - ctx->ph_off[p]);
-        potrf_persistent_kernel<true><<<grid, NTHREADS, smem, st>>>(a, tmap, lmap);
-        CK(cudaGetLastError());
-        for (int r = p; r < q; ++r) CK(cudaEventRecord(ev.v[nph + 1 + r], st));   // phases p..q-1 done
-        ctx->launches += 1;
-        p = q;
     }
     CK(cudaEventRecord(ctx->ev1, st));
     int hs[8];
@@ -1888,14 +1942,13 @@ int potrf_run_streamed(Context *ctx, const double *hA, double *A0, double *L, in
     cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
     ctx->last_factor_ms = ms;
     if (tl) {
-        // per phase: host copy landed, phase finished (ms from the start)
+        // per phase: host copy landed (ms from the start); the factorization's end
         for (int p = 0; p < nph; ++p) {
-            float c = 0.f, f = 0.f;
+            float c = 0.f;
             cudaEventElapsedTime(&c, ctx->ev0, ev.v[p]);
-            cudaEventElapsedTime(&f, ctx->ev0, ev.v[nph + 1 + p]);
-            fprintf(stderr, "stream phase %d: copied %.2f finished %.2f ms (%lld tickets)\n", p, c, f,
-                    ctx->ph_off[p + 1] - ctx->ph_off[p]);
+            fprintf(stderr, "stream phase %d: copied %.2f ms (%lld tickets)\n", p, c, ctx->ph_off[p + 1] - ctx->ph_off[p]);
         }
+        fprintf(stderr, "stream factorization finished %.2f ms\n", ms);
     }
     if (hs[3] != ST_OK) {
         ctx->set_error("streamed potrf scheduler status %d; site %d cta %d values %d %d", hs[3], hs[4], hs[5], hs[6],
@@ -2020,6 +2073,9 @@ int potrf_launch_prealloc(cudaStream_t st, double *dA, int mt, int nbi, int nb_u
     a.tc_trsm = 0;
     a.linv16 = nullptr;
     a.linv_scl = nullptr;
+    a.A0 = nullptr;
+    a.arrived = nullptr;
+    a.stream_cb = 1;
     CUtensorMap tmap;
     memset(&tmap, 0, sizeof(tmap));
     const size_t smem = potrf_smem_bytes(false);

@@ -1,10 +1,12 @@
 """GPU tests of the streamed mixed-precision solve: a host matrix in pinned
 memory is copied in phases of tile columns while the factorization runs
-(potrf_run_streamed).  Every tile receives the same chunk updates in the same
-order as in the single-launch factorization, so the refinement takes the same
-steps and the solution agrees with that of the same call on pageable host
-memory (which uploads first) to the rounding of the residual products (whose
-reductions across CTAs are unordered); both meet the check_zaxmb bar of
+(potrf_run_streamed: one launch over the phases' ticket orders; the first
+task touching a tile column waits for that phase's arrival flag and reads the
+untouched copy).  Every tile receives the same chunk updates in the same
+order as in the factorization of an uploaded matrix, so the refinement takes
+the same steps and the solution agrees with that of the same call on pageable
+host memory (which uploads first) to the rounding of the residual products
+(whose reductions across CTAs are unordered); both meet the check_zaxmb bar of
 src/dplasma_zcheck.c."""
 import os
 
@@ -56,9 +58,7 @@ def test_streamed_solve_matches_uploaded(N, fmt, cb):
             del os.environ["DPLASMA_B200_STREAM_CB"]
         else:
             os.environ["DPLASMA_B200_STREAM_CB"] = old
-    mt = N // NB
-    phases = -(-mt // max(cb, 16 if fmt != db.FP16_SPLIT else 8))
-    assert launches >= phases                      # one scheduler launch per phase (and more kernels around)
+    assert launches >= 2                           # the factorization and the refinement's kernels
     assert sts["iter"] == stu["iter"] and sts["fallback"] == stu["fallback"] == 0, (sts, stu)
     assert np.abs(Xs - Xu).max() <= 1e-13 * np.abs(Xu).max()
     keep = np.tril(np.ones((N, N), bool))
