@@ -537,6 +537,17 @@ __device__ void linv16_task(const PotrfArgs &a, int k, const double *Wk, const d
 // diagonal block in shared memory and inverts it, the panel solve and the
 // trailing update run on the FP64 tensor cores.
 // ---------------------------------------------------------------------------
+// Streamed matrix: POTRF(0) is the first touch of tile (0, 0), copied here from
+// the untouched copy by the consumer threads (potrf_task's first barrier
+// orders the copy before the factorization reads the tile).
+__device__ __forceinline__ void stream_first_tile(const PotrfArgs &a)
+{
+    double *T = tile_ptr(a, 0, 0);
+    const double2 *S = reinterpret_cast<const double2 *>(a.A0 + (T - a.A));
+    double2 *D = reinterpret_cast<double2 *>(T);
+    for (int e = threadIdx.x; e < a.nbi * a.nbi / 2; e += NCONS) D[e] = __ldcg(S + e);
+}
+
 template <bool MIXED>
 __device__ void potrf_task(const PotrfArgs &a, SmemCtl *ctl, double *ring, int k)
 {
@@ -554,12 +565,6 @@ __device__ void potrf_task(const PotrfArgs &a, SmemCtl *ctl, double *ring, int k
     double *Lb = Xs + 32 * XP;       // [8][32][4]: blocked copy of the 32x32 factor
 
     for (int e = tid; e < a.nbs * BLK * BLK; e += NCONS) Wk[e] = 0.0;
-    if (MIXED && a.A0 && k == 0) {
-        // streamed matrix: the first touch of tile (0, 0) copies it from the untouched copy
-        const double2 *S = reinterpret_cast<const double2 *>(a.A0 + (T - a.A));
-        double2 *D = reinterpret_cast<double2 *>(T);
-        for (int e = tid; e < nbi * nbi / 2; e += NCONS) D[e] = __ldcg(S + e);
-    }
     if (tid == 0) ctl->fail = 0;
     named_bar_sync(1, NCONS);
     unsigned long long tp = (a.ptrace && tid == 0) ? globaltimer_ns() : 0;
@@ -903,28 +908,36 @@ __device__ bool mixed_update(const PotrfArgs &a, SmemCtl *ctl, unsigned char *ri
         // round trip to memory on the epilogue's path.  Chunks of one tile are
         // still ordered by their dependencies (each waits for the previous
         // chunk's release), so the sum is taken in a fixed order per element.
-        for (int c0 = 0; c0 < a.nbi; c0 += 64) {
-            if (m == n && c0 > row - lane + 31) break;             // above the diagonal
-            float v[2][32];
-            tmem_ld32x2(tmem + ((uint32_t)lb << 16) + (uint32_t)(256 * half + c0), v[0], v[1]);
+        // (A streamed matrix's first chunk stores S + update instead: one
+        // branch per task, so the reduction loop stays as it is.)
+        if (!S) {
+            for (int c0 = 0; c0 < a.nbi; c0 += 64) {
+                if (m == n && c0 > row - lane + 31) break;             // above the diagonal
+                float v[2][32];
+                tmem_ld32x2(tmem + ((uint32_t)lb << 16) + (uint32_t)(256 * half + c0), v[0], v[1]);
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int cb = c0 + 32 * h;
-                // row and column scales are the same for every panel
-                const double inv = -1.0 / (sr * (double)a.scl[n * a.nbs + cb / BLK]);
-                if (S) {
-#pragma unroll
-                    for (int j = 0; j < 32; ++j) {
-                        const int col = cb + j;
-                        if (m != n || row >= col)
-                            C[(int64_t)col * a.nbi] = __ldcg(S + (int64_t)col * a.nbi) + (double)v[h][j] * inv;
-                    }
-                } else {
+                for (int h = 0; h < 2; ++h) {
+                    const int cb = c0 + 32 * h;
+                    // row and column scales are the same for every panel
+                    const double inv = -1.0 / (sr * (double)a.scl[n * a.nbs + cb / BLK]);
 #pragma unroll
                     for (int j = 0; j < 32; ++j) {
                         const int col = cb + j;
                         if (m != n || row >= col) red_add_f64(C + (int64_t)col * a.nbi, (double)v[h][j] * inv);
                     }
+                }
+            }
+        } else {
+            for (int c0 = 0; c0 < a.nbi; c0 += 32) {
+                if (m == n && c0 > row - lane + 31) break;
+                float v[32];
+                tmem_ld32(tmem + ((uint32_t)lb << 16) + (uint32_t)(256 * half + c0), v);
+                const double inv = -1.0 / (sr * (double)a.scl[n * a.nbs + c0 / BLK]);
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    const int col = c0 + j;
+                    if (m != n || row >= col)
+                        C[(int64_t)col * a.nbi] = __ldcg(S + (int64_t)col * a.nbi) + (double)v[j] * inv;
                 }
             }
         }
@@ -1140,6 +1153,7 @@ __device__ void consumer_warps(const PotrfArgs &a, SmemCtl *ctl, double *ring)
         int *release = nullptr;
         bool ok = true;
         if (ty == T_POTRF) {
+            if (MIXED && a.A0 && k == 0) stream_first_tile(a);
             potrf_task<MIXED>(a, ctl, ring, k);
             if (!ctl->fail) release = a.potrf_done + k;
         } else if (ty == T_TRSM && tc_strip<MIXED>(a, k, m)) {
