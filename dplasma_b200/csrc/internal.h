@@ -44,7 +44,6 @@ enum BufferId : int {
     BUF_LINV16,       // inverses of the diagonal tiles in split FP16 (tensor-core TRSM strips)
     BUF_WTRACE,       // opt-in trace of the triangular sweeps
     BUF_ARRIVED,      // streamed factorization: per-phase arrival flags
-    BUF_TASKS_PH,     // phased ticket order of the streamed factorization
     BUF_WM,           // triangular sweeps: the critical path's products W_b L_{b,b-1}
     BUF_COUNT
 };
@@ -84,8 +83,6 @@ struct Context {
     int stream_cb = 0;                       // tile columns per phase of the streamed factorization (0: 16)
     bool no_stream = false;                  // DPLASMA_B200_NO_STREAM: upload host matrices before factoring
     bool stream_trace = false;               // DPLASMA_B200_STREAM_TRACE: print the streamed phases' timeline
-    int ph_mt = -1, ph_chunk = -1, ph_cb = -1, ph_delay = -1;   // cached phased ticket order
-    std::vector<long long> ph_off;
     double last_factor_ms = 0.0, last_solve_ms = 0.0;
     int launches = 0;
     long long last_tasks_executed = 0;

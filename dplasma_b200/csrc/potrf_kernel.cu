@@ -62,14 +62,10 @@ __device__ bool wait_deps(const PotrfArgs &a, uint64_t t)
 {
     const int k = task_k(t), m = task_m(t), n = task_n(t);
     const int nbs = a.nbs;
-    if (MIXED && a.A0) {
-        // streamed matrix: a task that reads the untouched copy waits until
-        // its tile column has arrived (POTRF(0) and the strips of column 0,
-        // the first update chunk (k == 0) of tile (m, n))
-        const int ty = task_type(t);
-        const int col = (ty == T_GEMM) ? (k == 0 ? n : -1) : (k == 0 ? 0 : -1);
-        if (col >= 0 && !wait_flag_sys(a.arrived + col / a.stream_cb, a.abort_flag, a.status, a.dep_limit_ns))
-            return false;
+    if (MIXED && a.A0 && task_type(t) != T_GEMM) {
+        // streamed matrix: POTRF(k) and the strips of column k read the
+        // untouched copy of tile column k (the updates need no input data)
+        if (!wait_flag_sys(a.arrived + k / a.stream_cb, a.abort_flag, a.status, a.dep_limit_ns)) return false;
     }
     switch (task_type(t)) {
     case T_POTRF:
@@ -118,7 +114,7 @@ __device__ void producer_warp(const PotrfArgs &a, SmemCtl *ctl, double *ring, co
 {
     constexpr uint32_t NST = MIXED ? NSTAGE_MIXED : NSTAGE;
     const int lane = threadIdx.x & 31;
-    uint32_t stage_it = 0, task_it = 0, epi_it = 0, st16 = 0;
+    uint32_t stage_it = 0, task_it = 0, epi_it = 0, st16 = 0, prep_it = 0;
     unsigned char *ring16 = MIXED ? ring16_of(ring) : nullptr;
     if (MIXED && lane == 0) {
         tma_prefetch_desc(tmap);
@@ -271,6 +267,16 @@ __device__ void producer_warp(const PotrfArgs &a, SmemCtl *ctl, double *ring, co
             if (!pipe_ok) break;
             continue;
         }
+        if (MIXED && a.A0 && ty == T_TRSM) {
+            // streamed matrix: the consumers first add the untouched copy into the strip
+            if (!warp_mbar_wait(&ctl->prep, prep_it & 1, a.pipe_limit_ns)) {
+                if (lane == 0) report(a, ST_MBAR_TIMEOUT, 17, prep_it, tk);
+                pipe_ok = false;
+                break;
+            }
+            prep_it++;
+            fence_proxy_async();
+        }
         const int nj = task_njobs(a, t);
         bool prev_signal = false;
         for (int j = 0; j < nj && pipe_ok; ++j) {
@@ -386,8 +392,6 @@ __device__ __forceinline__ bool consume_job(const PotrfArgs &a, SmemCtl *ctl, co
                 double *p = jb.C + (int64_t)c * jb.ldc + r;
                 if (jb.mode == J_STORE) {
                     *p = acc[mi][ni][q];
-                } else if (jb.mode == J_SUB_SRC) {
-                    *p = __ldcg(jb.src + (int64_t)c * jb.ldc + r) - acc[mi][ni][q];
                 } else if (jb.mode == J_SUB || r >= c) {
                     atomicAdd(p, -acc[mi][ni][q]);
                 }
@@ -537,15 +541,21 @@ __device__ void linv16_task(const PotrfArgs &a, int k, const double *Wk, const d
 // diagonal block in shared memory and inverts it, the panel solve and the
 // trailing update run on the FP64 tensor cores.
 // ---------------------------------------------------------------------------
-// Streamed matrix: POTRF(0) is the first touch of tile (0, 0), copied here from
-// the untouched copy by the consumer threads (potrf_task's first barrier
-// orders the copy before the factorization reads the tile).
-__device__ __forceinline__ void stream_first_tile(const PotrfArgs &a)
+// Streamed matrix: the updates accumulated in A (from zero); the consumer
+// threads add the untouched copy of `rows` rows from row r0 of tile (m, k)
+// (all its columns) before the task that factors or solves it reads them.
+__device__ __forceinline__ void stream_add_rows(const PotrfArgs &a, int m, int k, int r0, int rows)
 {
-    double *T = tile_ptr(a, 0, 0);
-    const double2 *S = reinterpret_cast<const double2 *>(a.A0 + (T - a.A));
-    double2 *D = reinterpret_cast<double2 *>(T);
-    for (int e = threadIdx.x; e < a.nbi * a.nbi / 2; e += NCONS) D[e] = __ldcg(S + e);
+    double *T = tile_ptr(a, m, k) + r0;
+    const double *S = a.A0 + (T - a.A);
+    const int per_col = rows / 2;                 // double2 per column
+    for (int e = threadIdx.x; e < a.nbi * per_col; e += NCONS) {
+        const int c = e / per_col, r = 2 * (e % per_col);
+        double2 *d = reinterpret_cast<double2 *>(T + (int64_t)c * a.nbi + r);
+        const double2 s2 = __ldcg(reinterpret_cast<const double2 *>(S + (int64_t)c * a.nbi + r));
+        const double2 t2 = __ldcg(d);
+        *d = make_double2(t2.x + s2.x, t2.y + s2.y);
+    }
 }
 
 template <bool MIXED>
@@ -901,43 +911,24 @@ __device__ bool mixed_update(const PotrfArgs &a, SmemCtl *ctl, unsigned char *ri
         const int lb = (warp & 3) * 32, half = warp >> 2;
         const int row = half * BLK + lb + lane;                    // within the tile
         double *C = tile_ptr(a, m, n) + row;                       // column stride nbi
-        // streamed matrix: the first chunk writes the tile from the untouched copy
-        const double *S = (a.A0 && kc == 0) ? a.A0 + (C - a.A) : nullptr;
         const double sr = (double)a.scl[m * a.nbs + half];
         // the update goes to L2 as FP64 reductions: no read of C, so no
         // round trip to memory on the epilogue's path.  Chunks of one tile are
         // still ordered by their dependencies (each waits for the previous
         // chunk's release), so the sum is taken in a fixed order per element.
-        // (A streamed matrix's first chunk stores S + update instead: one
-        // branch per task, so the reduction loop stays as it is.)
-        if (!S) {
-            for (int c0 = 0; c0 < a.nbi; c0 += 64) {
-                if (m == n && c0 > row - lane + 31) break;             // above the diagonal
-                float v[2][32];
-                tmem_ld32x2(tmem + ((uint32_t)lb << 16) + (uint32_t)(256 * half + c0), v[0], v[1]);
+        for (int c0 = 0; c0 < a.nbi; c0 += 64) {
+            if (m == n && c0 > row - lane + 31) break;             // above the diagonal
+            float v[2][32];
+            tmem_ld32x2(tmem + ((uint32_t)lb << 16) + (uint32_t)(256 * half + c0), v[0], v[1]);
 #pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const int cb = c0 + 32 * h;
-                    // row and column scales are the same for every panel
-                    const double inv = -1.0 / (sr * (double)a.scl[n * a.nbs + cb / BLK]);
-#pragma unroll
-                    for (int j = 0; j < 32; ++j) {
-                        const int col = cb + j;
-                        if (m != n || row >= col) red_add_f64(C + (int64_t)col * a.nbi, (double)v[h][j] * inv);
-                    }
-                }
-            }
-        } else {
-            for (int c0 = 0; c0 < a.nbi; c0 += 32) {
-                if (m == n && c0 > row - lane + 31) break;
-                float v[32];
-                tmem_ld32(tmem + ((uint32_t)lb << 16) + (uint32_t)(256 * half + c0), v);
-                const double inv = -1.0 / (sr * (double)a.scl[n * a.nbs + c0 / BLK]);
+            for (int h = 0; h < 2; ++h) {
+                const int cb = c0 + 32 * h;
+                // row and column scales are the same for every panel
+                const double inv = -1.0 / (sr * (double)a.scl[n * a.nbs + cb / BLK]);
 #pragma unroll
                 for (int j = 0; j < 32; ++j) {
-                    const int col = c0 + j;
-                    if (m != n || row >= col)
-                        C[(int64_t)col * a.nbi] = __ldcg(S + (int64_t)col * a.nbi) + (double)v[j] * inv;
+                    const int col = cb + j;
+                    if (m != n || row >= col) red_add_f64(C + (int64_t)col * a.nbi, (double)v[h][j] * inv);
                 }
             }
         }
@@ -976,8 +967,8 @@ __device__ bool tc_trsm(const PotrfArgs &a, SmemCtl *ctl, unsigned char *ring16,
     const int nbi = a.nbi;
     const uint32_t tmem = ctl->tmem_base;
     double *Amk = tile_ptr(a, m, k) + bi * BLK;
-    // a streamed matrix's column 0 is read from the untouched copy (the strip's first touch)
-    const double *Asrc = (a.A0 && k == 0) ? a.A0 + (Amk - a.A) : Amk;
+    // streamed matrix: A is the untouched copy plus the accumulated updates
+    const double *A0mk = a.A0 ? a.A0 + (Amk - a.A) : nullptr;
     const double sm = (double)a.scl[m * a.nbs + bi];
     const int r = tid & (BLK - 1), kh = tid >> 7;
     const uint32_t sw = (r >> 1) & 3;
@@ -986,7 +977,11 @@ __device__ bool tc_trsm(const PotrfArgs &a, SmemCtl *ctl, unsigned char *ring16,
     // the A values of the next stage are loaded while this one is staged
     double v[16];
 #pragma unroll
-    for (int j = 0; j < 16; ++j) v[j] = __ldcg(Asrc + (int64_t)(kh * 16 + j) * nbi + r);
+    for (int j = 0; j < 16; ++j) v[j] = __ldcg(Amk + (int64_t)(kh * 16 + j) * nbi + r);
+    if (A0mk) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) v[j] += __ldcg(A0mk + (int64_t)(kh * 16 + j) * nbi + r);
+    }
     for (int s8 = 0; s8 < MX_NB / MX_KC_SPLIT; ++s8) {
         const uint32_t sidx = st16 % MX_NST, rr = st16 / MX_NST;
         const int q0 = s8 * MX_KC_SPLIT + kh * 16;
@@ -1008,7 +1003,11 @@ __device__ bool tc_trsm(const PotrfArgs &a, SmemCtl *ctl, unsigned char *ring16,
         }
         if (s8 + 1 < MX_NB / MX_KC_SPLIT) {
 #pragma unroll
-            for (int j = 0; j < 16; ++j) v[j] = __ldcg(Asrc + (int64_t)(q0 + MX_KC_SPLIT + j) * nbi + r);
+            for (int j = 0; j < 16; ++j) v[j] = __ldcg(Amk + (int64_t)(q0 + MX_KC_SPLIT + j) * nbi + r);
+            if (A0mk) {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) v[j] += __ldcg(A0mk + (int64_t)(q0 + MX_KC_SPLIT + j) * nbi + r);
+            }
         }
         if (rr > 0 && !warp_mbar_wait(&ctl->empty16[sidx], (rr - 1) & 1, a.pipe_limit_ns)) {
             if (lane == 0) report(a, ST_MBAR_TIMEOUT, 14, st16, warp);
@@ -1153,7 +1152,7 @@ __device__ void consumer_warps(const PotrfArgs &a, SmemCtl *ctl, double *ring)
         int *release = nullptr;
         bool ok = true;
         if (ty == T_POTRF) {
-            if (MIXED && a.A0 && k == 0) stream_first_tile(a);
+            if (MIXED && a.A0) stream_add_rows(a, k, k, 0, a.nbi);   // potrf_task's first barrier orders it
             potrf_task<MIXED>(a, ctl, ring, k);
             if (!ctl->fail) release = a.potrf_done + k;
         } else if (ty == T_TRSM && tc_strip<MIXED>(a, k, m)) {
@@ -1163,6 +1162,14 @@ __device__ void consumer_warps(const PotrfArgs &a, SmemCtl *ctl, double *ring)
             ok = mixed_update(a, ctl, ring16, t, st16, mx_it);
             release = a.upd_done + (int64_t)m * a.mt + n;
         } else {
+            if (MIXED && a.A0 && ty == T_TRSM) {
+                // streamed matrix: the strip's rows = untouched copy + updates,
+                // in place, before the producer loads them
+                stream_add_rows(a, m, k, task_bi(t) * BLK, BLK);
+                fence_proxy_async();
+                __syncwarp();
+                if ((tid & 31) == 0) mbar_arrive(&ctl->prep);
+            }
             const int nj = task_njobs(a, t);
             for (int j = 0; j < nj; ++j) {
                 const Job jb = task_job(a, t, j);
@@ -1233,6 +1240,7 @@ __global__ void __launch_bounds__(NTHREADS, 1)
         }
         mbar_init(&ctl->tmem_full, 1);
         mbar_init(&ctl->epi, 1);
+        mbar_init(&ctl->prep, NCONS / 32);
         ctl->fail = 0;
     }
     if (MIXED && threadIdx.x < 32) {
@@ -1402,94 +1410,6 @@ std::vector<uint64_t> build_potrf_tasks_mixed(int mt, int nbs, int delay, int S,
         v.insert(v.end(), rest.begin() + d, rest.end());
     }
     return v;
-}
-
-// Mixed-precision ticket order in phases of CB tile columns (CB a multiple
-// of S), for a matrix whose tile columns arrive over time and one launch over
-// all phases: phase p's own tickets touch only tile columns [c0, c1) =
-// [p CB, p CB + CB) and earlier ones.  A phase first applies to its columns
-// the chunks closed during the previous phase (catch-up, chunk by chunk so
-// the tiles of a column proceed in parallel), then runs the steps k of its
-// own columns as the single-launch order does, with updates restricted to
-// the phase's columns.  Interleaved with those steps (whose tasks mostly wait
-// on the POTRF -> TRSM chain) it applies to the NEXT phase's columns every
-// chunk closed before this phase began: work that depends on nothing of this
-// phase, only on the next columns' arrival, so the CTAs have work while the
-// chain runs.  Each phase is a topological segment: every ticket depends only
-// on tickets of earlier phases or earlier in its own; every tile receives its
-// chunks in increasing order.
-std::vector<std::vector<uint64_t>> build_potrf_tasks_mixed_phased(int mt, int nbs, int delay, int S, int CB, int bw,
-                                                                  int bh)
-{
-    std::vector<std::vector<uint64_t>> phases;
-    if (mt <= 0 || S <= 0 || CB <= 0 || CB % S) return phases;
-    // chunks c < lo(c0) of the columns of the phase starting at c0 are applied
-    // during the previous phase (those closed before that phase began)
-    auto lo = [&](int c0) { return c0 >= CB ? (c0 - CB) / S : 0; };
-    // chunks [cb, ce) applied to tile columns [n0, n1), chunk by chunk, each
-    // chunk's tiles in blocks
-    auto chunks_to = [&](std::vector<uint64_t> &out, int cb, int ce, int n0, int n1) {
-        for (int c = cb; c < ce; ++c) {
-            std::vector<uint64_t> ch;
-            for (int n = n0; n < n1; ++n)
-                for (int m = n; m < mt; ++m) ch.push_back(make_task(T_GEMM, c, m, n, 0, 0));
-            block_share(ch, bw, bh);
-            out.insert(out.end(), ch.begin(), ch.end());
-        }
-    };
-    for (int c0 = 0; c0 < mt; c0 += CB) {
-        const int c1 = std::min(mt, c0 + CB);
-        std::vector<uint64_t> v;
-        auto push_trsm = [&](int k) {
-            for (int m = k + 1; m < mt; ++m)
-                for (int bi = 0; bi < nbs; ++bi) v.push_back(make_task(T_TRSM, k, m, k, bi, 0));
-        };
-        // share[k - c0]: in-phase update tasks issued in step k
-        std::vector<std::vector<uint64_t>> share(c1 - c0);
-        for (int c = c0 / S; c * S + S - 1 < c1; ++c) {
-            const int k = c * S + S - 1;
-            long long work = 0;
-            for (int n = k + 2; n < c1; ++n) work += mt - n;
-            long long done = 0;
-            for (int n = k + 2; n < c1; ++n) {
-                int part = (int)((done * S) / (work > 0 ? work : 1));
-                part = std::min(part, std::min(S - 1, n - 2 - k));
-                for (int m = n; m < mt; ++m) share[k + part - c0].push_back(make_task(T_GEMM, c, m, n, 0, 0));
-                done += mt - n;
-            }
-        }
-        for (auto &sh : share) block_share(sh, bw, bh);
-        // the next phase's columns, chunks closed before this phase began
-        std::vector<uint64_t> next;
-        if (c1 < mt) chunks_to(next, 0, lo(c1), c1, std::min(mt, c1 + CB));
-        const int nsteps = c1 - c0 - 1;
-        size_t nx = 0;
-        auto filler = [&](int i) {   // the part of `next` issued after own step i of nsteps
-            const size_t e = nsteps > 0 ? next.size() * (size_t)(i + 1) / (size_t)nsteps : next.size();
-            v.insert(v.end(), next.begin() + nx, next.begin() + e);
-            nx = e;
-        };
-        // catch-up: chunks closed during the previous phase, first for column
-        // c0 (its POTRF follows), then for the others
-        chunks_to(v, lo(c0), c0 / S, c0, c0 + 1);
-        v.push_back(make_task(T_POTRF, c0, c0, c0, 0, 0));
-        push_trsm(c0);
-        chunks_to(v, lo(c0), c0 / S, c0 + 1, c1);
-        for (int k = c0; k + 1 < c1; ++k) {
-            const int c = k / S;
-            for (int m = k + 1; m < mt; ++m) v.push_back(make_task(T_GEMM, c, m, k + 1, 0, 0));
-            v.push_back(make_task(T_POTRF, k + 1, k + 1, k + 1, 0, 0));
-            const std::vector<uint64_t> &rest = share[k - c0];
-            const size_t d = std::min<size_t>(rest.size(), (size_t)std::max(delay, 0));
-            v.insert(v.end(), rest.begin(), rest.begin() + d);
-            push_trsm(k + 1);
-            v.insert(v.end(), rest.begin() + d, rest.end());
-            filler(k - c0);
-        }
-        if (nsteps <= 0) filler(0);
-        phases.push_back(std::move(v));
-    }
-    return phases;
 }
 
 // ---------------------------------------------------------------------------
@@ -1792,14 +1712,15 @@ int potrf_run(Context *ctx, double *dA, int mt, int nbi, int nb_user, int n_user
 // host: the mixed-precision factorization of a matrix streamed from pinned
 // host memory (lower tiles already in the device layout).  The tile columns
 // are copied in phases of cb columns on the context's copy stream into A0
-// (the untouched copy the refinement reads); phase p of the phased ticket
-// order runs as soon as its columns are on the device: the compute stream
-// waits for the copy stream's event of that phase, copies the phase's tiles
-// into L (the working copy) and launches the phase, so the host copies of
-// the next phases overlap the factorization of this one and no kernel ever
-// waits for a copy.  The diagonal tiles go first, for the 16-bit scales.
-// Dependency counters carry over from phase to phase; only the ticket
-// counter restarts.  DPLASMA_B200_STREAM_TRACE=1 prints the timeline.
+// (the untouched copy the refinement reads), each phase followed by a 4-byte
+// copy that sets its arrival flag.  One launch of the ordinary ticket order
+// runs meanwhile on a working copy L that starts at zero: the update tasks
+// accumulate into it without waiting for any data, and POTRF(k) and the
+// strips of tile column k wait (bounded) for that column's flag and add A0 to
+// what has accumulated.  So the trailing updates of the first panels, most
+// of the work, run while the rest of the matrix is still in flight.  The
+// diagonal tiles go first, for the 16-bit scales.
+// DPLASMA_B200_STREAM_TRACE=1 prints the timeline.
 // ---------------------------------------------------------------------------
 int potrf_run_streamed(Context *ctx, const double *hA, double *A0, double *L, int mt, int nbi, int nb_user,
                        int n_user, int *info, int p16_fmt)
@@ -1812,27 +1733,22 @@ int potrf_run_streamed(Context *ctx, const double *hA, double *A0, double *L, in
         return DPLASMA_ERR_NOT_SUPPORTED;
     }
     const int chunk = ctx->mx_chunk > 0 ? ctx->mx_chunk : (p16_fmt == 2 ? 8 : 16);
-    int cb = ctx->stream_cb > 0 ? ctx->stream_cb : 16;
-    cb = ((std::max(cb, chunk) + chunk - 1) / chunk) * chunk;
-    if (ctx->ph_mt != mt || ctx->ph_chunk != chunk || ctx->ph_cb != cb || ctx->ph_delay != ctx->mx_delay) {
-        const auto ph = build_potrf_tasks_mixed_phased(mt, nbs, ctx->mx_delay, chunk, cb, ctx->mx_block_w,
-                                                       ctx->mx_block_h);
-        std::vector<uint64_t> all;
-        ctx->ph_off.assign(1, 0);
-        for (const auto &v : ph) {
-            all.insert(all.end(), v.begin(), v.end());
-            ctx->ph_off.push_back((long long)all.size());
-        }
-        uint64_t *dt = (uint64_t *)ctx->buffer(BUF_TASKS_PH, all.size() * sizeof(uint64_t));
+    const int cb = ctx->stream_cb > 0 ? ctx->stream_cb : 16;       // tile columns per copy phase
+    // the ticket order of the mixed factorization (the same as for a matrix
+    // already on the device, and the same cache)
+    if (ctx->task_mt != mt || ctx->task_nbs != nbs || ctx->task_delay != ctx->mx_delay || ctx->task_mixed != chunk) {
+        std::vector<uint64_t> tasks =
+            build_potrf_tasks_mixed(mt, nbs, ctx->mx_delay, chunk, ctx->mx_block_w, ctx->mx_block_h);
+        uint64_t *dt = (uint64_t *)ctx->buffer(BUF_TASKS, tasks.size() * sizeof(uint64_t));
         if (!dt) return DPLASMA_ERR_OUT_OF_RESOURCES;
-        CK(cudaMemcpyAsync(dt, all.data(), all.size() * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
-        CK(cudaStreamSynchronize(st));
-        ctx->ph_mt = mt;
-        ctx->ph_chunk = chunk;
-        ctx->ph_cb = cb;
-        ctx->ph_delay = ctx->mx_delay;
+        CK(cudaMemcpyAsync(dt, tasks.data(), tasks.size() * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+        ctx->task_mt = mt;
+        ctx->task_nbs = nbs;
+        ctx->task_delay = ctx->mx_delay;
+        ctx->task_mixed = chunk;
+        ctx->ntasks = (int)tasks.size();
     }
-    const int nph = (int)ctx->ph_off.size() - 1;
+    const int nph = (mt + cb - 1) / cb;
     double *W = (double *)ctx->buffer(BUF_W, (size_t)mt * nbs * BLK * BLK * sizeof(double));
     const size_t nctr = 8 + (size_t)mt + 2 * (size_t)mt * mt + grid;
     int *ctr = (int *)ctx->buffer(BUF_COUNTERS, nctr * sizeof(int));
@@ -1918,6 +1834,9 @@ int potrf_run_streamed(Context *ctx, const double *hA, double *A0, double *L, in
     const size_t tile = (size_t)nbi * nbi;
     CK(cudaMemsetAsync(ctr, 0, nctr * sizeof(int), st));
     CK(cudaMemsetAsync(arrived, 0, (size_t)nph * sizeof(int), st));
+    // the working copy starts at zero: the updates accumulate there before
+    // their tiles arrive
+    CK(cudaMemsetAsync(L, 0, ntl * tile * sizeof(double), st));
     CK(cudaEventRecord(ctx->ev0, st));
     CK(cudaStreamWaitEvent(cs, ctx->ev0, 0));
     // the diagonal tiles first (the row scales of the 16-bit panels)
@@ -1930,12 +1849,11 @@ int potrf_run_streamed(Context *ctx, const double *hA, double *A0, double *L, in
     p16_scale_kernel<<<mt, nbi, 0, st>>>(A0, mt, nbi, a.p16_target, a.scl);
     CK(cudaGetLastError());
     ctx->launches += 1;
-    // One launch over all phases (their ticket orders concatenated): a task
-    // that first touches a tile column waits for that column's phase to have
-    // arrived, so the work of the next phase starts while this one's last
-    // steps run.  The columns of phase p are one contiguous run of tiles.
-    a.tasks = (const uint64_t *)ctx->buffer(BUF_TASKS_PH, 0);
-    a.ntasks = (int)ctx->ph_off[nph];
+    // One launch in the ordinary ticket order: the updates never wait for
+    // data, POTRF(k) and the strips of column k wait for column k's phase.
+    // The columns of phase p are one contiguous run of tiles.
+    a.tasks = (const uint64_t *)ctx->buffer(BUF_TASKS, 0);
+    a.ntasks = ctx->ntasks;
     potrf_persistent_kernel<true><<<grid, NTHREADS, smem, st>>>(a, tmap, lmap);
     CK(cudaGetLastError());
     ctx->launches += 1;
@@ -1960,7 +1878,7 @@ int potrf_run_streamed(Context *ctx, const double *hA, double *A0, double *L, in
         for (int p = 0; p < nph; ++p) {
             float c = 0.f;
             cudaEventElapsedTime(&c, ctx->ev0, ev.v[p]);
-            fprintf(stderr, "stream phase %d: copied %.2f ms (%lld tickets)\n", p, c, ctx->ph_off[p + 1] - ctx->ph_off[p]);
+            fprintf(stderr, "stream phase %d: copied %.2f ms\n", p, c);
         }
         fprintf(stderr, "stream factorization finished %.2f ms\n", ms);
     }
@@ -2122,21 +2040,6 @@ extern "C" int dplasma_b200_debug_task_list_blocked(int mixed_chunk, int mt, int
     return (int)v.size();
 }
 
-// The phased order: all phases concatenated into `out`; ends[p] = end of phase p.
-extern "C" int dplasma_b200_debug_task_list_phased(int mixed_chunk, int mt, int nbs, int delay, int cb,
-                                                   unsigned long long *out, int cap, int *ends, int ends_cap)
-{
-    const auto ph = db2::build_potrf_tasks_mixed_phased(mt, nbs, delay, mixed_chunk, cb, 16, 16);
-    size_t n = 0;
-    for (size_t p = 0; p < ph.size(); ++p) {
-        for (uint64_t t : ph[p]) {
-            if ((int)n < cap) out[n] = t;
-            ++n;
-        }
-        if ((int)p < ends_cap) ends[p] = (int)n;
-    }
-    return (int)n;
-}
 
 extern "C" int dplasma_b200_debug_task_list(int mixed_chunk, int mt, int nbs, int delay, unsigned long long *out,
                                             int cap)

@@ -136,9 +136,9 @@ struct PotrfArgs {
     // mixed precision, matrix streamed from the host (null otherwise): the
     // untouched copy A0 (same layout as A) receives the tile columns phase by
     // phase (arrived[p] != 0 once columns [p*stream_cb, (p+1)*stream_cb) are
-    // in, written by the copy engine); the first task touching a tile reads
-    // A0 and writes A: POTRF(0), the TRSM strips of column 0, and the first
-    // update chunk of every other tile
+    // in, written by the copy engine).  A starts at zero and accumulates the
+    // updates, which therefore need no input data; POTRF(k) and the strips of
+    // tile column k wait for that column and add A0 to what accumulated
     const double *A0;
     const int *arrived;
     int stream_cb;
@@ -156,9 +156,7 @@ __device__ __forceinline__ double *wblk_ptr(const PotrfArgs &a, int k, int b)
 // One GEMM job: C(128x128) {-=, =} A(128 x K) * B(128 x K)^T.  A and B are
 // given by their first element and column stride; every column segment of
 // 128 doubles is contiguous (1 KB), which is what the bulk copies move.
-// J_SUB_SRC: C = src - A B^T, src the block of the untouched copy at C's place
-// (first touch of a tile of a streamed matrix)
-enum : int { J_SUB = 0, J_SUB_LOWER = 1, J_STORE = 2, J_SUB_SRC = 3 };
+enum : int { J_SUB = 0, J_SUB_LOWER = 1, J_STORE = 2 };
 struct Job {
     const double *A;
     const double *B;
@@ -171,7 +169,6 @@ struct Job {
     // written by the same epilogue (K-major rows of pitch nbi; null otherwise)
     unsigned short *p16;
     float p16_scale;
-    const double *src;   // J_SUB_SRC only
 };
 
 // The job sequence of a task (identical on producer and consumer sides).
@@ -198,7 +195,6 @@ __device__ __forceinline__ Job task_job(const PotrfArgs &a, uint64_t t, int j)
         jb.signal = false;
         jb.p16 = nullptr;
         jb.p16_scale = 1.f;
-        jb.src = nullptr;
     } else if (a.nbs == 2 && a.Wx && !a.tc_trsm) {
         // TRSM strip bi of a 256-wide tile (m,k) with the whole inverse of
         // L(k,k) = [L00 0; L10 L11]:  L^-1 = [W0 0; Linv10 W1],
@@ -221,7 +217,6 @@ __device__ __forceinline__ Job task_job(const PotrfArgs &a, uint64_t t, int j)
         jb.signal = false;
         jb.p16 = nullptr;
         jb.p16_scale = 1.f;
-        jb.src = nullptr;
         if (a.P16) {
             const int64_t row0 = lower_tile_index(m, k, a.mt) * nbi + bi * BLK;
             jb.p16 = reinterpret_cast<unsigned short *>(a.P16) + row0 * nbi + p * BLK;
@@ -234,12 +229,8 @@ __device__ __forceinline__ Job task_job(const PotrfArgs &a, uint64_t t, int j)
         const bool store = (j % 2) == 0;
         double *Amk = tile_ptr(a, m, k);
         double *Cp = Amk + (int64_t)p * BLK * nbi + bi * BLK;
-        // a streamed matrix's column 0 is read from the untouched copy: the
-        // strip's first touch of the tile
-        const double *Sp = (a.A0 && k == 0) ? a.A0 + (Cp - a.A) : nullptr;
-        jb.src = nullptr;
         if (store) {
-            jb.A = (Sp && p == 0) ? Sp : Cp; jb.lda = nbi;
+            jb.A = Cp; jb.lda = nbi;
             jb.B = wblk_ptr(a, k, p); jb.ldb = BLK;
             jb.K = BLK;
             jb.mode = J_STORE;
@@ -248,8 +239,7 @@ __device__ __forceinline__ Job task_job(const PotrfArgs &a, uint64_t t, int j)
             jb.A = Amk + bi * BLK; jb.lda = nbi;                    // X_0..X_{p-1}
             jb.B = tile_ptr(a, k, k) + p * BLK; jb.ldb = nbi;        // L(k,k)[p, 0:p]
             jb.K = p * BLK;
-            jb.mode = Sp ? J_SUB_SRC : J_SUB;
-            jb.src = Sp;
+            jb.mode = J_SUB;
             jb.signal = true;
         }
         jb.C = Cp; jb.ldc = nbi;
@@ -271,6 +261,7 @@ struct __align__(16) SmemCtl {
     uint64_t tfull[TASKQ];
     uint64_t tempty[TASKQ];
     uint64_t epi;
+    uint64_t prep;     // streamed matrix: the consumers added A0 into an FP64 strip's rows
     uint64_t task[TASKQ];
     uint64_t full16[MX_NST];
     uint64_t empty16[MX_NST];

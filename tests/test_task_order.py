@@ -103,45 +103,3 @@ def test_mixed_blocked_ticket_order(mt, S, bw, bh, delay):
     tl = tasks_blocked(S, mt, 2, delay, bw, bh)
     replay(tl, mt, 2, S)
     assert sorted(tl) == sorted(tasks(S, mt, 2, delay))
-
-
-def tasks_phased(chunk, mt, nbs, delay, cb):
-    L = db.lib()
-    f = L.dplasma_b200_debug_task_list_phased
-    f.argtypes = [ctypes.c_int] * 5 + [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int]
-    n = f(chunk, mt, nbs, delay, cb, None, 0, None, 0)
-    out = np.zeros(n, dtype=np.uint64)
-    nph = -(-mt // cb)
-    ends = np.zeros(nph, dtype=np.int32)
-    assert f(chunk, mt, nbs, delay, cb, out.ctypes.data, n, ends.ctypes.data, nph) == n
-    tl = [(int(t) & 0xF, (int(t) >> 4) & 0xFFFF, (int(t) >> 20) & 0xFFFF, (int(t) >> 36) & 0xFFFF,
-           (int(t) >> 52) & 0xF, (int(t) >> 56) & 0xF) for t in out]
-    return tl, [int(e) for e in ends]
-
-
-@pytest.mark.parametrize("mt,S,cb,delay", [(33, 4, 8, 100), (65, 8, 16, 444), (64, 16, 16, 444), (20, 8, 8, 0),
-                                           (7, 4, 8, 3), (1, 8, 16, 0), (97, 8, 8, 888), (49, 8, 24, 888)])
-def test_mixed_phased_ticket_order(mt, S, cb, delay):
-    # the phases in sequence are a valid order of all the tasks ...
-    tl, ends = tasks_phased(S, mt, 2, delay, cb)
-    replay(tl, mt, 2, S)
-    assert sorted(tl) == sorted(tasks(S, mt, 2, delay))
-    # ... phase p touches only tile columns below (p + 1) * cb, except the
-    # next phase's columns, which it gives only chunks closed before phase p
-    # began (chunk index below p * cb / S: panels of phases before p)
-    start = 0
-    for p, e in enumerate(ends):
-        c1 = min(mt, (p + 1) * cb)
-        for ty, k, m, n, bi, bj in tl[start:e]:
-            if n < c1:
-                assert k < c1, (p, ty, k, m, n)
-            else:
-                assert ty == 3 and n < min(mt, c1 + cb) and k < p * cb // S, (p, ty, k, m, n)
-        start = e
-    assert start == len(tl)
-    # every tile receives its chunks in increasing order
-    last = {}
-    for ty, k, m, n, bi, bj in tl:
-        if ty == 3:
-            assert last.get((m, n), -1) == k - 1, (k, m, n, last.get((m, n)))
-            last[(m, n)] = k
