@@ -1733,7 +1733,7 @@ int potrf_run_streamed(Context *ctx, const double *hA, double *A0, double *L, in
         return DPLASMA_ERR_NOT_SUPPORTED;
     }
     const int chunk = ctx->mx_chunk > 0 ? ctx->mx_chunk : (p16_fmt == 2 ? 8 : 16);
-    const int cb = ctx->stream_cb > 0 ? ctx->stream_cb : 16;       // tile columns per copy phase
+    const int cb = ctx->stream_cb > 0 ? ctx->stream_cb : 8;        // tile columns per copy phase
     // the ticket order of the mixed factorization (the same as for a matrix
     // already on the device, and the same cache)
     if (ctx->task_mt != mt || ctx->task_nbs != nbs || ctx->task_delay != ctx->mx_delay || ctx->task_mixed != chunk) {
