@@ -629,6 +629,13 @@ def run_gpu(args):
                 _, b, _, n0 = line.split()
                 traffic = float(b) * (N / float(n0)) ** 3
     peak16 = peaks.get("bf16_tflops")
+    if peak16:
+        peak_src = "measured dense bf16 burst (MEASURED_PEAKS.json)"
+    else:
+        # no measured figure on this box: the earlier measurement of this
+        # GPU pool (cuBLAS bf16 burst, 1.59 PFLOP/s)
+        peak16 = 1590.0
+        peak_src = "fallback: 1.59 PFLOP/s dense bf16 burst measured earlier on this pool (no MEASURED_PEAKS.json)"
     achieved = potrf_flops(N) / (fac_ms * 1e-3) / 1e12
     tensor_flops = potrf_flops(N) * (3.0 if fmt == 2 else 1.0)
     fac64 = statistics.median(r[2] for r in fp64)
@@ -657,10 +664,11 @@ def run_gpu(args):
                      "tensor_flops_per_launch": tensor_flops,
                      "tensor_achieved": tensor_flops / (fac_ms * 1e-3) / 1e12 if fac_ms else None,
                      "tensor_frac": tensor_flops / (fac_ms * 1e-3) / 1e12 / peak16 if (fac_ms and peak16) else None,
+                     "peak_source": peak_src,
                      "note": "achieved counts N^3/3 (FP64-equivalent) per launch, tensor_achieved the 16-bit "
-                             "tensor work actually issued (x3 in the split form); peak = dense bf16 burst of "
-                             "measured (MEASURED_PEAKS.json); the update tasks run the tensor pipe near its "
-                             "peak, the rest of the launch is the FP64 POTRF/TRSM work and its chain"},
+                             "tensor work actually issued (x3 in the split form); the update tasks run the "
+                             "tensor pipe near its peak, the rest of the launch is the POTRF work, the TRSM "
+                             "strips and their chain"},
         "roofline_fp64": {"bound": "tensor", "achieved": ach64, "peak": peak64, "unit": "TFLOP/s",
                           "frac": ach64 / peak64 if peak64 > 0 else None,
                           "kernel": "potrf_persistent_kernel<false> (FP64 DMMA)",
